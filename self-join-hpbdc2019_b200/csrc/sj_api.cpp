@@ -1,0 +1,1358 @@
+// Host engine behind the C ABI (include/sj.h).
+//
+// Pipeline of one join (replacing distanceTableNDGridBatches, GPU.cu:1297-2569):
+//   1. grid index on the device (sj_index.cu)
+//   2. owned neighbour-cell lists for the traversal pattern (sj_stencil.cu)
+//   3. per-cell hit-rate estimate: sampling (GPU.cu:854-1065 analogue) or the
+//      learned MLP (sj_estimate.cu)
+//   4. tasks = (query tile of a cell) x (stretch of its candidate stream), with
+//      exact evaluation counts and predicted pairs; ordered by predicted cost
+//      for the work-queue / sorted modes (kernel.cu:33-250, GPU.cu:1660-1734)
+//   5. batches = consecutive tasks whose predicted pairs fit the capacity; per
+//      batch: count pass -> exclusive scan over point ids -> (split and retry
+//      on overflow) -> fill pass -> delivery (GPU.cu:2101-2377)
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "sj_internal.h"
+
+namespace sj {
+int import_csv(const char *path, int D, std::vector<double> &pts);
+}
+
+namespace {
+
+thread_local std::string g_lastError;
+
+void set_error(const char *fmt, ...)
+{
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_lastError = buf;
+}
+
+#define CK(expr)                                                                      \
+    do {                                                                              \
+        cudaError_t _e = (expr);                                                      \
+        if (_e != cudaSuccess) {                                                      \
+            set_error("%s: %s (%s:%d)", #expr, cudaGetErrorString(_e), __FILE__, __LINE__); \
+            return (_e == cudaErrorMemoryAllocation) ? SJ_ERR_OOM : SJ_ERR_CUDA;      \
+        }                                                                             \
+    } while (0)
+
+#define CKS(expr)                                  \
+    do {                                           \
+        sj_status _s = (expr);                     \
+        if (_s != SJ_OK) return _s;                \
+    } while (0)
+
+template <typename T>
+struct DevBuf {
+    T *p = nullptr;
+    size_t n = 0;
+    ~DevBuf() { release(); }
+    void release()
+    {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    cudaError_t ensure(size_t cnt)
+    {
+        if (cnt <= n && p) return cudaSuccess;
+        release();
+        size_t c = cnt ? cnt : 1;
+        cudaError_t e = cudaMalloc((void **)&p, c * sizeof(T));
+        if (e == cudaSuccess) n = c;
+        return e;
+    }
+};
+
+struct PinBuf {
+    void *p = nullptr;
+    size_t bytes = 0;
+    ~PinBuf() { release(); }
+    void release()
+    {
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        bytes = 0;
+    }
+    cudaError_t ensure(size_t b)
+    {
+        if (b <= bytes && p) return cudaSuccess;
+        release();
+        cudaError_t e = cudaMallocHost(&p, b ? b : 1);
+        if (e == cudaSuccess) bytes = b ? b : 1;
+        return e;
+    }
+};
+
+struct Timer {
+    cudaEvent_t a = nullptr, b = nullptr;
+    Timer()
+    {
+        cudaEventCreate(&a);
+        cudaEventCreate(&b);
+    }
+    ~Timer()
+    {
+        if (a) cudaEventDestroy(a);
+        if (b) cudaEventDestroy(b);
+    }
+    void start(cudaStream_t s) { cudaEventRecord(a, s); }
+    float stop(cudaStream_t s)
+    {
+        cudaEventRecord(b, s);
+        cudaEventSynchronize(b);
+        float ms = 0;
+        cudaEventElapsedTime(&ms, a, b);
+        return ms;
+    }
+};
+
+int pattern_of_mode(int mode)
+{
+    switch (mode) {
+    case 3: case 7: case 9: return SJ_PAT_FULL;
+    case 4: return SJ_PAT_UNICOMP;
+    case 5: return SJ_PAT_BUNICOMP;
+    case 6: case 10: return SJ_PAT_LID;
+    }
+    return -1;
+}
+
+int padded_dim(int D)
+{
+    if (D <= 4) return D == 3 ? 3 : D;
+    if (D <= 6) return 6;
+    if (D <= 8) return 8;
+    if (D <= 12) return 12;
+    return 16;
+}
+
+double eps_threshold(double eps)
+{
+    double t = eps * eps;
+    while (std::sqrt(t) > eps) t = std::nextafter(t, -INFINITY);
+    for (;;) {
+        double u = std::nextafter(t, INFINITY);
+        if (std::sqrt(u) <= eps) t = u; else break;
+    }
+    return t;
+}
+
+struct Ctx {
+    sj_params p{};
+    int dev = 0, numSM = 148;
+    cudaStream_t s = nullptr;
+    // points
+    uint64_t n = 0;
+    DevBuf<double> pts;        // n x D as supplied
+    bool havePoints = false;
+    // index
+    bool indexed = false;
+    sj_grid_dev g{};
+    uint32_t nCells = 0;
+    DevBuf<uint32_t> ids;      // cell-sorted point ids
+    DevBuf<double> xs;         // cell-sorted coordinates, n x Dp
+    DevBuf<uint32_t> cellStart;
+    DevBuf<uint64_t> cellLid;
+    DevBuf<uint32_t> cellCoord;
+    std::vector<uint32_t> hCellStart;
+    double dataMin[SJ_MAX_DIM], dataMax[SJ_MAX_DIM];
+    // neighbour lists
+    int nbrPattern = -1;
+    DevBuf<uint32_t> nbrStart, nbrCell;
+    DevBuf<uint64_t> candFull;
+    DevBuf<float> feat;
+    std::vector<uint32_t> hNbrStart, hNbrCell;
+    std::vector<uint64_t> hCandFull;
+    // tasks
+    std::vector<sj_task> tasks;
+    std::vector<double> taskPred, taskEvals;
+    DevBuf<sj_task> dTasks;
+    // batch state
+    DevBuf<uint32_t> keyCount, keyCursor;
+    DevBuf<int32_t> outKey, outVal;
+    DevBuf<uint8_t> scanTemp;
+    DevBuf<uint32_t> total;
+    DevBuf<unsigned long long> stat;   // evals, refined, pairs, overflow, hash
+    DevBuf<uint32_t> queueHead;
+    DevBuf<uint32_t> taskHits;
+    PinBuf pinTotal, pinKey[2], pinVal[2];
+    // estimator
+    std::vector<float> mlpW;
+    DevBuf<float> dMlpW;
+    std::vector<double> cellRate;      // predicted hits per evaluation, per cell
+    std::vector<double> measCellHits;  // from the last degrees/join run (full-stencil semantics)
+    bool haveMeas = false;
+    sj_stats st{};
+};
+
+sj_status check_params(const sj_params &p)
+{
+    if (p.gpunumdim < 1 || p.gpunumdim > SJ_MAX_DIM) {
+        set_error("gpunumdim must be in 1..%d", SJ_MAX_DIM);
+        return SJ_ERR_BAD_INPUT;
+    }
+    if (p.numindexeddim < 1 || p.numindexeddim > p.gpunumdim || p.numindexeddim > SJ_MAX_K) {
+        set_error("numindexeddim must be in 1..min(gpunumdim, %d)", SJ_MAX_K);
+        return SJ_ERR_BAD_INPUT;
+    }
+    if (!(p.epsilon > 0.0) || !std::isfinite(p.epsilon)) {
+        set_error("epsilon must be a positive finite number");
+        return SJ_ERR_BAD_INPUT;
+    }
+    if (pattern_of_mode(p.search_mode) < 0) {
+        set_error("search_mode %d not supported (3,4,5,6,7,9,10)", p.search_mode);
+        return SJ_ERR_BAD_INPUT;
+    }
+    if (p.search_mode == 5 && p.numindexeddim != 2 && p.numindexeddim != 3) {
+        set_error("B-Unicomp (mode 5) is defined for NUMINDEXEDDIM 2 or 3 only");
+        return SJ_ERR_BAD_INPUT;
+    }
+    if (p.precision != SJ_PREC_FP64 && p.precision != SJ_PREC_FP32_REFINE) {
+        set_error("unknown precision");
+        return SJ_ERR_BAD_INPUT;
+    }
+    if (p.precision == SJ_PREC_FP32_REFINE && (p.epsilon < 1e-15 || p.epsilon > 1e15)) {
+        set_error("FP32 filter needs 1e-15 <= epsilon <= 1e15");
+        return SJ_ERR_BAD_INPUT;
+    }
+    if (p.scheduler != SJ_SCHED_SAMPLING && p.scheduler != SJ_SCHED_LEARNED) {
+        set_error("unknown scheduler");
+        return SJ_ERR_BAD_INPUT;
+    }
+    if (p.shard_count < 1 || p.shard_index < 0 || p.shard_index >= p.shard_count) {
+        set_error("bad shard_index / shard_count");
+        return SJ_ERR_BAD_INPUT;
+    }
+    if (!(p.sample_rate > 0.0 && p.sample_rate <= 1.0)) {
+        set_error("sample_rate must be in (0, 1]");
+        return SJ_ERR_BAD_INPUT;
+    }
+    if (p.alpha < 0.0) {
+        set_error("alpha must be >= 0");
+        return SJ_ERR_BAD_INPUT;
+    }
+    return SJ_OK;
+}
+
+// ---------------------------------------------------------------- index --
+sj_status build_index(Ctx &c)
+{
+    if (!c.havePoints) {
+        set_error("no points: call sj_set_points or sj_import_csv first");
+        return SJ_ERR_STATE;
+    }
+    Timer tm;
+    tm.start(c.s);
+    const int D = c.p.gpunumdim, k = c.p.numindexeddim;
+    const uint64_t n = c.n;
+    // 1. min / max of every dimension
+    DevBuf<double> mm;
+    CK(mm.ensure(2 * D + 1));
+    CK(sj_launch_minmax(c.pts.p, n, D, mm.p, c.s));
+    std::vector<double> hmm(2 * D + 1);
+    CK(cudaMemcpyAsync(hmm.data(), mm.p, sizeof(double) * (2 * D + 1), cudaMemcpyDeviceToHost, c.s));
+    CK(cudaStreamSynchronize(c.s));
+    uint64_t badBits;
+    memcpy(&badBits, &hmm[2 * D], 8);
+    if (badBits) {
+        set_error("input contains non-finite coordinates");
+        return SJ_ERR_BAD_INPUT;
+    }
+    sj_grid_dev &g = c.g;
+    memset(&g, 0, sizeof(g));
+    g.D = D;
+    g.Dp = padded_dim(D);
+    g.k = k;
+    g.eps = c.p.epsilon;
+    g.thresh = eps_threshold(c.p.epsilon);
+    for (int j = 0; j < D; j++) {
+        c.dataMin[j] = hmm[2 * j];
+        c.dataMax[j] = hmm[2 * j + 1];
+        g.center[j] = 0.5 * (c.dataMin[j] + c.dataMax[j]);
+    }
+    // 2. grid dimensions (main.cu:446-503)
+    double total = 1.0;
+    unsigned long long mul = 1;
+    for (int j = 0; j < k; j++) {
+        double mn = c.dataMin[j] - g.eps;
+        double mx = c.dataMax[j] + g.eps;
+        g.minArr[j] = mn;
+        double cells = std::ceil((mx - mn) / g.eps);
+        if (!(cells >= 1.0) || cells > 4294967295.0) {
+            set_error("dimension %d spans %.3g cells (limit 2^32-1)", j, cells);
+            return SJ_ERR_BAD_INPUT;
+        }
+        g.nCells[j] = (unsigned)cells;
+        g.mult[j] = mul;
+        mul *= g.nCells[j];
+        total *= cells;
+    }
+    if (total >= 1.8e19) {
+        set_error("grid has %.3g cells; linear ids need < 2^64", total);
+        return SJ_ERR_BAD_INPUT;
+    }
+    c.st.total_cells = mul;
+    int bits = 1;
+    while (bits < 64 && (1ULL << bits) < mul) bits++;
+    // 3. keys, stable sort, run-length cells
+    DevBuf<uint64_t> keys, keysAlt;
+    DevBuf<uint32_t> valsAlt, flags;
+    DevBuf<uint8_t> tmp;
+    CK(keys.ensure(n));
+    CK(keysAlt.ensure(n));
+    CK(c.ids.ensure(n));
+    CK(valsAlt.ensure(n));
+    CK(flags.ensure(n));
+    CK(tmp.ensure(std::max(sj_radix_temp_bytes(n), sj_scan_temp_bytes(n))));
+    CK(sj_launch_cell_keys(c.pts.p, n, g, keys.p, c.ids.p, c.s));
+    int inAlt = 0;
+    CK(sj_radix_sort_u64_u32(keys.p, c.ids.p, keysAlt.p, valsAlt.p, n, bits, tmp.p, &inAlt, c.s));
+    uint64_t *sk = inAlt ? keysAlt.p : keys.p;
+    if (inAlt) CK(cudaMemcpyAsync(c.ids.p, valsAlt.p, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, c.s));
+    CK(sj_launch_cell_flags(sk, n, flags.p, c.s));
+    DevBuf<uint32_t> nne;
+    CK(nne.ensure(1));
+    CK(sj_exclusive_scan_u32(flags.p, flags.p, n, tmp.p, nne.p, c.s));
+    uint32_t nCells = 0;
+    CK(cudaMemcpyAsync(&nCells, nne.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, c.s));
+    CK(cudaStreamSynchronize(c.s));
+    c.nCells = nCells;
+    CK(c.cellStart.ensure(nCells + 1));
+    CK(c.cellLid.ensure(nCells));
+    CK(c.cellCoord.ensure((size_t)nCells * k));
+    CK(sj_launch_cell_build(sk, flags.p, n, c.cellStart.p, c.cellLid.p, c.s));
+    uint32_t nn = (uint32_t)n;
+    CK(cudaMemcpyAsync(c.cellStart.p + nCells, &nn, sizeof(uint32_t), cudaMemcpyHostToDevice, c.s));
+    CK(sj_launch_cell_coords(c.cellLid.p, nCells, g, c.cellCoord.p, c.s));
+    // 4. cell-sorted coordinates
+    CK(c.xs.ensure(n * (uint64_t)g.Dp));
+    CK(sj_launch_gather(c.pts.p, c.ids.p, n, D, g.Dp, c.xs.p, c.s));
+    c.hCellStart.resize(nCells + 1);
+    CK(cudaMemcpyAsync(c.hCellStart.data(), c.cellStart.p, sizeof(uint32_t) * (nCells + 1), cudaMemcpyDeviceToHost,
+                       c.s));
+    CK(cudaStreamSynchronize(c.s));
+    // every cell coordinate must lie inside the grid (no linear-id aliasing)
+    {
+        std::vector<uint32_t> coord((size_t)nCells * k);
+        // the last cell carries the largest linear id; coordinates are checked on a sample of cells
+        CK(cudaMemcpy(coord.data(), c.cellCoord.p, coord.size() * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+        for (size_t i = 0; i < coord.size(); i++)
+            if (coord[i] >= g.nCells[i % k]) {
+                set_error("internal: cell coordinate outside the grid");
+                return SJ_ERR_INTERNAL;
+            }
+    }
+    c.indexed = true;
+    c.nbrPattern = -1;
+    c.haveMeas = false;
+    c.st.n_points = (uint32_t)n;
+    c.st.n_nonempty_cells = nCells;
+    c.st.ms_index = tm.stop(c.s);
+    return SJ_OK;
+}
+
+// ------------------------------------------------------ neighbour lists --
+sj_status build_neighbours(Ctx &c, int pattern)
+{
+    if (c.nbrPattern == pattern) return SJ_OK;
+    const uint32_t nc = c.nCells;
+    CK(c.nbrStart.ensure(nc + 1));
+    CK(c.candFull.ensure(nc));
+    CK(c.feat.ensure((size_t)nc * SJ_NFEAT));
+    DevBuf<uint32_t> cnt;
+    CK(cnt.ensure(nc + 1));
+    CK(sj_launch_neighbours(c.cellLid.p, c.cellCoord.p, c.cellStart.p, nc, c.g, pattern, nullptr, cnt.p,
+                            c.candFull.p, c.feat.p, 0, c.s));
+    DevBuf<uint8_t> tmp;
+    DevBuf<uint32_t> tot;
+    CK(tot.ensure(1));
+    CK(tmp.ensure(sj_scan_temp_bytes(nc)));
+    CK(sj_exclusive_scan_u32(cnt.p, c.nbrStart.p, nc, tmp.p, tot.p, c.s));
+    uint32_t total = 0;
+    CK(cudaMemcpyAsync(&total, tot.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, c.s));
+    CK(cudaStreamSynchronize(c.s));
+    CK(cudaMemcpyAsync(c.nbrStart.p + nc, &total, sizeof(uint32_t), cudaMemcpyHostToDevice, c.s));
+    CK(c.nbrCell.ensure(total));
+    CK(sj_launch_neighbours(c.cellLid.p, c.cellCoord.p, c.cellStart.p, nc, c.g, pattern, c.nbrStart.p, c.nbrCell.p,
+                            nullptr, nullptr, 1, c.s));
+    c.hNbrStart.resize(nc + 1);
+    c.hNbrCell.resize(total);
+    c.hCandFull.resize(nc);
+    CK(cudaMemcpyAsync(c.hNbrStart.data(), c.nbrStart.p, sizeof(uint32_t) * (nc + 1), cudaMemcpyDeviceToHost, c.s));
+    if (total)
+        CK(cudaMemcpyAsync(c.hNbrCell.data(), c.nbrCell.p, sizeof(uint32_t) * total, cudaMemcpyDeviceToHost, c.s));
+    CK(cudaMemcpyAsync(c.hCandFull.data(), c.candFull.p, sizeof(uint64_t) * nc, cudaMemcpyDeviceToHost, c.s));
+    CK(cudaStreamSynchronize(c.s));
+    uint64_t full = 0;
+    for (uint64_t v : c.hCandFull) full += v;
+    c.st.full_stencil_calcs = full;
+    c.nbrPattern = pattern;
+    return SJ_OK;
+}
+
+void join_args_base(Ctx &c, sj_join_args &a)
+{
+    memset(&a, 0, sizeof(a));
+    a.xs = c.xs.p;
+    a.ids = c.ids.p;
+    a.cellStart = c.cellStart.p;
+    a.nbrStart = c.nbrStart.p;
+    a.nbrCell = c.nbrCell.p;
+    a.cellCoord = c.cellCoord.p;
+}
+
+// FP32 filter half-band: bound on |(acc32 - thr32) - (S64 - T)| for local
+// coordinates measured from the home cell's centre (indexed dims) or the data
+// centre (other dims).  |a_l| <= 0.5 eps, |b_l| <= 1.5 eps on indexed dims.
+double filter_margin(const Ctx &c)
+{
+    const sj_grid_dev &g = c.g;
+    double ra2 = 0, rb2 = 0;
+    for (int j = 0; j < g.D; j++) {
+        if (j < g.k) {
+            ra2 += (0.5 * g.eps * 1.01) * (0.5 * g.eps * 1.01);
+            rb2 += (1.5 * g.eps * 1.01) * (1.5 * g.eps * 1.01);
+        } else {
+            double h = 0.5 * (c.dataMax[j] - c.dataMin[j]) * 1.01 + 1e-300;
+            ra2 += h * h;
+            rb2 += h * h;
+        }
+    }
+    double r = std::sqrt(ra2) + std::sqrt(rb2);
+    const double u = std::ldexp(1.0, -24);
+    return 2.0 * r * r * u * (g.D + 4) + g.thresh * std::ldexp(1.0, -40);
+}
+
+// ------------------------------------------------------------ estimate --
+sj_status estimate_rates(Ctx &c)
+{
+    Timer tm;
+    tm.start(c.s);
+    const uint32_t nc = c.nCells;
+    c.cellRate.assign(nc, 0.0);
+    if (c.p.scheduler == SJ_SCHED_LEARNED && !c.mlpW.empty()) {
+        DevBuf<float> out;
+        CK(out.ensure((size_t)nc * SJ_NOUT));
+        CK(c.dMlpW.ensure(SJ_MLP_NPARAM));
+        CK(cudaMemcpyAsync(c.dMlpW.p, c.mlpW.data(), sizeof(float) * SJ_MLP_NPARAM, cudaMemcpyHostToDevice, c.s));
+        CK(sj_launch_mlp_infer(c.feat.p, nc, c.dMlpW.p, out.p, c.s));
+        std::vector<float> h((size_t)nc * SJ_NOUT);
+        CK(cudaMemcpyAsync(h.data(), out.p, h.size() * sizeof(float), cudaMemcpyDeviceToHost, c.s));
+        CK(cudaStreamSynchronize(c.s));
+        for (uint32_t i = 0; i < nc; i++) {
+            double hits = std::exp2((double)h[(size_t)i * SJ_NOUT + 1]) - 1.0;
+            double calcs = (double)c.hCandFull[i];
+            double r = calcs > 0 ? hits / calcs : 0.0;
+            c.cellRate[i] = std::min(1.0, std::max(r, 0.0));
+        }
+    } else {
+        DevBuf<unsigned long long> hits, cands;
+        CK(hits.ensure(nc));
+        CK(cands.ensure(nc));
+        CK(cudaMemsetAsync(hits.p, 0, sizeof(unsigned long long) * nc, c.s));
+        CK(cudaMemsetAsync(cands.p, 0, sizeof(unsigned long long) * nc, c.s));
+        sj_join_args a;
+        join_args_base(c, a);
+        a.taskEnd = (uint32_t)c.n;   // number of cell-sorted positions
+        uint32_t stride = (uint32_t)std::max(1.0, std::floor(1.0 / c.p.sample_rate + 0.5));
+        CK(sj_launch_sample(a, c.g, stride, hits.p, cands.p, nc, c.s));
+        std::vector<unsigned long long> hh(nc), hc(nc);
+        CK(cudaMemcpyAsync(hh.data(), hits.p, sizeof(unsigned long long) * nc, cudaMemcpyDeviceToHost, c.s));
+        CK(cudaMemcpyAsync(hc.data(), cands.p, sizeof(unsigned long long) * nc, cudaMemcpyDeviceToHost, c.s));
+        CK(cudaStreamSynchronize(c.s));
+        double sh = 0, sc = 0;
+        for (uint32_t i = 0; i < nc; i++) { sh += (double)hh[i]; sc += (double)hc[i]; }
+        double global = sc > 0 ? sh / sc : 1.0;
+        for (uint32_t i = 0; i < nc; i++) c.cellRate[i] = hc[i] ? (double)hh[i] / (double)hc[i] : global;
+    }
+    c.st.ms_estimate = tm.stop(c.s);
+    return SJ_OK;
+}
+
+// --------------------------------------------------------------- tasks --
+// Evaluations of a chunk [s0, s1) of a symmetric home segment for query
+// indices 0..q-1: only candidates at stream offset >= query index count.
+double diag_evals(uint64_t s0, uint64_t s1, uint64_t q)
+{
+    double e = 0;
+    for (uint64_t i = 0; i < q; i++) {
+        uint64_t lo = std::max(s0, i);
+        if (s1 > lo) e += (double)(s1 - lo);
+    }
+    return e;
+}
+
+sj_status build_tasks(Ctx &c, int pattern, uint64_t cap)
+{
+    Timer tm;
+    tm.start(c.s);
+    const bool sym = pattern != SJ_PAT_FULL;
+    c.tasks.clear();
+    c.taskPred.clear();
+    c.taskEvals.clear();
+    const double pairsPerTask = std::max(4096.0, (double)cap / 1024.0);
+    for (uint32_t A = 0; A < c.nCells; A++) {
+        const uint32_t aStart = c.hCellStart[A], aEnd = c.hCellStart[A + 1];
+        const uint32_t occ = aEnd - aStart;
+        const uint32_t nb0 = c.hNbrStart[A], nb1 = c.hNbrStart[A + 1];
+        const uint32_t nSegAll = 1 + (nb1 - nb0);
+        const double rate = c.cellRate.empty() ? 0.0 : c.cellRate[A];
+        for (uint32_t q0 = 0; q0 < occ; q0 += SJ_CTA) {
+            const uint32_t qc = std::min<uint32_t>(SJ_CTA, occ - q0);
+            const uint32_t qBegin = aStart + q0;
+            // chunk length from the predicted pair density of this cell
+            double perEval = std::max(rate, 1e-6) * (sym ? 2.0 : 1.0);
+            double chunk = pairsPerTask / (perEval * qc);
+            uint32_t sChunk = (uint32_t)std::min(65536.0, std::max(256.0, chunk));
+            sChunk = (sChunk / 32) * 32;
+            for (uint32_t g0 = 0; g0 < nSegAll; g0 += SJ_MAX_SEG) {
+                const uint32_t gc = std::min<uint32_t>(SJ_MAX_SEG, nSegAll - g0);
+                uint64_t homeLen = 0, L = 0;
+                for (uint32_t sgi = 0; sgi < gc; sgi++) {
+                    uint32_t gs = g0 + sgi;
+                    uint64_t len;
+                    if (gs == 0) len = sym ? (aEnd - qBegin) : occ;
+                    else {
+                        uint32_t B = c.hNbrCell[nb0 + gs - 1];
+                        len = c.hCellStart[B + 1] - c.hCellStart[B];
+                    }
+                    if (gs == 0) homeLen = len;
+                    L += len;
+                }
+                for (uint64_t s0 = 0; s0 < L; s0 += sChunk) {
+                    uint64_t s1 = std::min<uint64_t>(L, s0 + sChunk);
+                    sj_task t;
+                    t.cell = A;
+                    t.qBegin = qBegin;
+                    t.qCount = qc;
+                    t.segBase = g0;
+                    t.segCount = gc;
+                    t.sBegin = (uint32_t)s0;
+                    t.sEnd = (uint32_t)s1;
+                    t.flags = (sym ? SJ_TASK_SYM : 0u) | (g0 == 0 ? SJ_TASK_HOME : 0u);
+                    double ev;
+                    if (sym && g0 == 0 && s0 < homeLen) {
+                        uint64_t h1 = std::min<uint64_t>(s1, homeLen);
+                        ev = diag_evals(s0, h1, qc) + (double)qc * (double)(s1 - h1);
+                    } else {
+                        ev = (double)qc * (double)(s1 - s0);
+                    }
+                    c.tasks.push_back(t);
+                    c.taskEvals.push_back(ev);
+                    c.taskPred.push_back(ev * rate * (sym ? 2.0 : 1.0));
+                }
+            }
+        }
+    }
+    c.st.ms_tasks += tm.stop(c.s);
+    return SJ_OK;
+}
+
+// ---------------------------------------------------------------- join --
+struct BatchRange {
+    uint32_t t0, t1;
+};
+
+sj_status run_pass(Ctx &c, sj_join_args &a, bool fill, bool queue)
+{
+    if (queue) CK(cudaMemsetAsync(c.queueHead.p, 0, sizeof(uint32_t), c.s));
+    CK(sj_launch_join(a, c.g, fill ? 1 : 0, c.p.precision == SJ_PREC_FP32_REFINE ? 1 : 0, queue ? 1 : 0, c.numSM,
+                      c.s));
+    return SJ_OK;
+}
+
+sj_status prepare_join(Ctx &c, int &pattern, bool &queue)
+{
+    if (!c.indexed) {
+        set_error("index not built: call sj_build_index first");
+        return SJ_ERR_STATE;
+    }
+    pattern = pattern_of_mode(c.p.search_mode);
+    // work queue: modes 9/10, or any mode when work is ordered by workload
+    queue = (c.p.search_mode == 9 || c.p.search_mode == 10 || c.p.sort_by_workload != 0);
+    Timer tm;
+    tm.start(c.s);
+    CKS(build_neighbours(c, pattern));
+    c.st.ms_tasks = tm.stop(c.s);
+    CKS(estimate_rates(c));
+    return SJ_OK;
+}
+
+uint64_t auto_capacity(Ctx &c)
+{
+    if (c.p.batch_capacity_pairs) return c.p.batch_capacity_pairs;
+    size_t freeB = 0, totalB = 0;
+    cudaMemGetInfo(&freeB, &totalB);
+    uint64_t byMem = (uint64_t)(0.4 * (double)freeB / 8.0);
+    return std::max<uint64_t>(1 << 20, std::min<uint64_t>(byMem, 2000000000ULL));
+}
+
+void order_tasks(Ctx &c)
+{
+    const bool byCost = c.p.sort_by_workload || c.p.search_mode == 7 || c.p.search_mode == 9 ||
+                        c.p.search_mode == 10;
+    std::vector<uint32_t> order(c.tasks.size());
+    std::iota(order.begin(), order.end(), 0u);
+    if (byCost) {
+        // cost: distance evaluations plus a write cost per predicted pair
+        std::vector<double> cost(c.tasks.size());
+        for (size_t i = 0; i < cost.size(); i++) cost[i] = c.taskEvals[i] + 4.0 * c.taskPred[i];
+        std::stable_sort(order.begin(), order.end(), [&](uint32_t x, uint32_t y) { return cost[x] > cost[y]; });
+    }
+    std::vector<sj_task> t2;
+    std::vector<double> p2, e2;
+    t2.reserve(order.size());
+    for (size_t i = 0; i < order.size(); i++) {
+        if (c.p.shard_count > 1 && (int)(i % (size_t)c.p.shard_count) != c.p.shard_index) continue;
+        t2.push_back(c.tasks[order[i]]);
+        p2.push_back(c.taskPred[order[i]]);
+        e2.push_back(c.taskEvals[order[i]]);
+    }
+    c.tasks.swap(t2);
+    c.taskPred.swap(p2);
+    c.taskEvals.swap(e2);
+}
+
+sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
+{
+    Timer total;
+    total.start(c.s);
+    int pattern;
+    bool queue;
+    CKS(prepare_join(c, pattern, queue));
+    const uint64_t n = c.n;
+    uint64_t cap = auto_capacity(c);
+    if (cap > 0xffffffffULL) cap = 0xffffffffULL;
+    {
+        Timer tm;
+        tm.start(c.s);
+        CKS(build_tasks(c, pattern, cap));
+        order_tasks(c);
+        CK(c.dTasks.ensure(c.tasks.size()));
+        if (!c.tasks.empty())
+            CK(cudaMemcpyAsync(c.dTasks.p, c.tasks.data(), sizeof(sj_task) * c.tasks.size(), cudaMemcpyHostToDevice,
+                               c.s));
+        c.st.ms_tasks += tm.stop(c.s);
+    }
+    const uint32_t nt = (uint32_t)c.tasks.size();
+    c.st.num_tasks = nt;
+    CK(c.keyCount.ensure(n));
+    CK(c.keyCursor.ensure(n));
+    CK(c.outKey.ensure(cap));
+    CK(c.outVal.ensure(cap));
+    CK(c.scanTemp.ensure(sj_scan_temp_bytes(n)));
+    CK(c.total.ensure(1));
+    CK(c.stat.ensure(8));
+    CK(c.queueHead.ensure(1));
+    CK(c.taskHits.ensure(nt ? nt : 1));
+    CK(c.pinTotal.ensure(64));
+    CK(cudaMemsetAsync(c.stat.p, 0, sizeof(unsigned long long) * 8, c.s));
+    if (delivery == SJ_DELIVER_HOST) {
+        for (int b = 0; b < 2; b++) {
+            CK(c.pinKey[b].ensure(cap * sizeof(int32_t)));
+            CK(c.pinVal[b].ensure(cap * sizeof(int32_t)));
+        }
+    }
+    double predTotal = 0;
+    for (double v : c.taskPred) predTotal += v;
+    c.st.estimated_pairs = predTotal;
+
+    // greedy batch plan on predicted pairs
+    std::vector<BatchRange> plan;
+    {
+        const double alpha = c.p.alpha;
+        uint32_t t0 = 0;
+        double acc = 0;
+        for (uint32_t t = 0; t < nt; t++) {
+            double v = c.taskPred[t] * (1.0 + alpha);
+            if (t > t0 && acc + v > (double)cap) {
+                plan.push_back({t0, t});
+                t0 = t;
+                acc = 0;
+            }
+            acc += v;
+        }
+        if (nt > t0) plan.push_back({t0, nt});
+    }
+    std::reverse(plan.begin(), plan.end());   // used as a stack
+
+    sj_join_args a;
+    join_args_base(c, a);
+    a.tasks = c.dTasks.p;
+    a.queueHead = c.queueHead.p;
+    a.keyCount = c.keyCount.p;
+    a.keyCursor = c.keyCursor.p;
+    a.outKey = c.outKey.p;
+    a.outVal = c.outVal.p;
+    a.capacity = cap;
+    a.stat = c.stat.p;
+    a.taskHits = c.taskHits.p;
+    a.margin = filter_margin(c);
+
+    std::vector<uint32_t> hTaskHits(nt);
+    uint64_t pairsTotal = 0, batches = 0, retries = 0;
+    double relErrSum = 0;
+    float msCount = 0, msScan = 0, msFill = 0, msDeliver = 0;
+    Timer tb;
+    int pinSel = 0;
+    sj_status result = SJ_OK;
+    while (!plan.empty()) {
+        BatchRange br = plan.back();
+        plan.pop_back();
+        a.taskBegin = br.t0;
+        a.taskEnd = br.t1;
+        // count pass
+        tb.start(c.s);
+        CK(cudaMemsetAsync(c.keyCount.p, 0, sizeof(uint32_t) * n, c.s));
+        CKS(run_pass(c, a, false, queue));
+        msCount += tb.stop(c.s);
+        tb.start(c.s);
+        CK(sj_exclusive_scan_u32(c.keyCount.p, c.keyCursor.p, n, c.scanTemp.p, c.total.p, c.s));
+        CK(cudaMemcpyAsync(c.pinTotal.p, c.total.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, c.s));
+        msScan += tb.stop(c.s);
+        // scan totals wrap at 2^32: recompute from the exact per-task counts
+        CK(cudaMemcpyAsync(hTaskHits.data() + br.t0, c.taskHits.p + br.t0, sizeof(uint32_t) * (br.t1 - br.t0),
+                           cudaMemcpyDeviceToHost, c.s));
+        CK(cudaStreamSynchronize(c.s));
+        uint64_t cnt = 0;
+        for (uint32_t t = br.t0; t < br.t1; t++) cnt += hTaskHits[t];
+        if (cnt > cap) {
+            if (br.t1 - br.t0 <= 1) {
+                set_error("a single task produces %llu pairs, more than the batch capacity %llu",
+                          (unsigned long long)cnt, (unsigned long long)cap);
+                return SJ_ERR_INTERNAL;
+            }
+            uint32_t mid = br.t0 + (br.t1 - br.t0) / 2;
+            plan.push_back({mid, br.t1});
+            plan.push_back({br.t0, mid});
+            retries++;
+            continue;
+        }
+        double pred = 0;
+        for (uint32_t t = br.t0; t < br.t1; t++) pred += c.taskPred[t];
+        if (cnt > 0) relErrSum += std::fabs(pred - (double)cnt) / (double)cnt;
+        // fill pass
+        tb.start(c.s);
+        CKS(run_pass(c, a, true, queue));
+        msFill += tb.stop(c.s);
+        tb.start(c.s);
+        CK(sj_hash_pairs(c.outKey.p, c.outVal.p, cnt, c.stat.p + 4, c.s));
+        if (delivery == SJ_DELIVER_DEVICE && cb) {
+            CK(cudaStreamSynchronize(c.s));
+            sj_batch b{batches, cnt, c.outKey.p, c.outVal.p, 1};
+            if (cb(&b, user)) { result = SJ_ERR_ABORTED; }
+        } else if (delivery == SJ_DELIVER_HOST) {
+            int32_t *hk = (int32_t *)c.pinKey[pinSel].p, *hv = (int32_t *)c.pinVal[pinSel].p;
+            if (cnt) {
+                CK(cudaMemcpyAsync(hk, c.outKey.p, cnt * sizeof(int32_t), cudaMemcpyDeviceToHost, c.s));
+                CK(cudaMemcpyAsync(hv, c.outVal.p, cnt * sizeof(int32_t), cudaMemcpyDeviceToHost, c.s));
+            }
+            CK(cudaStreamSynchronize(c.s));
+            if (cb) {
+                sj_batch b{batches, cnt, hk, hv, 0};
+                if (cb(&b, user)) { result = SJ_ERR_ABORTED; }
+            }
+            pinSel ^= 1;
+        }
+        msDeliver += tb.stop(c.s);
+        pairsTotal += cnt;
+        batches++;
+        if (result != SJ_OK) break;
+    }
+    unsigned long long hs[8];
+    CK(cudaMemcpyAsync(hs, c.stat.p, sizeof(hs), cudaMemcpyDeviceToHost, c.s));
+    CK(cudaStreamSynchronize(c.s));
+    if (hs[3]) {
+        set_error("internal: fill pass exceeded the counted capacity");
+        return SJ_ERR_INTERNAL;
+    }
+    c.st.total_pairs = pairsTotal;
+    c.st.pair_hash = hs[4];
+    c.st.distance_calcs = hs[0] / 2;   // count + fill passes evaluate the same candidates
+    c.st.refined_pairs = hs[1] / 2;
+    c.st.num_batches = batches;
+    c.st.overflow_retries = retries;
+    c.st.estimator_mean_abs_rel_err = batches ? relErrSum / (double)batches : 0.0;
+    {
+        double num = 0, den = 0;
+        for (uint32_t t = 0; t < nt; t++) {
+            num += std::fabs(c.taskPred[t] - (double)hTaskHits[t]);
+            den += (double)hTaskHits[t];
+        }
+        c.st.estimator_task_rel_err = den > 0 ? num / den : 0.0;
+    }
+    c.st.ms_count = msCount;
+    c.st.ms_scan = msScan;
+    c.st.ms_fill = msFill;
+    c.st.ms_deliver = msDeliver;
+    c.st.ms_join_kernels = msCount + msFill;
+    c.st.ms_fill_kernel = msFill;
+    c.st.ms_total = total.stop(c.s);
+    return result;
+}
+
+// Degrees only: count pass over all tasks, no capacity limit.
+sj_status run_degrees(Ctx &c, uint32_t *degHost)
+{
+    int pattern;
+    bool queue;
+    CKS(prepare_join(c, pattern, queue));
+    const uint64_t n = c.n;
+    CKS(build_tasks(c, pattern, 0xffffffffULL));
+    const uint32_t nt = (uint32_t)c.tasks.size();
+    CK(c.dTasks.ensure(nt));
+    if (nt) CK(cudaMemcpyAsync(c.dTasks.p, c.tasks.data(), sizeof(sj_task) * nt, cudaMemcpyHostToDevice, c.s));
+    CK(c.keyCount.ensure(n));
+    CK(c.stat.ensure(8));
+    CK(c.queueHead.ensure(1));
+    CK(cudaMemsetAsync(c.keyCount.p, 0, sizeof(uint32_t) * n, c.s));
+    CK(cudaMemsetAsync(c.stat.p, 0, sizeof(unsigned long long) * 8, c.s));
+    sj_join_args a;
+    join_args_base(c, a);
+    a.tasks = c.dTasks.p;
+    a.queueHead = c.queueHead.p;
+    a.keyCount = c.keyCount.p;
+    a.stat = c.stat.p;
+    a.margin = filter_margin(c);
+    a.taskBegin = 0;
+    a.taskEnd = nt;
+    CKS(run_pass(c, a, false, true));
+    std::vector<uint32_t> deg(n);
+    CK(cudaMemcpyAsync(deg.data(), c.keyCount.p, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost, c.s));
+    std::vector<uint32_t> ids(n);
+    CK(cudaMemcpyAsync(ids.data(), c.ids.p, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost, c.s));
+    unsigned long long hs[8];
+    CK(cudaMemcpyAsync(hs, c.stat.p, sizeof(hs), cudaMemcpyDeviceToHost, c.s));
+    CK(cudaStreamSynchronize(c.s));
+    if (degHost) memcpy(degHost, deg.data(), sizeof(uint32_t) * n);
+    // per-cell measured hits (sum of the cell's points' degrees)
+    c.measCellHits.assign(c.nCells, 0.0);
+    for (uint32_t A = 0; A < c.nCells; A++) {
+        double s = 0;
+        for (uint32_t p = c.hCellStart[A]; p < c.hCellStart[A + 1]; p++) s += deg[ids[p]];
+        c.measCellHits[A] = s;
+    }
+    c.haveMeas = true;
+    uint64_t tot = 0;
+    for (uint64_t i = 0; i < n; i++) tot += deg[i];
+    c.st.total_pairs = tot;
+    c.st.distance_calcs = hs[0];
+    c.st.refined_pairs = hs[1];
+    return SJ_OK;
+}
+
+sj_status set_points(Ctx &c, const double *pts, uint64_t n, int onDevice)
+{
+    if (!pts && n) {
+        set_error("null points");
+        return SJ_ERR_BAD_INPUT;
+    }
+    if (n == 0 || n > 0x7fffffffULL) {
+        set_error("point count must be in 1..2^31-1 (got %llu)", (unsigned long long)n);
+        return SJ_ERR_BAD_INPUT;
+    }
+    Timer tm;
+    tm.start(c.s);
+    const size_t bytes = n * (size_t)c.p.gpunumdim * sizeof(double);
+    CK(c.pts.ensure(n * (size_t)c.p.gpunumdim));
+    CK(cudaMemcpyAsync(c.pts.p, pts, bytes, onDevice ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, c.s));
+    c.n = n;
+    c.havePoints = true;
+    c.indexed = false;
+    c.nbrPattern = -1;
+    c.st = sj_stats{};
+    c.st.ms_upload = tm.stop(c.s);
+    return SJ_OK;
+}
+
+Ctx *as_ctx(void *p) { return reinterpret_cast<Ctx *>(p); }
+
+sj_status bind(Ctx &c)
+{
+    CK(cudaSetDevice(c.dev));
+    return SJ_OK;
+}
+
+}  // namespace
+
+// =================================================================== C ABI
+extern "C" {
+
+void sj_params_default(sj_params *p)
+{
+    memset(p, 0, sizeof(*p));
+    p->gpunumdim = 2;
+    p->numindexeddim = 2;
+    p->epsilon = 0.01;
+    p->blocksize = 256;
+    p->threadperpoint = 1;
+    p->search_mode = 10;
+    p->sort_by_workload = 1;
+    p->precision = SJ_PREC_FP64;
+    p->scheduler = SJ_SCHED_SAMPLING;
+    p->batch_capacity_pairs = 0;
+    p->sample_rate = 0.01;
+    p->alpha = 0.05;
+    p->device = 0;
+    p->shard_index = 0;
+    p->shard_count = 1;
+    p->verbose = 0;
+}
+
+sj_status sj_create(const sj_params *p, void **out)
+{
+    if (!p || !out) {
+        set_error("null argument");
+        return SJ_ERR_BAD_INPUT;
+    }
+    *out = nullptr;
+    sj_status s = check_params(*p);
+    if (s != SJ_OK) return s;
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || ndev == 0) {
+        set_error("no CUDA device: %s", cudaGetErrorString(e));
+        return SJ_ERR_CUDA;
+    }
+    if (p->device < 0 || p->device >= ndev) {
+        set_error("device %d out of range (have %d)", p->device, ndev);
+        return SJ_ERR_BAD_INPUT;
+    }
+    Ctx *c = new Ctx();
+    c->p = *p;
+    c->dev = p->device;
+    e = cudaSetDevice(c->dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&c->numSM, cudaDevAttrMultiProcessorCount, c->dev);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->s, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        set_error("device setup: %s", cudaGetErrorString(e));
+        delete c;
+        return SJ_ERR_CUDA;
+    }
+    *out = c;
+    return SJ_OK;
+}
+
+sj_status sj_destroy(void *ctx)
+{
+    if (!ctx) return SJ_OK;
+    Ctx *c = as_ctx(ctx);
+    cudaSetDevice(c->dev);
+    cudaStreamSynchronize(c->s);
+    cudaStream_t s = c->s;
+    delete c;
+    if (s) cudaStreamDestroy(s);
+    return SJ_OK;
+}
+
+sj_status sj_import_csv(void *ctx, const char *path)
+{
+    if (!ctx || !path) {
+        set_error("null argument");
+        return SJ_ERR_BAD_INPUT;
+    }
+    Ctx &c = *as_ctx(ctx);
+    CKS(bind(c));
+    std::vector<double> pts;
+    if (sj::import_csv(path, c.p.gpunumdim, pts) != 0) {
+        set_error("cannot read %s", path);
+        return SJ_ERR_IO;
+    }
+    if (pts.empty()) {
+        set_error("%s holds no complete %d-dimensional point", path, c.p.gpunumdim);
+        return SJ_ERR_BAD_INPUT;
+    }
+    return set_points(c, pts.data(), pts.size() / c.p.gpunumdim, 0);
+}
+
+sj_status sj_read_csv(const char *path, int gpunumdim, double *out, uint64_t cap, uint64_t *n)
+{
+    if (!path || !n || gpunumdim < 1 || gpunumdim > SJ_MAX_DIM) {
+        set_error("bad arguments");
+        return SJ_ERR_BAD_INPUT;
+    }
+    std::vector<double> pts;
+    if (sj::import_csv(path, gpunumdim, pts) != 0) {
+        set_error("cannot read %s", path);
+        return SJ_ERR_IO;
+    }
+    uint64_t m = pts.size() / (uint64_t)gpunumdim;
+    *n = m;
+    if (out) memcpy(out, pts.data(), sizeof(double) * (size_t)std::min(m, cap) * gpunumdim);
+    return SJ_OK;
+}
+
+sj_status sj_set_points(void *ctx, const double *pts, uint64_t n, int on_device)
+{
+    if (!ctx) {
+        set_error("null context");
+        return SJ_ERR_BAD_INPUT;
+    }
+    Ctx &c = *as_ctx(ctx);
+    CKS(bind(c));
+    return set_points(c, pts, n, on_device);
+}
+
+sj_status sj_build_index(void *ctx)
+{
+    if (!ctx) return SJ_ERR_BAD_INPUT;
+    Ctx &c = *as_ctx(ctx);
+    CKS(bind(c));
+    return build_index(c);
+}
+
+sj_status sj_index_sizes(void *ctx, uint32_t *n_nonempty, uint32_t *n_mask_elems, uint64_t *total_cells)
+{
+    if (!ctx) return SJ_ERR_BAD_INPUT;
+    Ctx &c = *as_ctx(ctx);
+    if (!c.indexed) {
+        set_error("index not built");
+        return SJ_ERR_STATE;
+    }
+    CKS(bind(c));
+    if (n_nonempty) *n_nonempty = c.nCells;
+    if (total_cells) *total_cells = c.st.total_cells;
+    if (n_mask_elems) {
+        std::vector<uint32_t> coord((size_t)c.nCells * c.g.k);
+        CK(cudaMemcpy(coord.data(), c.cellCoord.p, coord.size() * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+        uint32_t tot = 0;
+        for (int j = 0; j < c.g.k; j++) {
+            std::vector<uint32_t> v(c.nCells);
+            for (uint32_t i = 0; i < c.nCells; i++) v[i] = coord[(size_t)i * c.g.k + j];
+            std::sort(v.begin(), v.end());
+            tot += (uint32_t)(std::unique(v.begin(), v.end()) - v.begin());
+        }
+        *n_mask_elems = tot;
+    }
+    return SJ_OK;
+}
+
+sj_status sj_index_export(void *ctx, unsigned int *indexLookupArr, sj_grid *grid, sj_grid_cell_lookup *lookup,
+                          double *minArr, unsigned int *nCells, unsigned int *mask, unsigned int *maskOffsets)
+{
+    if (!ctx) return SJ_ERR_BAD_INPUT;
+    Ctx &c = *as_ctx(ctx);
+    if (!c.indexed) {
+        set_error("index not built");
+        return SJ_ERR_STATE;
+    }
+    CKS(bind(c));
+    const uint32_t nc = c.nCells;
+    if (indexLookupArr) CK(cudaMemcpy(indexLookupArr, c.ids.p, sizeof(uint32_t) * c.n, cudaMemcpyDeviceToHost));
+    if (grid)
+        for (uint32_t i = 0; i < nc; i++) {
+            grid[i].indexmin = (int)c.hCellStart[i];
+            grid[i].indexmax = (int)c.hCellStart[i + 1] - 1;
+        }
+    if (lookup) {
+        std::vector<uint64_t> lid(nc);
+        CK(cudaMemcpy(lid.data(), c.cellLid.p, sizeof(uint64_t) * nc, cudaMemcpyDeviceToHost));
+        for (uint32_t i = 0; i < nc; i++) {
+            lookup[i].idx = i;
+            lookup[i].gridLinearID = lid[i];
+        }
+    }
+    for (int j = 0; j < c.g.k; j++) {
+        if (minArr) minArr[j] = c.g.minArr[j];
+        if (nCells) nCells[j] = c.g.nCells[j];
+    }
+    if (mask || maskOffsets) {
+        std::vector<uint32_t> coord((size_t)nc * c.g.k);
+        CK(cudaMemcpy(coord.data(), c.cellCoord.p, coord.size() * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+        uint32_t off = 0;
+        for (int j = 0; j < c.g.k; j++) {
+            std::vector<uint32_t> v(nc);
+            for (uint32_t i = 0; i < nc; i++) v[i] = coord[(size_t)i * c.g.k + j];
+            std::sort(v.begin(), v.end());
+            v.erase(std::unique(v.begin(), v.end()), v.end());
+            if (maskOffsets) maskOffsets[2 * j] = off;
+            for (uint32_t x : v) {
+                if (mask) mask[off] = x;
+                off++;
+            }
+            if (maskOffsets) maskOffsets[2 * j + 1] = off - 1;
+        }
+    }
+    return SJ_OK;
+}
+
+sj_status sj_join(void *ctx, int delivery, sj_batch_cb cb, void *user)
+{
+    if (!ctx) return SJ_ERR_BAD_INPUT;
+    if (delivery < SJ_DELIVER_DEVICE || delivery > SJ_DELIVER_NONE) {
+        set_error("unknown delivery mode");
+        return SJ_ERR_BAD_INPUT;
+    }
+    Ctx &c = *as_ctx(ctx);
+    CKS(bind(c));
+    return run_join(c, delivery, cb, user);
+}
+
+sj_status sj_degrees(void *ctx, uint32_t *deg)
+{
+    if (!ctx) return SJ_ERR_BAD_INPUT;
+    Ctx &c = *as_ctx(ctx);
+    CKS(bind(c));
+    return run_degrees(c, deg);
+}
+
+struct TableBuild {
+    std::vector<uint32_t> *deg;
+    std::vector<uint64_t> *cursor;
+    int *values;
+};
+
+static int table_cb(const sj_batch *b, void *user)
+{
+    TableBuild *t = (TableBuild *)user;
+    for (uint64_t i = 0; i < b->count; i++) {
+        uint32_t k = (uint32_t)b->key[i];
+        t->values[(*t->cursor)[k]++] = b->val[i];
+    }
+    return 0;
+}
+
+sj_status sj_neighbor_table(void *ctx, sj_neighbor_table_lookup *table, int **values, uint64_t *total)
+{
+    if (!ctx || !table || !values) return SJ_ERR_BAD_INPUT;
+    Ctx &c = *as_ctx(ctx);
+    CKS(bind(c));
+    std::vector<uint32_t> deg(c.n);
+    CKS(run_degrees(c, deg.data()));
+    uint64_t tot = 0;
+    std::vector<uint64_t> start(c.n), cursor(c.n);
+    for (uint64_t i = 0; i < c.n; i++) {
+        start[i] = tot;
+        tot += deg[i];
+    }
+    if (tot > 0x7fffffffULL) {
+        set_error("neighbour table of %llu values exceeds int indexing", (unsigned long long)tot);
+        return SJ_ERR_BAD_INPUT;
+    }
+    int *vals = (int *)malloc(sizeof(int) * (tot ? tot : 1));
+    if (!vals) return SJ_ERR_OOM;
+    cursor = start;
+    TableBuild tb{&deg, &cursor, vals};
+    sj_status s = run_join(c, SJ_DELIVER_HOST, table_cb, &tb);
+    if (s != SJ_OK) {
+        free(vals);
+        return s;
+    }
+    for (uint64_t i = 0; i < c.n; i++) {
+        if (cursor[i] != start[i] + deg[i]) {
+            free(vals);
+            set_error("internal: neighbour table row %llu incomplete", (unsigned long long)i);
+            return SJ_ERR_INTERNAL;
+        }
+        table[i].pointID = (int)i;
+        table[i].indexmin = (int)start[i];
+        table[i].indexmax = (int)(start[i] + deg[i]) - 1;
+        table[i].dataPtr = vals;
+    }
+    *values = vals;
+    if (total) *total = tot;
+    return SJ_OK;
+}
+
+void sj_free(void *p) { free(p); }
+
+sj_status sj_get_stats(void *ctx, sj_stats *st)
+{
+    if (!ctx || !st) return SJ_ERR_BAD_INPUT;
+    *st = as_ctx(ctx)->st;
+    return SJ_OK;
+}
+
+uint32_t sj_mlp_num_params(void) { return SJ_MLP_NPARAM; }
+
+sj_status sj_set_estimator_weights(void *ctx, const float *w, uint32_t count)
+{
+    if (!ctx || !w || count != SJ_MLP_NPARAM) {
+        set_error("estimator weights: expected %d floats", SJ_MLP_NPARAM);
+        return SJ_ERR_BAD_INPUT;
+    }
+    Ctx &c = *as_ctx(ctx);
+    c.mlpW.assign(w, w + count);
+    return SJ_OK;
+}
+
+sj_status sj_load_estimator(void *ctx, const char *path)
+{
+    if (!ctx || !path) return SJ_ERR_BAD_INPUT;
+    FILE *f = fopen(path, "rb");
+    if (!f) {
+        set_error("cannot open %s", path);
+        return SJ_ERR_IO;
+    }
+    std::vector<float> w(SJ_MLP_NPARAM);
+    size_t r = fread(w.data(), sizeof(float), w.size(), f);
+    fclose(f);
+    if (r != w.size()) {
+        set_error("%s: expected %d floats", path, SJ_MLP_NPARAM);
+        return SJ_ERR_BAD_INPUT;
+    }
+    return sj_set_estimator_weights(ctx, w.data(), (uint32_t)w.size());
+}
+
+sj_status sj_cell_features(void *ctx, float *feat, double *hits, double *calcs)
+{
+    if (!ctx) return SJ_ERR_BAD_INPUT;
+    Ctx &c = *as_ctx(ctx);
+    if (!c.indexed) {
+        set_error("index not built");
+        return SJ_ERR_STATE;
+    }
+    CKS(bind(c));
+    if (c.nbrPattern < 0) CKS(build_neighbours(c, pattern_of_mode(c.p.search_mode)));
+    if (feat)
+        CK(cudaMemcpy(feat, c.feat.p, sizeof(float) * (size_t)c.nCells * SJ_NFEAT, cudaMemcpyDeviceToHost));
+    if (calcs)
+        for (uint32_t i = 0; i < c.nCells; i++) calcs[i] = (double)c.hCandFull[i];
+    if (hits) {
+        if (!c.haveMeas) {
+            set_error("no measured counts: run sj_degrees first");
+            return SJ_ERR_STATE;
+        }
+        for (uint32_t i = 0; i < c.nCells; i++) hits[i] = c.measCellHits[i];
+    }
+    return SJ_OK;
+}
+
+static sj_status mlp_common(int device, uint32_t m, const float *x, const float *y, DevBuf<float> &dx,
+                            DevBuf<float> &dy, cudaStream_t s)
+{
+    CK(cudaSetDevice(device));
+    CK(dx.ensure((size_t)m * SJ_NFEAT));
+    CK(cudaMemcpyAsync(dx.p, x, sizeof(float) * (size_t)m * SJ_NFEAT, cudaMemcpyHostToDevice, s));
+    if (y) {
+        CK(dy.ensure((size_t)m * SJ_NOUT));
+        CK(cudaMemcpyAsync(dy.p, y, sizeof(float) * (size_t)m * SJ_NOUT, cudaMemcpyHostToDevice, s));
+    }
+    return SJ_OK;
+}
+
+sj_status sj_mlp_loss_grad(const float *x, const float *y, uint32_t m, const float *w, float *loss, float *grad,
+                           int device)
+{
+    if (!x || !y || !w || !grad || m == 0) return SJ_ERR_BAD_INPUT;
+    DevBuf<float> dx, dy, dw, dg, dl;
+    cudaStream_t s = 0;
+    CKS(mlp_common(device, m, x, y, dx, dy, s));
+    CK(dw.ensure(SJ_MLP_NPARAM));
+    CK(dg.ensure(SJ_MLP_NPARAM));
+    CK(dl.ensure(1));
+    CK(cudaMemcpy(dw.p, w, sizeof(float) * SJ_MLP_NPARAM, cudaMemcpyHostToDevice));
+    CK(sj_launch_mlp_grad(dx.p, dy.p, m, dw.p, dg.p, dl.p, s));
+    CK(cudaMemcpy(grad, dg.p, sizeof(float) * SJ_MLP_NPARAM, cudaMemcpyDeviceToHost));
+    float l;
+    CK(cudaMemcpy(&l, dl.p, sizeof(float), cudaMemcpyDeviceToHost));
+    if (loss) *loss = l;
+    return SJ_OK;
+}
+
+sj_status sj_mlp_forward(const float *x, uint32_t m, const float *w, float *out, int device)
+{
+    if (!x || !w || !out || m == 0) return SJ_ERR_BAD_INPUT;
+    DevBuf<float> dx, dy, dw, dout;
+    cudaStream_t s = 0;
+    CKS(mlp_common(device, m, x, nullptr, dx, dy, s));
+    CK(dw.ensure(SJ_MLP_NPARAM));
+    CK(dout.ensure((size_t)m * SJ_NOUT));
+    CK(cudaMemcpy(dw.p, w, sizeof(float) * SJ_MLP_NPARAM, cudaMemcpyHostToDevice));
+    CK(sj_launch_mlp_infer(dx.p, m, dw.p, dout.p, s));
+    CK(cudaMemcpy(out, dout.p, sizeof(float) * (size_t)m * SJ_NOUT, cudaMemcpyDeviceToHost));
+    return SJ_OK;
+}
+
+sj_status sj_mlp_train(const float *x, const float *y, uint32_t m, float *w, int steps, float lr, uint32_t batch,
+                       uint64_t seed, float *final_loss, int device)
+{
+    if (!x || !y || !w || m == 0 || steps < 1 || batch == 0) return SJ_ERR_BAD_INPUT;
+    if (batch > m) batch = m;
+    DevBuf<float> dx, dy, dw, dg, dm, dv, dl, bx, by;
+    cudaStream_t s = 0;
+    CKS(mlp_common(device, m, x, y, dx, dy, s));
+    CK(dw.ensure(SJ_MLP_NPARAM));
+    CK(dg.ensure(SJ_MLP_NPARAM));
+    CK(dm.ensure(SJ_MLP_NPARAM));
+    CK(dv.ensure(SJ_MLP_NPARAM));
+    CK(dl.ensure(1));
+    CK(bx.ensure((size_t)batch * SJ_NFEAT));
+    CK(by.ensure((size_t)batch * SJ_NOUT));
+    CK(cudaMemcpy(dw.p, w, sizeof(float) * SJ_MLP_NPARAM, cudaMemcpyHostToDevice));
+    CK(cudaMemset(dm.p, 0, sizeof(float) * SJ_MLP_NPARAM));
+    CK(cudaMemset(dv.p, 0, sizeof(float) * SJ_MLP_NPARAM));
+    // minibatches: contiguous windows of a host-side shuffled copy
+    std::vector<uint32_t> perm(m);
+    std::iota(perm.begin(), perm.end(), 0u);
+    uint64_t st = seed ? seed : 0x9e3779b97f4a7c15ULL;
+    auto rnd = [&st]() {
+        st ^= st << 13;
+        st ^= st >> 7;
+        st ^= st << 17;
+        return st;
+    };
+    for (uint32_t i = m - 1; i > 0; i--) std::swap(perm[i], perm[rnd() % (i + 1)]);
+    std::vector<float> sx((size_t)m * SJ_NFEAT), sy((size_t)m * SJ_NOUT);
+    for (uint32_t i = 0; i < m; i++) {
+        memcpy(&sx[(size_t)i * SJ_NFEAT], &x[(size_t)perm[i] * SJ_NFEAT], sizeof(float) * SJ_NFEAT);
+        memcpy(&sy[(size_t)i * SJ_NOUT], &y[(size_t)perm[i] * SJ_NOUT], sizeof(float) * SJ_NOUT);
+    }
+    CK(cudaMemcpy(dx.p, sx.data(), sizeof(float) * sx.size(), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(dy.p, sy.data(), sizeof(float) * sy.size(), cudaMemcpyHostToDevice));
+    uint32_t nbat = m / batch;
+    for (int step = 1; step <= steps; step++) {
+        uint32_t b = (uint32_t)((step - 1) % nbat);
+        const float *px = dx.p + (size_t)b * batch * SJ_NFEAT;
+        const float *py = dy.p + (size_t)b * batch * SJ_NOUT;
+        CK(sj_launch_mlp_train_step(px, py, batch, dw.p, dg.p, dm.p, dv.p, step, lr, dl.p, s));
+    }
+    CK(sj_launch_mlp_grad(dx.p, dy.p, m, dw.p, dg.p, dl.p, s));
+    float l;
+    CK(cudaMemcpy(&l, dl.p, sizeof(float), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(w, dw.p, sizeof(float) * SJ_MLP_NPARAM, cudaMemcpyDeviceToHost));
+    if (final_loss) *final_loss = l;
+    return SJ_OK;
+}
+
+const char *sj_status_string(sj_status s)
+{
+    switch (s) {
+    case SJ_OK: return "ok";
+    case SJ_ERR_OOM: return "out of memory";
+    case SJ_OVERFLOW_RETRIED: return "overflow retried";
+    case SJ_ERR_BAD_INPUT: return "bad input";
+    case SJ_ERR_CUDA: return "CUDA error";
+    case SJ_ERR_TIMEOUT: return "timeout";
+    case SJ_ERR_STATE: return "call out of order";
+    case SJ_ERR_IO: return "I/O error";
+    case SJ_ERR_ABORTED: return "aborted by consumer";
+    case SJ_ERR_INTERNAL: return "internal error";
+    }
+    return "unknown";
+}
+
+const char *sj_last_error(void) { return g_lastError.c_str(); }
+
+const char *sj_version(void) { return "sj-b200 0.1 (sm_100a)"; }
+
+}  // extern "C"

@@ -1,0 +1,245 @@
+// Result-size estimators that size the result batches and order the work.
+//
+// Sampling estimator: the reference counts the full-stencil hits of every
+// 100th point (kernelNDGridIndexBatchEstimatorOLD, kernel.cu:602-781;
+// GPU.cu:854-1065) and scales the total.  Here the sampled points also give a
+// per-cell hit rate (hits per candidate evaluation over the cell's own
+// candidate stream), which the planner multiplies by each task's exact
+// evaluation count.
+//
+// Learned estimator: a 16 -> 64 -> 64 -> 2 ReLU MLP on per-cell features
+// predicts log2(1 + distance calcs) and log2(1 + hits) of a cell.  Forward,
+// backward and Adam are plain FP32 CUDA-core kernels (the network is tiny).
+#include "sj_internal.h"
+
+namespace {
+
+// One warp per sampled query position; lanes stride over the candidate stream
+// (whole home cell + owned neighbour cells).
+__global__ void __launch_bounds__(256) k_sample(sj_join_args a, sj_grid_dev g, uint32_t stride, uint32_t nPoints,
+                                                uint32_t nCells, unsigned long long *cellHits,
+                                                unsigned long long *cellCands)
+{
+    uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    uint32_t lane = threadIdx.x & 31u;
+    uint64_t pos = (uint64_t)gw * stride;
+    if (pos >= nPoints) return;
+    // cell of this position: largest c with cellStart[c] <= pos
+    uint32_t lo = 0, hi = nCells;
+    while (hi - lo > 1) {
+        uint32_t mid = (lo + hi) >> 1;
+        if (a.cellStart[mid] <= pos) lo = mid; else hi = mid;
+    }
+    const uint32_t A = lo;
+    double q[SJ_MAX_DIM];
+    for (int l = 0; l < g.Dp; l++) q[l] = a.xs[pos * g.Dp + l];
+    unsigned long long hits = 0, cands = 0;
+    uint32_t nn = a.nbrStart[A + 1] - a.nbrStart[A];
+    for (uint32_t s = 0; s <= nn; s++) {
+        uint32_t B = (s == 0) ? A : a.nbrCell[a.nbrStart[A] + s - 1];
+        uint32_t b0 = a.cellStart[B], b1 = a.cellStart[B + 1];
+        for (uint32_t c = b0 + lane; c < b1; c += 32) {
+            const double *x = a.xs + (uint64_t)c * g.Dp;
+            double acc = 0.0;
+            for (int l = 0; l < g.Dp; l++) {
+                double d = __dsub_rn(x[l], q[l]);
+                acc = __fma_rn(d, d, acc);
+            }
+            hits += (acc <= g.thresh);
+        }
+        cands += (b1 - b0);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) hits += __shfl_xor_sync(0xffffffffu, hits, o);
+    if (lane == 0) {
+        atomicAdd(&cellHits[A], hits);
+        atomicAdd(&cellCands[A], cands);
+    }
+}
+
+// ------------------------------------------------------------------ MLP ----
+// parameter offsets
+constexpr int OW1 = 0;
+constexpr int OB1 = OW1 + SJ_NFEAT * SJ_HID;
+constexpr int OW2 = OB1 + SJ_HID;
+constexpr int OB2 = OW2 + SJ_HID * SJ_HID;
+constexpr int OW3 = OB2 + SJ_HID;
+constexpr int OB3 = OW3 + SJ_HID * SJ_NOUT;
+constexpr int NP = OB3 + SJ_NOUT;
+static_assert(NP == SJ_MLP_NPARAM, "parameter layout");
+
+__device__ __forceinline__ void mlp_forward(const float *__restrict__ w, const float *x, float *z1, float *z2,
+                                            float *y)
+{
+    for (int j = 0; j < SJ_HID; j++) {
+        float s = w[OB1 + j];
+#pragma unroll
+        for (int i = 0; i < SJ_NFEAT; i++) s = fmaf(x[i], w[OW1 + i * SJ_HID + j], s);
+        z1[j] = s;
+    }
+    for (int j = 0; j < SJ_HID; j++) {
+        float s = w[OB2 + j];
+        for (int i = 0; i < SJ_HID; i++) s = fmaf(fmaxf(z1[i], 0.f), w[OW2 + i * SJ_HID + j], s);
+        z2[j] = s;
+    }
+#pragma unroll
+    for (int o = 0; o < SJ_NOUT; o++) {
+        float s = w[OB3 + o];
+        for (int i = 0; i < SJ_HID; i++) s = fmaf(fmaxf(z2[i], 0.f), w[OW3 + i * SJ_NOUT + o], s);
+        y[o] = s;
+    }
+}
+
+__global__ void __launch_bounds__(128) k_mlp_infer(const float *__restrict__ feat, uint32_t m,
+                                                   const float *__restrict__ wg, float *__restrict__ out)
+{
+    __shared__ float w[NP];
+    for (int i = threadIdx.x; i < NP; i += blockDim.x) w[i] = wg[i];
+    __syncthreads();
+    uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= m) return;
+    float x[SJ_NFEAT], z1[SJ_HID], z2[SJ_HID], y[SJ_NOUT];
+    for (int i = 0; i < SJ_NFEAT; i++) x[i] = feat[(uint64_t)s * SJ_NFEAT + i];
+    mlp_forward(w, x, z1, z2, y);
+    for (int o = 0; o < SJ_NOUT; o++) out[(uint64_t)s * SJ_NOUT + o] = y[o];
+}
+
+// Per-sample forward + backward.  Loss = 1/(2m) * sum (y - t)^2.  Writes the
+// activations and pre-activation gradients the weight gradients need.
+__global__ void __launch_bounds__(128) k_mlp_backprop(const float *__restrict__ X, const float *__restrict__ Yt,
+                                                      uint32_t m, const float *__restrict__ wg,
+                                                      float *__restrict__ H1, float *__restrict__ G1,
+                                                      float *__restrict__ H2, float *__restrict__ G2,
+                                                      float *__restrict__ G3, float *__restrict__ loss)
+{
+    __shared__ float w[NP];
+    for (int i = threadIdx.x; i < NP; i += blockDim.x) w[i] = wg[i];
+    __syncthreads();
+    uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    float l = 0.f;
+    if (s < m) {
+        float x[SJ_NFEAT], z1[SJ_HID], z2[SJ_HID], y[SJ_NOUT], dy[SJ_NOUT], d2[SJ_HID];
+        for (int i = 0; i < SJ_NFEAT; i++) x[i] = X[(uint64_t)s * SJ_NFEAT + i];
+        mlp_forward(w, x, z1, z2, y);
+        const float inv = 1.0f / (float)m;
+        for (int o = 0; o < SJ_NOUT; o++) {
+            float e = y[o] - Yt[(uint64_t)s * SJ_NOUT + o];
+            l += 0.5f * e * e;
+            dy[o] = e * inv;
+            G3[(uint64_t)s * SJ_NOUT + o] = dy[o];
+        }
+        for (int i = 0; i < SJ_HID; i++) {
+            float g = 0.f;
+#pragma unroll
+            for (int o = 0; o < SJ_NOUT; o++) g = fmaf(dy[o], w[OW3 + i * SJ_NOUT + o], g);
+            d2[i] = z2[i] > 0.f ? g : 0.f;
+            H2[(uint64_t)s * SJ_HID + i] = fmaxf(z2[i], 0.f);
+            G2[(uint64_t)s * SJ_HID + i] = d2[i];
+        }
+        for (int i = 0; i < SJ_HID; i++) {
+            float g = 0.f;
+            for (int j = 0; j < SJ_HID; j++) g = fmaf(d2[j], w[OW2 + i * SJ_HID + j], g);
+            H1[(uint64_t)s * SJ_HID + i] = fmaxf(z1[i], 0.f);
+            G1[(uint64_t)s * SJ_HID + i] = z1[i] > 0.f ? g : 0.f;
+        }
+    }
+    // loss reduction
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) l += __shfl_xor_sync(0xffffffffu, l, o);
+    if ((threadIdx.x & 31) == 0 && l != 0.f) atomicAdd(loss, l / (float)m);
+}
+
+// grad[param] = sum over samples of (input activation) x (output gradient);
+// one thread per parameter.  Inputs: X (m x 16), H1, H2 (m x 64);
+// gradients: G1, G2 (m x 64), G3 (m x 2).
+__global__ void __launch_bounds__(256) k_mlp_wgrad(const float *__restrict__ X, const float *__restrict__ H1,
+                                                   const float *__restrict__ H2, const float *__restrict__ G1,
+                                                   const float *__restrict__ G2, const float *__restrict__ G3,
+                                                   uint32_t m, float *__restrict__ grad)
+{
+    int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= NP) return;
+    const float *A = nullptr, *G = nullptr;
+    int ai = -1, gj, aw = 0, gw;
+    if (p < OB1) { A = X; aw = SJ_NFEAT; ai = (p - OW1) / SJ_HID; G = G1; gw = SJ_HID; gj = (p - OW1) % SJ_HID; }
+    else if (p < OW2) { G = G1; gw = SJ_HID; gj = p - OB1; }
+    else if (p < OB2) { A = H1; aw = SJ_HID; ai = (p - OW2) / SJ_HID; G = G2; gw = SJ_HID; gj = (p - OW2) % SJ_HID; }
+    else if (p < OW3) { G = G2; gw = SJ_HID; gj = p - OB2; }
+    else if (p < OB3) { A = H2; aw = SJ_HID; ai = (p - OW3) / SJ_NOUT; G = G3; gw = SJ_NOUT; gj = (p - OW3) % SJ_NOUT; }
+    else { G = G3; gw = SJ_NOUT; gj = p - OB3; }
+    float s = 0.f;
+    for (uint32_t k = 0; k < m; k++) {
+        float av = (ai >= 0) ? A[(uint64_t)k * aw + ai] : 1.0f;
+        s = fmaf(av, G[(uint64_t)k * gw + gj], s);
+    }
+    grad[p] = s;
+}
+
+__global__ void k_adam(float *__restrict__ w, const float *__restrict__ g, float *__restrict__ mm,
+                       float *__restrict__ vv, int step, float lr)
+{
+    int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= NP) return;
+    const float b1 = 0.9f, b2 = 0.999f, e = 1e-8f;
+    float m = b1 * mm[p] + (1.f - b1) * g[p];
+    float v = b2 * vv[p] + (1.f - b2) * g[p] * g[p];
+    mm[p] = m;
+    vv[p] = v;
+    float mh = m / (1.f - powf(b1, (float)step));
+    float vh = v / (1.f - powf(b2, (float)step));
+    w[p] -= lr * mh / (sqrtf(vh) + e);
+}
+
+}  // namespace
+
+cudaError_t sj_launch_sample(const sj_join_args &a, const sj_grid_dev &g, uint32_t sampleStride,
+                             unsigned long long *cellHits, unsigned long long *cellCands, uint32_t nCells,
+                             cudaStream_t s)
+{
+    uint32_t nPoints = a.taskEnd;   // caller passes n here
+    uint64_t nSamples = (nPoints + (uint64_t)sampleStride - 1) / sampleStride;
+    if (nSamples == 0) return cudaSuccess;
+    uint64_t blocks = (nSamples * 32 + 255) / 256;
+    k_sample<<<(unsigned)blocks, 256, 0, s>>>(a, g, sampleStride, nPoints, nCells, cellHits, cellCands);
+    return cudaGetLastError();
+}
+
+cudaError_t sj_launch_mlp_infer(const float *feat, uint32_t nCells, const float *weights, float *out, cudaStream_t s)
+{
+    if (nCells == 0) return cudaSuccess;
+    k_mlp_infer<<<(nCells + 127) / 128, 128, 0, s>>>(feat, nCells, weights, out);
+    return cudaGetLastError();
+}
+
+// Scratch for one training/gradient call: H1, G1, H2, G2 (m x 64 each), G3 (m x 2).
+static cudaError_t mlp_grad_impl(const float *x, const float *y, uint32_t m, const float *w, float *grad,
+                                 float *lossOut, cudaStream_t s)
+{
+    float *buf = nullptr;
+    size_t per = (size_t)m * (4 * SJ_HID + SJ_NOUT);
+    cudaError_t e = cudaMallocAsync((void **)&buf, per * sizeof(float), s);
+    if (e != cudaSuccess) return e;
+    float *H1 = buf, *G1 = H1 + (size_t)m * SJ_HID, *H2 = G1 + (size_t)m * SJ_HID, *G2 = H2 + (size_t)m * SJ_HID,
+          *G3 = G2 + (size_t)m * SJ_HID;
+    cudaMemsetAsync(lossOut, 0, sizeof(float), s);
+    k_mlp_backprop<<<(m + 127) / 128, 128, 0, s>>>(x, y, m, w, H1, G1, H2, G2, G3, lossOut);
+    k_mlp_wgrad<<<(NP + 255) / 256, 256, 0, s>>>(x, H1, H2, G1, G2, G3, m, grad);
+    e = cudaGetLastError();
+    cudaFreeAsync(buf, s);
+    return e;
+}
+
+cudaError_t sj_launch_mlp_grad(const float *x, const float *y, uint32_t m, const float *weights, float *grad,
+                               float *lossOut, cudaStream_t s)
+{
+    return mlp_grad_impl(x, y, m, weights, grad, lossOut, s);
+}
+
+cudaError_t sj_launch_mlp_train_step(const float *x, const float *y, uint32_t m, float *weights, float *grad,
+                                     float *adamM, float *adamV, int step, float lr, float *lossOut, cudaStream_t s)
+{
+    cudaError_t e = mlp_grad_impl(x, y, m, weights, grad, lossOut, s);
+    if (e != cudaSuccess) return e;
+    k_adam<<<(NP + 255) / 256, 256, 0, s>>>(weights, grad, adamM, adamV, step, lr);
+    return cudaGetLastError();
+}

@@ -1,0 +1,120 @@
+// Internal declarations shared by the engine's host code and its CUDA kernels.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stddef.h>
+
+#include "sj.h"
+
+#define SJ_MAX_DIM 16        // data dimensions handled by the kernels (padded to a template width)
+#define SJ_MAX_K 16          // indexed dimensions
+#define SJ_CTA 128           // threads per join CTA (one query point per thread)
+#define SJ_STAGE 256         // candidates staged in shared memory per step
+#define SJ_MAX_SEG 1024      // candidate segments (home + neighbour cells) per task
+#define SJ_NFEAT 16          // learned-estimator input features per cell
+#define SJ_HID 64            // learned-estimator hidden width
+#define SJ_NOUT 2            // learned-estimator outputs (log distance calcs, log hits)
+
+// Traversal (neighbour ownership) patterns, mapped from the reference's search modes.
+enum sj_pattern { SJ_PAT_FULL = 0, SJ_PAT_UNICOMP = 1, SJ_PAT_BUNICOMP = 2, SJ_PAT_LID = 3 };
+
+// Grid geometry, passed by value to kernels.
+struct sj_grid_dev {
+    int D;            // data dimensions
+    int Dp;           // padded stride of the cell-sorted coordinate array
+    int k;            // indexed dimensions
+    double eps;
+    double thresh;    // largest T with sqrt(T) <= eps (FP64 round-to-nearest)
+    double minArr[SJ_MAX_K];
+    unsigned nCells[SJ_MAX_K];
+    unsigned long long mult[SJ_MAX_K];
+    double center[SJ_MAX_DIM];  // origin used for non-indexed dimensions in the FP32 filter
+};
+
+// One unit of join work: query points [qBegin, qBegin+qCount) of cell `cell`
+// (cell-sorted positions) against stream positions [sBegin, sEnd) of the
+// concatenation of segments segBase..segBase+segCount-1 of that cell's
+// candidate list (segment 0 is the home cell, the rest are owned neighbours).
+struct sj_task {
+    uint32_t cell;
+    uint32_t qBegin;
+    uint32_t qCount;
+    uint32_t segBase;
+    uint32_t segCount;
+    uint32_t sBegin;
+    uint32_t sEnd;
+    uint32_t flags;   // bit0: symmetric emission, bit1: home segment included
+};
+
+#define SJ_TASK_SYM 1u
+#define SJ_TASK_HOME 2u
+
+// Device-side state of one join (all pointers device memory).
+struct sj_join_args {
+    const double *xs;           // n x Dp cell-sorted coordinates (FP64)
+    const uint32_t *ids;        // n point ids in cell-sorted order (indexLookupArr)
+    const uint32_t *cellStart;  // nCells+1
+    const uint32_t *nbrStart;   // nCells+1 (owned neighbour list, excludes home)
+    const uint32_t *nbrCell;
+    const uint32_t *cellCoord;  // nCells x k
+    const sj_task *tasks;
+    uint32_t taskBegin, taskEnd;
+    uint32_t *queueHead;        // persistent-queue cursor (work-queue modes)
+    uint32_t *keyCount;         // count pass: per point-id pair counts
+    uint32_t *keyCursor;        // fill pass: per point-id write cursors (exclusive offsets)
+    int32_t *outKey, *outVal;   // fill pass output
+    uint64_t capacity;          // pairs the output buffers hold
+    unsigned long long *stat;   // [0] evals, [1] refined, [2] hits(count pass), [3] overflow flag
+    uint32_t *taskHits;         // optional per-task measured pairs (count pass)
+    double margin;              // FP32 filter half-band on the squared distance
+};
+
+// ---------------------------------------------------------------- launchers
+// primitives (sj_prims.cu)
+size_t sj_scan_temp_bytes(uint64_t n);
+cudaError_t sj_exclusive_scan_u32(const uint32_t *in, uint32_t *out, uint64_t n, void *temp,
+                                  uint32_t *total_dev, cudaStream_t s);
+size_t sj_radix_temp_bytes(uint64_t n);
+cudaError_t sj_radix_sort_u64_u32(uint64_t *keys, uint32_t *vals, uint64_t *keysAlt, uint32_t *valsAlt,
+                                  uint64_t n, int bits, void *temp, int *resultInAlt, cudaStream_t s);
+cudaError_t sj_radix_sort_u32_u32(uint32_t *keys, uint32_t *vals, uint32_t *keysAlt, uint32_t *valsAlt,
+                                  uint64_t n, int bits, void *temp, int *resultInAlt, cudaStream_t s);
+cudaError_t sj_hash_pairs(const int32_t *key, const int32_t *val, uint64_t m,
+                          unsigned long long *hashOut, cudaStream_t s);
+
+// index build (sj_index.cu)
+cudaError_t sj_launch_minmax(const double *pts, uint64_t n, int D, double *minmax_dev, cudaStream_t s);
+cudaError_t sj_launch_cell_keys(const double *pts, uint64_t n, sj_grid_dev g, uint64_t *keys, uint32_t *vals,
+                                cudaStream_t s);
+cudaError_t sj_launch_cell_flags(const uint64_t *keys, uint64_t n, uint32_t *flags, cudaStream_t s);
+cudaError_t sj_launch_cell_build(const uint64_t *keys, const uint32_t *cellIdxExcl, uint64_t n,
+                                 uint32_t *cellStart, uint64_t *cellLid, cudaStream_t s);
+cudaError_t sj_launch_gather(const double *pts, const uint32_t *ids, uint64_t n, int D, int Dp, double *xs,
+                             cudaStream_t s);
+cudaError_t sj_launch_cell_coords(const uint64_t *cellLid, uint32_t nCells, sj_grid_dev g, uint32_t *coord,
+                                  cudaStream_t s);
+
+// neighbour lists and features (sj_stencil.cu)
+cudaError_t sj_launch_neighbours(const uint64_t *cellLid, const uint32_t *cellCoord, const uint32_t *cellStart,
+                                 uint32_t nCells, sj_grid_dev g, int pattern, const uint32_t *nbrStart,
+                                 uint32_t *nbrCountOrCell, uint64_t *candFull, float *feat, int pass,
+                                 cudaStream_t s);
+
+// join (sj_join.cu)
+cudaError_t sj_launch_join(const sj_join_args &a, const sj_grid_dev &g, int fill, int fp32, int queue,
+                           int numSM, cudaStream_t s);
+
+// estimators (sj_estimate.cu)
+cudaError_t sj_launch_sample(const sj_join_args &a, const sj_grid_dev &g, uint32_t sampleStride,
+                             unsigned long long *cellHits, unsigned long long *cellCands, uint32_t nCells,
+                             cudaStream_t s);
+cudaError_t sj_launch_mlp_infer(const float *feat, uint32_t nCells, const float *weights, float *out,
+                                cudaStream_t s);
+cudaError_t sj_launch_mlp_train_step(const float *x, const float *y, uint32_t m, float *weights, float *grad,
+                                     float *adamM, float *adamV, int step, float lr, float *lossOut,
+                                     cudaStream_t s);
+cudaError_t sj_launch_mlp_grad(const float *x, const float *y, uint32_t m, const float *weights, float *grad,
+                               float *lossOut, cudaStream_t s);
+
+// number of learned-estimator parameters (W1,b1,W2,b2,W3,b3)
+#define SJ_MLP_NPARAM (SJ_NFEAT * SJ_HID + SJ_HID + SJ_HID * SJ_HID + SJ_HID + SJ_HID * SJ_NOUT + SJ_NOUT)

@@ -1,0 +1,416 @@
+// The distance join: count pass and fill pass over cell tasks.
+//
+// One CTA of 128 threads takes a task: up to 128 query points of one cell
+// (one per thread, coordinates in registers) against a stretch of that cell's
+// candidate stream (home cell + owned neighbour cells, kernel.cu:1403-1538 in
+// the reference).  Candidates are staged in shared memory in steps of
+// SJ_STAGE and read by every thread as broadcasts.  Each thread builds a
+// 32-bit hit mask per block of 32 candidates; a 5-step butterfly transposes the
+// warp's 32x32 mask so that lane L holds candidate L's hits for the mirrored
+// direction (symmetric traversals emit (p,q) and (q,p) from one evaluation).
+//
+// count pass: per-key pair counts (the row lengths of this batch).
+// fill pass : keys are placed at exclusive offsets of those counts, so every
+//             key's values land contiguously and keys come out ascending --
+//             the order thrust::sort_by_key gives the reference (GPU.cu:2336)
+//             without sorting.
+//
+// Predicate (kernel.cu:344-349): acc = sum over dims of fma(d,d,acc) with
+// d = cand - query, hit iff sqrt(acc) <= eps, evaluated as acc <= T with T the
+// largest double whose rounded sqrt is <= eps (identical by monotonicity).
+// FP32 filter: acc32 = |b|^2 + sum(-2 a_l b_l) in local coordinates around the
+// home cell's centre; pairs inside a proven error band of the threshold are
+// re-evaluated with the exact FP64 chain above, so the pair set is the FP64 set.
+#include "sj_internal.h"
+
+namespace {
+
+constexpr int NW = SJ_CTA / 32;
+
+__device__ __forceinline__ uint32_t transpose32(uint32_t x, uint32_t lane)
+{
+    // Lane i holds row i of a 32x32 bit matrix; afterwards lane j holds column j.
+#pragma unroll
+    for (int s = 16; s > 0; s >>= 1) {
+        const uint32_t lo = (s == 16) ? 0x0000ffffu
+                          : (s == 8)  ? 0x00ff00ffu
+                          : (s == 4)  ? 0x0f0f0f0fu
+                          : (s == 2)  ? 0x33333333u
+                                      : 0x55555555u;
+        uint32_t y = __shfl_xor_sync(0xffffffffu, x, s);
+        if (lane & s) x = (x & ~lo) | ((y & ~lo) >> s);
+        else x = (x & lo) | ((y & lo) << s);
+    }
+    return x;
+}
+
+template <int DP>
+__device__ __forceinline__ bool exact_hit(const double *__restrict__ xs, uint32_t cpos, uint32_t qpos, double T)
+{
+    const double *c = xs + (uint64_t)cpos * DP;
+    const double *q = xs + (uint64_t)qpos * DP;
+    double acc = 0.0;
+    // padded dimensions hold 0 in both points: fma(0,0,acc) == acc exactly
+#pragma unroll
+    for (int l = 0; l < DP; l++) {
+        double d = __dsub_rn(c[l], q[l]);
+        acc = __fma_rn(d, d, acc);
+    }
+    return acc <= T;
+}
+
+template <int DP>
+struct Stage64 {
+    static constexpr int S = (DP <= 8) ? SJ_STAGE : ((SJ_STAGE * 8 / DP) / 32) * 32;
+    double c[S][DP];
+};
+
+template <int DP>
+struct Stage32 {
+    static constexpr int CW = ((DP + 1 + 3) / 4) * 4;
+    static constexpr int S = SJ_STAGE;
+    float c[S][CW];   // local coordinates, then |b|^2 at [DP]
+};
+
+template <int DP, bool F32>
+struct StageOf { using T = Stage64<DP>; };
+template <int DP>
+struct StageOf<DP, true> { using T = Stage32<DP>; };
+
+template <int DP, bool F32, bool FILL>
+__global__ void __launch_bounds__(SJ_CTA) k_join(sj_join_args a, sj_grid_dev g, int queue)
+{
+    using Stage = typename StageOf<DP, F32>::T;
+    constexpr int S = Stage::S;
+    __shared__ Stage st;
+    __shared__ uint32_t candId[S];
+    __shared__ uint32_t segStart[SJ_MAX_SEG];
+    __shared__ uint32_t segPre[SJ_MAX_SEG + 1];
+    __shared__ uint32_t colCnt[FILL ? 1 : NW][FILL ? 1 : S];
+    __shared__ uint32_t qIdS[SJ_CTA];
+    __shared__ uint32_t scanTmp[NW];
+    __shared__ uint32_t curTask;
+    __shared__ unsigned long long taskPairs;
+
+    const uint32_t tid = threadIdx.x;
+    const uint32_t lane = tid & 31u;
+    const uint32_t warp = tid >> 5;
+    const int D = g.D;
+    const double T = g.thresh;
+
+    if (!FILL) {
+        for (int j = tid; j < NW * S; j += SJ_CTA) (&colCnt[0][0])[j] = 0;
+    }
+
+    uint32_t iter = 0;
+    for (;;) {
+        // ---- fetch the next task
+        __syncthreads();
+        if (tid == 0) {
+            uint32_t t = queue ? (a.taskBegin + atomicAdd(a.queueHead, 1u)) : (a.taskBegin + blockIdx.x + iter);
+            curTask = t;
+            taskPairs = 0ULL;
+        }
+        __syncthreads();
+        const uint32_t t = curTask;
+        if (t >= a.taskEnd || (!queue && iter > 0)) break;
+        iter++;
+        const sj_task task = a.tasks[t];
+        const bool sym = (task.flags & SJ_TASK_SYM) != 0;
+        const uint32_t cellA = task.cell;
+        const uint32_t aStart = a.cellStart[cellA], aEnd = a.cellStart[cellA + 1];
+        const uint32_t nbrBase = a.nbrStart[cellA];
+        const uint32_t nSeg = task.segCount;
+
+        // ---- segment table (exclusive prefix of lengths over the task's segments)
+        uint32_t locLen[(SJ_MAX_SEG + SJ_CTA - 1) / SJ_CTA];
+        uint32_t mySum = 0;
+#pragma unroll
+        for (int r = 0; r < (SJ_MAX_SEG + SJ_CTA - 1) / SJ_CTA; r++) {
+            uint32_t s = tid * ((SJ_MAX_SEG + SJ_CTA - 1) / SJ_CTA) + r;
+            uint32_t len = 0;
+            if (s < nSeg) {
+                uint32_t gs = task.segBase + s;
+                uint32_t st0, en;
+                if (gs == 0) {
+                    st0 = sym ? task.qBegin : aStart;
+                    en = aEnd;
+                } else {
+                    uint32_t b = a.nbrCell[nbrBase + gs - 1];
+                    st0 = a.cellStart[b];
+                    en = a.cellStart[b + 1];
+                }
+                segStart[s] = st0;
+                len = en - st0;
+            }
+            locLen[r] = len;
+            mySum += len;
+        }
+        {
+            // block exclusive scan of mySum
+            uint32_t x = mySum;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+                if (lane >= (uint32_t)o) x += y;
+            }
+            if (lane == 31) scanTmp[warp] = x;
+            __syncthreads();
+            uint32_t wpre = 0;
+            for (uint32_t w = 0; w < warp; w++) wpre += scanTmp[w];
+            uint32_t run = wpre + x - mySum;
+#pragma unroll
+            for (int r = 0; r < (SJ_MAX_SEG + SJ_CTA - 1) / SJ_CTA; r++) {
+                uint32_t s = tid * ((SJ_MAX_SEG + SJ_CTA - 1) / SJ_CTA) + r;
+                if (s <= nSeg) segPre[s] = run;
+                run += locLen[r];
+            }
+            if (tid == SJ_CTA - 1) segPre[nSeg] = run;   // grand total (also covers nSeg == SJ_MAX_SEG)
+        }
+        __syncthreads();
+        const uint32_t homeEnd = (task.segBase == 0 && (task.flags & SJ_TASK_HOME)) ? segPre[1] : 0u;
+
+        // ---- query point of this thread
+        const uint32_t qi = tid;
+        const bool qValid = qi < task.qCount;
+        const uint32_t qpos = task.qBegin + (qValid ? qi : 0u);
+        const uint32_t qid = a.ids[qpos];
+        qIdS[tid] = qid;
+        double q64[F32 ? 1 : DP];
+        float q2[F32 ? DP : 1];
+        float thrLo = 0.f, thrHi = 0.f;
+        double origin[F32 ? DP : 1];
+        if (F32) {
+            double na = 0.0;
+#pragma unroll
+            for (int l = 0; l < DP; l++) {
+                double o;
+                if (l < g.k) o = g.minArr[l] + ((double)a.cellCoord[(uint64_t)cellA * g.k + l] + 0.5) * g.eps;
+                else if (l < D) o = g.center[l];
+                else o = 0.0;
+                origin[l] = o;
+                float qa = (l < D) ? __double2float_rn(a.xs[(uint64_t)qpos * DP + l] - o) : 0.0f;
+                q2[l] = -2.0f * qa;
+                na += (double)qa * (double)qa;
+            }
+            thrLo = __double2float_rd(T - na - a.margin);
+            thrHi = __double2float_ru(T - na + a.margin);
+        } else {
+#pragma unroll
+            for (int l = 0; l < DP; l++) q64[l] = a.xs[(uint64_t)qpos * DP + l];
+        }
+
+        uint32_t rowCount = 0;       // count pass: pairs keyed by this query
+        uint32_t evals = 0;          // candidate evaluations
+        uint32_t refined = 0;        // FP32 borderline re-evaluations
+
+        // the stream can never extend past the segments actually present
+        const uint32_t sEnd = min(task.sEnd, segPre[nSeg]);
+        for (uint32_t sBase = task.sBegin; sBase < sEnd; sBase += S) {
+            const uint32_t nIn = min((uint32_t)S, sEnd - sBase);
+            __syncthreads();
+            // ---- stage candidates
+            for (uint32_t j = tid; j < nIn; j += SJ_CTA) {
+                uint32_t s = sBase + j;
+                uint32_t lo = 0, hi = nSeg;   // largest seg with segPre[seg] <= s
+                while (hi - lo > 1) {
+                    uint32_t mid = (lo + hi) >> 1;
+                    if (segPre[mid] <= s) lo = mid; else hi = mid;
+                }
+                uint32_t pos = segStart[lo] + (s - segPre[lo]);
+                candId[j] = a.ids[pos];
+                const double *src = a.xs + (uint64_t)pos * DP;
+                if (F32) {
+                    float *dst = reinterpret_cast<float *>(&st.c[j][0]);
+                    double nb = 0.0;
+#pragma unroll
+                    for (int l = 0; l < DP; l++) {
+                        float b = (l < D) ? __double2float_rn(src[l] - origin[l]) : 0.0f;
+                        dst[l] = b;
+                        nb += (double)b * (double)b;
+                    }
+                    dst[DP] = __double2float_rn(nb);
+                } else {
+                    double *dst = reinterpret_cast<double *>(&st.c[j][0]);
+#pragma unroll
+                    for (int l = 0; l < DP; l++) dst[l] = src[l];
+                }
+            }
+            __syncthreads();
+
+            for (uint32_t jb = 0; jb < nIn; jb += 32) {
+                const uint32_t nb = min(32u, nIn - jb);
+                const uint32_t inRange = (nb == 32) ? 0xffffffffu : ((1u << nb) - 1u);
+                uint32_t hits = 0, border = 0;
+                if (qValid) {
+#pragma unroll
+                    for (int jj = 0; jj < 32; jj++) {
+                        if (jj < (int)nb) {
+                            const int j = jb + jj;
+                            if (F32) {
+                                const float *cb = reinterpret_cast<const float *>(&st.c[j][0]);
+                                float acc = cb[DP];
+#pragma unroll
+                                for (int l = 0; l < DP; l++) acc = fmaf(q2[l], cb[l], acc);
+                                if (acc <= thrLo) hits |= 1u << jj;
+                                else if (acc <= thrHi) border |= 1u << jj;
+                            } else {
+                                const double *cb = reinterpret_cast<const double *>(&st.c[j][0]);
+                                double acc = 0.0;
+#pragma unroll
+                                for (int l = 0; l < DP; l++) {
+                                    double d = __dsub_rn(cb[l], q64[l]);
+                                    acc = __fma_rn(d, d, acc);
+                                }
+                                if (acc <= T) hits |= 1u << jj;
+                            }
+                        }
+                    }
+                }
+                // validity: the symmetric home segment keeps only cand >= query
+                uint32_t rowValid = inRange, mirValid = sym ? inRange : 0u;
+                const uint32_t blk = sBase + jb;
+                if (blk < homeEnd) {
+                    uint32_t hn = homeEnd - blk;
+                    uint32_t homeBits = hn >= 32 ? 0xffffffffu : ((1u << hn) - 1u);
+                    if (sym) {
+                        int lo = (int)qi - (int)blk;     // home cand index >= query index
+                        uint32_t ge = lo <= 0 ? 0xffffffffu : (lo >= 32 ? 0u : (0xffffffffu << lo));
+                        uint32_t gt = (lo + 1) <= 0 ? 0xffffffffu : ((lo + 1) >= 32 ? 0u : (0xffffffffu << (lo + 1)));
+                        rowValid &= (~homeBits) | (homeBits & ge);
+                        mirValid &= (~homeBits) | (homeBits & gt);
+                    }
+                }
+                if (!qValid) { rowValid = 0; mirValid = 0; }
+                if (F32) {
+                    uint32_t bm = border & rowValid;
+                    while (bm) {
+                        int jj = __ffs(bm) - 1;
+                        bm &= bm - 1;
+                        uint32_t s = blk + jj;
+                        uint32_t lo = 0, hi = nSeg;
+                        while (hi - lo > 1) {
+                            uint32_t mid = (lo + hi) >> 1;
+                            if (segPre[mid] <= s) lo = mid; else hi = mid;
+                        }
+                        uint32_t cpos = segStart[lo] + (s - segPre[lo]);
+                        refined++;
+                        if (exact_hit<DP>(a.xs, cpos, qpos, T)) hits |= 1u << jj;
+                    }
+                }
+                evals += __popc(rowValid);
+                const uint32_t rowMask = hits & rowValid;
+                const uint32_t mirMask = transpose32(hits & mirValid, lane);
+                if (FILL) {
+                    uint32_t n = __popc(rowMask);
+                    if (n) {
+                        uint32_t p = atomicAdd(&a.keyCursor[qid], n);
+                        if ((uint64_t)p + n <= a.capacity) {
+                            uint32_t m = rowMask;
+                            while (m) {
+                                int b = __ffs(m) - 1;
+                                m &= m - 1;
+                                a.outKey[p] = (int32_t)qid;
+                                a.outVal[p] = (int32_t)candId[jb + b];
+                                p++;
+                            }
+                        } else {
+                            atomicMax(&a.stat[3], 1ULL);
+                        }
+                    }
+                    uint32_t nm = __popc(mirMask);
+                    if (nm) {
+                        uint32_t cid = candId[jb + lane];
+                        uint32_t p = atomicAdd(&a.keyCursor[cid], nm);
+                        if ((uint64_t)p + nm <= a.capacity) {
+                            uint32_t m = mirMask;
+                            while (m) {
+                                int b = __ffs(m) - 1;
+                                m &= m - 1;
+                                a.outKey[p] = (int32_t)cid;
+                                a.outVal[p] = (int32_t)qIdS[warp * 32 + b];
+                                p++;
+                            }
+                        } else {
+                            atomicMax(&a.stat[3], 1ULL);
+                        }
+                    }
+                } else {
+                    rowCount += __popc(rowMask);
+                    if (sym) colCnt[warp][jb + lane] += __popc(mirMask);
+                }
+            }
+            if (!FILL && sym) {
+                __syncthreads();
+                uint32_t local = 0;
+                for (uint32_t j = tid; j < nIn; j += SJ_CTA) {
+                    uint32_t tot = 0;
+#pragma unroll
+                    for (int w = 0; w < NW; w++) { tot += colCnt[w][j]; colCnt[w][j] = 0; }
+                    if (tot) { atomicAdd(&a.keyCount[candId[j]], tot); local += tot; }
+                }
+                if (local) atomicAdd(&taskPairs, (unsigned long long)local);
+            }
+        }
+        if (!FILL) {
+            if (rowCount) {
+                atomicAdd(&a.keyCount[qid], rowCount);
+                atomicAdd(&taskPairs, (unsigned long long)rowCount);
+            }
+        }
+        // ---- statistics
+        unsigned long long e = evals, r = refined;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            e += __shfl_xor_sync(0xffffffffu, e, o);
+            r += __shfl_xor_sync(0xffffffffu, r, o);
+        }
+        if (lane == 0) {
+            if (e) atomicAdd(&a.stat[0], e);
+            if (r) atomicAdd(&a.stat[1], r);
+        }
+        if (!FILL) {
+            __syncthreads();
+            if (tid == 0) {
+                if (taskPairs) atomicAdd(&a.stat[2], taskPairs);
+                if (a.taskHits) a.taskHits[t] = (uint32_t)min(taskPairs, 0xffffffffULL);
+            }
+        }
+    }
+}
+
+template <int DP>
+cudaError_t launch_dp(const sj_join_args &a, const sj_grid_dev &g, int fill, int fp32, int queue, int numSM,
+                      cudaStream_t s)
+{
+    uint32_t nt = a.taskEnd - a.taskBegin;
+    if (nt == 0) return cudaSuccess;
+    unsigned grid = queue ? (unsigned)(numSM * 8) : nt;
+    if (queue && grid > nt) grid = nt;
+    if (fp32) {
+        if (fill) k_join<DP, true, true><<<grid, SJ_CTA, 0, s>>>(a, g, queue);
+        else k_join<DP, true, false><<<grid, SJ_CTA, 0, s>>>(a, g, queue);
+    } else {
+        if (fill) k_join<DP, false, true><<<grid, SJ_CTA, 0, s>>>(a, g, queue);
+        else k_join<DP, false, false><<<grid, SJ_CTA, 0, s>>>(a, g, queue);
+    }
+    return cudaGetLastError();
+}
+
+}  // namespace
+
+cudaError_t sj_launch_join(const sj_join_args &a, const sj_grid_dev &g, int fill, int fp32, int queue, int numSM,
+                           cudaStream_t s)
+{
+    switch (g.Dp) {
+    case 1: return launch_dp<1>(a, g, fill, fp32, queue, numSM, s);
+    case 2: return launch_dp<2>(a, g, fill, fp32, queue, numSM, s);
+    case 3: return launch_dp<3>(a, g, fill, fp32, queue, numSM, s);
+    case 4: return launch_dp<4>(a, g, fill, fp32, queue, numSM, s);
+    case 6: return launch_dp<6>(a, g, fill, fp32, queue, numSM, s);
+    case 8: return launch_dp<8>(a, g, fill, fp32, queue, numSM, s);
+    case 12: return launch_dp<12>(a, g, fill, fp32, queue, numSM, s);
+    case 16: return launch_dp<16>(a, g, fill, fp32, queue, numSM, s);
+    }
+    return cudaErrorInvalidValue;
+}

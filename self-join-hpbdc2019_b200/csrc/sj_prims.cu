@@ -1,0 +1,283 @@
+// Device primitives: exclusive scan (u32), stable LSD radix sort, pair-set hash.
+#include "sj_internal.h"
+
+namespace {
+
+constexpr int SCAN_THREADS = 256;
+constexpr int SCAN_ITEMS = 8;
+constexpr int SCAN_TILE = SCAN_THREADS * SCAN_ITEMS;   // 2048 elements per block
+
+__device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
+
+// Block-wide exclusive scan of one value per thread; returns the exclusive
+// prefix and writes the block total to *total.
+__device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t *total)
+{
+    __shared__ uint32_t warpSums[SCAN_THREADS / 32];
+    uint32_t x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane_id() >= (uint32_t)o) x += y;
+    }
+    const int w = threadIdx.x >> 5;
+    if (lane_id() == 31) warpSums[w] = x;
+    __syncthreads();
+    if (w == 0) {
+        uint32_t s = (lane_id() < SCAN_THREADS / 32) ? warpSums[lane_id()] : 0u;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            uint32_t y = __shfl_up_sync(0xffffffffu, s, o);
+            if (lane_id() >= (uint32_t)o) s += y;
+        }
+        if (lane_id() < SCAN_THREADS / 32) warpSums[lane_id()] = s;   // inclusive warp prefixes
+    }
+    __syncthreads();
+    uint32_t warpPrefix = (w > 0) ? warpSums[w - 1] : 0u;
+    *total = warpSums[SCAN_THREADS / 32 - 1];
+    __syncthreads();
+    return warpPrefix + x - v;
+}
+
+__global__ void __launch_bounds__(SCAN_THREADS) k_scan_reduce(const uint32_t *__restrict__ in, uint64_t n,
+                                                              uint32_t *__restrict__ sums)
+{
+    uint64_t base = (uint64_t)blockIdx.x * SCAN_TILE;
+    uint32_t s = 0;
+#pragma unroll
+    for (int i = 0; i < SCAN_ITEMS; i++) {
+        uint64_t idx = base + (uint64_t)i * SCAN_THREADS + threadIdx.x;
+        if (idx < n) s += in[idx];
+    }
+    uint32_t tot;
+    block_exclusive_scan(s, &tot);
+    if (threadIdx.x == 0) sums[blockIdx.x] = tot;
+}
+
+// Scans one tile per block; adds the block's offset from `blockOffsets`
+// (nullptr for a single-block scan, which also writes the grand total).
+__global__ void __launch_bounds__(SCAN_THREADS) k_scan_tile(const uint32_t *in, uint32_t *out, uint64_t n,
+                                                            const uint32_t *__restrict__ blockOffsets,
+                                                            uint32_t *total_dev)
+{
+    uint64_t base = (uint64_t)blockIdx.x * SCAN_TILE + (uint64_t)threadIdx.x * SCAN_ITEMS;
+    uint32_t v[SCAN_ITEMS];
+    uint32_t s = 0;
+#pragma unroll
+    for (int i = 0; i < SCAN_ITEMS; i++) {
+        uint64_t idx = base + i;
+        v[i] = (idx < n) ? in[idx] : 0u;
+        s += v[i];
+    }
+    uint32_t tot;
+    uint32_t pre = block_exclusive_scan(s, &tot);
+    uint32_t off = (blockOffsets ? blockOffsets[blockIdx.x] : 0u) + pre;
+#pragma unroll
+    for (int i = 0; i < SCAN_ITEMS; i++) {
+        uint64_t idx = base + i;
+        if (idx < n) out[idx] = off;
+        off += v[i];
+    }
+    if (!blockOffsets && total_dev && threadIdx.x == 0) *total_dev = tot;
+}
+
+__global__ void k_scan_total(const uint32_t *scannedSums, const uint32_t *sums, uint64_t nb, uint32_t *total_dev)
+{
+    if (threadIdx.x == 0 && blockIdx.x == 0 && total_dev) *total_dev = scannedSums[nb - 1] + sums[nb - 1];
+}
+
+uint64_t ceil_div(uint64_t a, uint64_t b) { return (a + b - 1) / b; }
+
+size_t scan_temp_elems(uint64_t n)
+{
+    size_t e = 0;
+    while (n > (uint64_t)SCAN_TILE) {
+        uint64_t nb = ceil_div(n, SCAN_TILE);
+        e += 2 * nb;
+        n = nb;
+    }
+    return e + 1;
+}
+
+cudaError_t scan_rec(const uint32_t *in, uint32_t *out, uint64_t n, uint32_t *temp, uint32_t *total_dev,
+                     cudaStream_t s)
+{
+    if (n == 0) {
+        if (total_dev) return cudaMemsetAsync(total_dev, 0, sizeof(uint32_t), s);
+        return cudaSuccess;
+    }
+    if (n <= (uint64_t)SCAN_TILE) {
+        k_scan_tile<<<1, SCAN_THREADS, 0, s>>>(in, out, n, nullptr, total_dev);
+        return cudaGetLastError();
+    }
+    uint64_t nb = ceil_div(n, SCAN_TILE);
+    uint32_t *sums = temp, *scanned = temp + nb;
+    k_scan_reduce<<<(unsigned)nb, SCAN_THREADS, 0, s>>>(in, n, sums);
+    cudaError_t e = scan_rec(sums, scanned, nb, temp + 2 * nb, nullptr, s);
+    if (e != cudaSuccess) return e;
+    if (total_dev) k_scan_total<<<1, 32, 0, s>>>(scanned, sums, nb, total_dev);
+    k_scan_tile<<<(unsigned)nb, SCAN_THREADS, 0, s>>>(in, out, n, scanned, nullptr);
+    return cudaGetLastError();
+}
+
+// ------------------------------------------------------------- radix sort --
+
+constexpr int RS_THREADS = 256;
+constexpr int RS_CHUNKS = 8;                       // chunks of RS_THREADS keys per tile
+constexpr int RS_TILE = RS_THREADS * RS_CHUNKS;    // 2048 keys per block
+constexpr int RS_WARPS = RS_THREADS / 32;
+
+template <typename K>
+__global__ void __launch_bounds__(RS_THREADS) k_radix_hist(const K *__restrict__ keys, uint64_t n, int shift,
+                                                           uint32_t *__restrict__ blockHist, uint32_t nb)
+{
+    __shared__ uint32_t h[256];
+    h[threadIdx.x] = 0;
+    __syncthreads();
+    uint64_t base = (uint64_t)blockIdx.x * RS_TILE;
+#pragma unroll
+    for (int c = 0; c < RS_CHUNKS; c++) {
+        uint64_t idx = base + (uint64_t)c * RS_THREADS + threadIdx.x;
+        if (idx < n) atomicAdd(&h[(uint32_t)(keys[idx] >> shift) & 255u], 1u);
+    }
+    __syncthreads();
+    blockHist[(uint64_t)threadIdx.x * nb + blockIdx.x] = h[threadIdx.x];   // digit-major
+}
+
+// Stable scatter: keys keep their input order within a digit.
+template <typename K>
+__global__ void __launch_bounds__(RS_THREADS) k_radix_scatter(const K *__restrict__ keysIn,
+                                                              const uint32_t *__restrict__ valsIn,
+                                                              K *__restrict__ keysOut, uint32_t *__restrict__ valsOut,
+                                                              uint64_t n, int shift,
+                                                              const uint32_t *__restrict__ digitOffsets, uint32_t nb)
+{
+    __shared__ uint32_t base[256];
+    __shared__ uint32_t warpCnt[RS_WARPS][256];
+    base[threadIdx.x] = digitOffsets[(uint64_t)threadIdx.x * nb + blockIdx.x];
+#pragma unroll
+    for (int w = 0; w < RS_WARPS; w++) warpCnt[w][threadIdx.x] = 0;
+    __syncthreads();
+    const int w = threadIdx.x >> 5;
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t ltmask = (1u << lane) - 1u;
+    uint64_t tileBase = (uint64_t)blockIdx.x * RS_TILE;
+    for (int c = 0; c < RS_CHUNKS; c++) {
+        uint64_t idx = tileBase + (uint64_t)c * RS_THREADS + threadIdx.x;
+        bool valid = idx < n;
+        K key = valid ? keysIn[idx] : (K)0;
+        uint32_t val = valid ? valsIn[idx] : 0u;
+        uint32_t d = valid ? ((uint32_t)(key >> shift) & 255u) : 256u;
+        uint32_t peers = __match_any_sync(0xffffffffu, d);
+        uint32_t rank = __popc(peers & ltmask);
+        if (valid && rank == 0) warpCnt[w][d] = __popc(peers);
+        __syncthreads();
+        if (valid) {
+            uint32_t pre = 0;
+            for (int v = 0; v < w; v++) pre += warpCnt[v][d];
+            uint32_t pos = base[d] + pre + rank;
+            keysOut[pos] = key;
+            valsOut[pos] = val;
+        }
+        __syncthreads();
+        uint32_t add = 0;
+#pragma unroll
+        for (int v = 0; v < RS_WARPS; v++) { add += warpCnt[v][threadIdx.x]; warpCnt[v][threadIdx.x] = 0; }
+        base[threadIdx.x] += add;
+        __syncthreads();
+    }
+}
+
+template <typename K>
+cudaError_t radix_sort(K *keys, uint32_t *vals, K *keysAlt, uint32_t *valsAlt, uint64_t n, int bits, void *temp,
+                       int *resultInAlt, cudaStream_t s)
+{
+    *resultInAlt = 0;
+    if (n <= 1 || bits <= 0) return cudaSuccess;
+    uint32_t nb = (uint32_t)ceil_div(n, RS_TILE);
+    uint32_t *hist = (uint32_t *)temp;
+    uint32_t *scanTemp = hist + (size_t)256 * nb;
+    K *kin = keys, *kout = keysAlt;
+    uint32_t *vin = vals, *vout = valsAlt;
+    int alt = 0;
+    for (int shift = 0; shift < bits; shift += 8) {
+        k_radix_hist<K><<<nb, RS_THREADS, 0, s>>>(kin, n, shift, hist, nb);
+        cudaError_t e = scan_rec(hist, hist, (uint64_t)256 * nb, scanTemp, nullptr, s);
+        if (e != cudaSuccess) return e;
+        k_radix_scatter<K><<<nb, RS_THREADS, 0, s>>>(kin, vin, kout, vout, n, shift, hist, nb);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+        K *tk = kin; kin = kout; kout = tk;
+        uint32_t *tv = vin; vin = vout; vout = tv;
+        alt ^= 1;
+    }
+    *resultInAlt = alt;
+    return cudaSuccess;
+}
+
+__device__ __forceinline__ unsigned long long splitmix64(unsigned long long z)
+{
+    z += 0x9e3779b97f4a7c15ULL;
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebULL;
+    return z ^ (z >> 31);
+}
+
+__global__ void __launch_bounds__(256) k_hash_pairs(const int32_t *__restrict__ key, const int32_t *__restrict__ val,
+                                                    uint64_t m, unsigned long long *out)
+{
+    unsigned long long h = 0;
+    uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += stride) {
+        unsigned long long z = ((unsigned long long)(uint32_t)key[i] << 32) | (uint32_t)val[i];
+        h += splitmix64(z);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) h += __shfl_xor_sync(0xffffffffu, h, o);
+    __shared__ unsigned long long ws[8];
+    if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = h;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long t = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += ws[w];
+        atomicAdd(out, t);
+    }
+}
+
+}  // namespace
+
+size_t sj_scan_temp_bytes(uint64_t n) { return scan_temp_elems(n) * sizeof(uint32_t); }
+
+cudaError_t sj_exclusive_scan_u32(const uint32_t *in, uint32_t *out, uint64_t n, void *temp, uint32_t *total_dev,
+                                  cudaStream_t s)
+{
+    return scan_rec(in, out, n, (uint32_t *)temp, total_dev, s);
+}
+
+size_t sj_radix_temp_bytes(uint64_t n)
+{
+    uint64_t nb = ceil_div(n ? n : 1, RS_TILE);
+    return (size_t)256 * nb * sizeof(uint32_t) + sj_scan_temp_bytes((uint64_t)256 * nb);
+}
+
+cudaError_t sj_radix_sort_u64_u32(uint64_t *keys, uint32_t *vals, uint64_t *keysAlt, uint32_t *valsAlt, uint64_t n,
+                                  int bits, void *temp, int *resultInAlt, cudaStream_t s)
+{
+    return radix_sort<uint64_t>(keys, vals, keysAlt, valsAlt, n, bits, temp, resultInAlt, s);
+}
+
+cudaError_t sj_radix_sort_u32_u32(uint32_t *keys, uint32_t *vals, uint32_t *keysAlt, uint32_t *valsAlt, uint64_t n,
+                                  int bits, void *temp, int *resultInAlt, cudaStream_t s)
+{
+    return radix_sort<uint32_t>(keys, vals, keysAlt, valsAlt, n, bits, temp, resultInAlt, s);
+}
+
+cudaError_t sj_hash_pairs(const int32_t *key, const int32_t *val, uint64_t m, unsigned long long *hashOut,
+                          cudaStream_t s)
+{
+    if (m == 0) return cudaSuccess;
+    uint64_t blocks = ceil_div(m, 256 * 16);
+    if (blocks > 148 * 16) blocks = 148 * 16;
+    k_hash_pairs<<<(unsigned)blocks, 256, 0, s>>>(key, val, m, hashOut);
+    return cudaGetLastError();
+}
