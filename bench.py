@@ -1,0 +1,315 @@
+#!/usr/bin/env python
+"""Epsilon self-join throughput on B200: pairs/s of one full self-join step.
+
+Workload (default c2): 2-D, n = 2,000,000 points with i.i.d. exponential(40)
+coordinates clipped to [0, 1] (seeded synthetic), eps = 0.0015, B-Unicomp
+traversal with workload-sorted tasks on a persistent work queue, FP64, result
+batches of at most 5e7 pairs.  One step = grid-index build + estimate + batched
+join (count, scan, fill per batch) + an on-device fold of every batch into the
+pair count and set hash, with the points already resident in HBM.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--workload c1..c5] [--n N]
+
+N > 1 (launched by torch.distributed.run): every rank runs its own replica of
+the workload on its own seed (weak scaling, no data-path collective); the
+per-step time is the maximum over ranks.
+
+--impl reference times the CPU restatement of the reference's path (the
+oracle port) on the host cores, on a bounded sample of the same workload,
+because the reference's own CUDA build does not produce pairs with this
+toolchain (its device cell lookups call a host-only comparison operator).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+sys.path.insert(0, os.path.join(REPO, "self-join-hpbdc2019_b200"))
+
+import numpy as np  # noqa: E402
+
+# dram__bytes_read.sum + dram__bytes_write.sum per output pair of the fill
+# kernel, from the ncu capture summarised in profiles/ (None until captured)
+FILL_TRAFFIC_BYTES_PER_PAIR = None
+
+L2_BYTES = 126 * 1024 * 1024
+
+
+def _peaks():
+    try:
+        with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        self.proc.wait()
+        rows = []
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        busy = [s for s in sm if mx and s > 0.3 * max(mx)] or sm
+        return {"sm_mhz": statistics.median(busy) if busy else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def _dist():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def cpu_oracle_rate(pts, eps, k, target_s=12.0, threads=0):
+    """Oracle grid join on a bounded sample of query points: (pairs/s, cores, sample text)."""
+    import oracle
+    ix = oracle.OracleIndex(pts, eps, k)
+    n = len(pts)
+    stride = max(1, n // 2000)
+    t0 = time.perf_counter()
+    P, _, E = ix.stats(qstride=stride, threads=threads)
+    dt = time.perf_counter() - t0
+    if dt < target_s / 4:
+        stride = max(1, int(stride * dt / target_s))
+        t0 = time.perf_counter()
+        P, _, E = ix.stats(qstride=stride, threads=threads)
+        dt = time.perf_counter() - t0
+    cores = threads or oracle.num_threads()
+    nq = (n + stride - 1) // stride
+    sample = f"every {stride}th query point ({nq} of {n}), full stencil, {E} candidate evaluations, {dt:.1f} s"
+    return P / dt, cores, sample, dt
+
+
+def run_reference(args):
+    import oracle
+    import sjoin
+    ws, rank, _ = _dist()
+    if rank != 0:
+        return
+    pts, eps, k, spec = sjoin.datasets.make(args.workload, n=args.n)
+    times, rates = [], []
+    for i in range(args.warmup + args.steps):
+        rate, cores, sample, dt = cpu_oracle_rate(pts, eps, k, target_s=args.ref_seconds)
+        if i >= args.warmup:
+            rates.append(rate)
+            times.append(dt)
+    v = statistics.mean(rates)
+    line = {
+        "impl": "reference", "metric": "self-join pairs/s", "value": v, "unit": "pairs/s", "n_gpus": ws,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * statistics.mean(times),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded)", "config": _config(args, spec),
+        "cpu_baseline": {"value": v, "unit": "pairs/s", "cores": cores, "kind": "port", "sample": sample},
+        "e2e": {"value": v, "unit": "pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def _config(args, spec):
+    mode_name = {3: "full stencil", 4: "Unicomp", 5: "B-Unicomp", 6: "linear-ID Unicomp", 7: "full stencil",
+                 9: "work queue", 10: "linear-ID Unicomp"}[spec["mode"]]
+    return {
+        "workload": (f"{args.workload}: {spec['D']}-D {spec['kind']}, n={spec['n']}, eps={spec['eps']}, "
+                     f"{mode_name} + workload-sorted work queue, "
+                     f"{'FP64' if spec['precision'] == 0 else 'FP32 filter + FP64 refine'}, "
+                     f"batches <= {spec['capacity'] or 'auto'} pairs"),
+        "n": spec["n"], "dims": spec["D"], "indexed_dims": spec["k"], "eps": spec["eps"],
+        "search_mode": spec["mode"], "batch_capacity_pairs": spec["capacity"],
+        "l2": "flushed between steps (256 MiB write); outputs far exceed L2",
+        "parallelism": f"replicas x{_dist()[0]}",
+    }
+
+
+def run_ours(args):
+    import torch
+
+    import sjoin
+    ws, rank, local = _dist()
+    torch.cuda.set_device(local)
+    if ws > 1:
+        import datetime
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    pts, eps, k, spec = sjoin.datasets.make(args.workload, n=args.n,
+                                            seed=sjoin.datasets.SEEDS[args.workload] + 1000 * rank)
+    prec = spec["precision"] if args.precision is None else args.precision
+    flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device="cuda")
+    sj = sjoin.SelfJoin(spec["D"], eps, indexed_dims=k, mode=spec["mode"], precision=prec,
+                        capacity=spec["capacity"], device=local)
+    if args.learned:
+        sj.load_estimator(args.learned)
+    host = torch.from_numpy(pts).pin_memory()
+    sj.set_points(host.numpy())
+    stream = torch.cuda.ExternalStream(sj.stream())
+
+    def step():
+        sj.build_index()
+        return sj.join(sjoin.DELIVER_NONE)
+
+    for _ in range(args.warmup):
+        step()
+    sampler = ClockSampler(torch.cuda.current_device())
+    sampler.start()
+    if ws > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    launches0 = sjoin.kernel_launch_count()
+    step_ms, stats = [], []
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        st = step()
+        e1.record(stream)
+        e1.synchronize()
+        step_ms.append(e0.elapsed_time(e1))
+        stats.append(st.as_dict())
+    torch.cuda.synchronize()
+    launches = sjoin.kernel_launch_count() - launches0
+    if ws > 1:
+        torch.distributed.barrier()
+    clocks = sampler.stop()
+    ms = statistics.mean(step_ms)
+    pairs = stats[-1]["total_pairs"]
+    job_ms, job_pairs = ms, pairs
+    if ws > 1:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        p = torch.tensor([pairs], device="cuda", dtype=torch.float64)
+        torch.distributed.all_reduce(p)
+        job_ms, job_pairs = float(t.item()), float(p.item())
+
+    # end to end through the C ABI with host buffers: pinned H2D of the points,
+    # index, join, and every batch copied device-to-host into pinned buffers
+    e2e = None
+    if not args.no_e2e:
+        def e2e_step():
+            sj.set_points(host.numpy())
+            sj.build_index()
+            return sj.join(sjoin.DELIVER_HOST, lambda i, kk, vv: None)
+
+        e2e_step()
+        torch.cuda.synchronize()
+        ems = []
+        for _ in range(max(1, min(args.steps, args.e2e_steps))):
+            flush.zero_()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            st_e = e2e_step()
+            e1.record(stream)
+            e1.synchronize()
+            ems.append(e0.elapsed_time(e1))
+        e_ms = statistics.mean(ems)
+        if ws > 1:
+            t = torch.tensor([e_ms], device="cuda", dtype=torch.float64)
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            e_ms = float(t.item())
+        e2e = {"value": job_pairs / (e_ms / 1e3), "unit": "pairs/s", "ms_per_step": e_ms,
+               "h2d_bytes_per_step": int(pts.nbytes), "d2h_bytes_per_step": int(st_e.total_pairs) * 8}
+
+    if rank != 0:
+        if ws > 1:
+            torch.distributed.destroy_process_group()
+        return
+    peak, peak_kind = _peaks()
+    s = stats[-1]
+    fill_ms = s["ms_fill_kernel"]
+    achieved = (pairs * 8) / (fill_ms / 1e3) / 1e9 if fill_ms > 0 else None
+    traffic = FILL_TRAFFIC_BYTES_PER_PAIR * pairs / max(1, s["num_batches"]) if FILL_TRAFFIC_BYTES_PER_PAIR else None
+    cpu = None
+    if not args.no_cpu:
+        rate, cores, sample, _ = cpu_oracle_rate(pts, eps, k, target_s=args.cpu_seconds)
+        cpu = {"value": rate, "unit": "pairs/s", "cores": cores, "kind": "port", "sample": sample}
+    line = {
+        "metric": "self-join pairs/s", "value": job_pairs / (job_ms / 1e3), "unit": "pairs/s", "n_gpus": ws,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": job_ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64" if prec == 0 else "f32+f64",
+        "data": "synthetic (seeded generator, same shapes and distributions)", "config": _config(args, spec),
+        "time_s": job_ms / 1e3, "pairs_per_step": pairs, "pair_hash": s["pair_hash"],
+        "roofline": {"bound": "hbm", "kernel": "k_join fill pass (pair writes)", "achieved": achieved,
+                     "peak": peak, "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
+                     "peak_kind": peak_kind, "algorithmic_bytes_per_pair": 8,
+                     "traffic": traffic, "launches": s["num_batches"]},
+        "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clocks,
+        "phases_ms": {k2: round(s[k2], 3) for k2 in ("ms_index", "ms_tasks", "ms_estimate", "ms_count", "ms_scan",
+                                                     "ms_fill", "ms_deliver", "ms_total")},
+        "batches": s["num_batches"], "overflow_retries": s["overflow_retries"],
+        "distance_calcs": s["distance_calcs"], "full_stencil_calcs": s["full_stencil_calcs"],
+        "refined_pairs": s["refined_pairs"], "step_ms": step_ms,
+    }
+    print(json.dumps(line), flush=True)
+    if ws > 1:
+        torch.distributed.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", default="c2")
+    ap.add_argument("--n", type=int, default=None)
+    ap.add_argument("--precision", type=int, default=None)
+    ap.add_argument("--learned", default=None)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--ref-seconds", type=float, default=10.0)
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

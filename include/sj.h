@@ -105,6 +105,7 @@ typedef struct {
     float ms_upload, ms_index, ms_tasks, ms_estimate, ms_count, ms_scan, ms_fill, ms_deliver, ms_total;
     float ms_join_kernels;      /* count + fill kernel time */
     float ms_fill_kernel;       /* fill kernel time alone */
+    uint64_t kernel_launches;   /* this library's kernel launches during the last join */
 } sj_stats;
 
 /* Fill `p` with params.h defaults: D=k=2, BLOCKSIZE 256, THREADPERPOINT 1,
@@ -163,6 +164,10 @@ void sj_free(void *p);
 
 sj_status sj_get_stats(void *ctx, sj_stats *st);
 
+/* The CUDA stream (cudaStream_t) all of this context's work is ordered on, so
+ * a caller can record events around sj_build_index / sj_join. */
+sj_status sj_get_stream(void *ctx, void **stream);
+
 /* Learned estimator.  Weights: SJ_MLP_NPARAM floats laid out W1[16x64], b1[64],
  * W2[64x64], b2[64], W3[64x2], b3[2] (row-major, input-major). */
 uint32_t sj_mlp_num_params(void);
@@ -184,6 +189,9 @@ sj_status sj_mlp_loss_grad(const float *x, const float *y, uint32_t m, const flo
                            float *grad, int device);
 /* Forward pass only: out m x 2. */
 sj_status sj_mlp_forward(const float *x, uint32_t m, const float *w, float *out, int device);
+
+/* Kernels this library has launched since it was loaded (all contexts). */
+uint64_t sj_kernel_launch_count(void);
 
 const char *sj_status_string(sj_status s);
 const char *sj_last_error(void);

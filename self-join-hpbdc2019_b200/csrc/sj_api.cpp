@@ -634,6 +634,7 @@ void order_tasks(Ctx &c)
 
 sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
 {
+    const unsigned long long launches0 = sj_launch_total();
     Timer total;
     total.start(c.s);
     int pattern;
@@ -657,8 +658,6 @@ sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
     c.st.num_tasks = nt;
     CK(c.keyCount.ensure(n));
     CK(c.keyCursor.ensure(n));
-    CK(c.outKey.ensure(cap));
-    CK(c.outVal.ensure(cap));
     CK(c.scanTemp.ensure(sj_scan_temp_bytes(n)));
     CK(c.total.ensure(1));
     CK(c.stat.ensure(8));
@@ -666,12 +665,6 @@ sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
     CK(c.taskHits.ensure(nt ? nt : 1));
     CK(c.pinTotal.ensure(64));
     CK(cudaMemsetAsync(c.stat.p, 0, sizeof(unsigned long long) * 8, c.s));
-    if (delivery == SJ_DELIVER_HOST) {
-        for (int b = 0; b < 2; b++) {
-            CK(c.pinKey[b].ensure(cap * sizeof(int32_t)));
-            CK(c.pinVal[b].ensure(cap * sizeof(int32_t)));
-        }
-    }
     double predTotal = 0;
     for (double v : c.taskPred) predTotal += v;
     c.st.estimated_pairs = predTotal;
@@ -750,6 +743,21 @@ sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
         double pred = 0;
         for (uint32_t t = br.t0; t < br.t1; t++) pred += c.taskPred[t];
         if (cnt > 0) relErrSum += std::fabs(pred - (double)cnt) / (double)cnt;
+        // output buffers follow the exact batch size (grow-only, 25% headroom, <= capacity)
+        if (cnt > c.outKey.n) {
+            uint64_t want = std::min<uint64_t>(cap, std::max<uint64_t>(cnt, (uint64_t)(1.25 * (double)c.outKey.n)));
+            CK(c.outKey.ensure(want));
+            CK(c.outVal.ensure(want));
+        }
+        if (delivery == SJ_DELIVER_HOST && cnt * sizeof(int32_t) > c.pinKey[pinSel].bytes) {
+            size_t want = std::max<size_t>(cnt * sizeof(int32_t), (size_t)(1.25 * (double)c.pinKey[pinSel].bytes));
+            want = std::min<size_t>(want, cap * sizeof(int32_t));
+            CK(c.pinKey[pinSel].ensure(want));
+            CK(c.pinVal[pinSel].ensure(want));
+        }
+        a.outKey = c.outKey.p;
+        a.outVal = c.outVal.p;
+        a.capacity = c.outKey.n;
         // fill pass
         tb.start(c.s);
         CKS(run_pass(c, a, true, queue));
@@ -807,6 +815,7 @@ sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
     c.st.ms_join_kernels = msCount + msFill;
     c.st.ms_fill_kernel = msFill;
     c.st.ms_total = total.stop(c.s);
+    c.st.kernel_launches = sj_launch_total() - launches0;
     return result;
 }
 
@@ -1175,6 +1184,13 @@ sj_status sj_neighbor_table(void *ctx, sj_neighbor_table_lookup *table, int **va
 
 void sj_free(void *p) { free(p); }
 
+sj_status sj_get_stream(void *ctx, void **stream)
+{
+    if (!ctx || !stream) return SJ_ERR_BAD_INPUT;
+    *stream = (void *)as_ctx(ctx)->s;
+    return SJ_OK;
+}
+
 sj_status sj_get_stats(void *ctx, sj_stats *st)
 {
     if (!ctx || !st) return SJ_ERR_BAD_INPUT;
@@ -1352,6 +1368,8 @@ const char *sj_status_string(sj_status s)
 }
 
 const char *sj_last_error(void) { return g_lastError.c_str(); }
+
+uint64_t sj_kernel_launch_count(void) { return sj_launch_total(); }
 
 const char *sj_version(void) { return "sj-b200 0.1 (sm_100a)"; }
 

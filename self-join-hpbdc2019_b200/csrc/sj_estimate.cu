@@ -200,14 +200,14 @@ cudaError_t sj_launch_sample(const sj_join_args &a, const sj_grid_dev &g, uint32
     uint64_t nSamples = (nPoints + (uint64_t)sampleStride - 1) / sampleStride;
     if (nSamples == 0) return cudaSuccess;
     uint64_t blocks = (nSamples * 32 + 255) / 256;
-    k_sample<<<(unsigned)blocks, 256, 0, s>>>(a, g, sampleStride, nPoints, nCells, cellHits, cellCands);
+    k_sample<<<(unsigned)blocks, 256, 0, s>>>(a, g, sampleStride, nPoints, nCells, cellHits, cellCands); sj_note_launch();
     return cudaGetLastError();
 }
 
 cudaError_t sj_launch_mlp_infer(const float *feat, uint32_t nCells, const float *weights, float *out, cudaStream_t s)
 {
     if (nCells == 0) return cudaSuccess;
-    k_mlp_infer<<<(nCells + 127) / 128, 128, 0, s>>>(feat, nCells, weights, out);
+    k_mlp_infer<<<(nCells + 127) / 128, 128, 0, s>>>(feat, nCells, weights, out); sj_note_launch();
     return cudaGetLastError();
 }
 
@@ -222,8 +222,8 @@ static cudaError_t mlp_grad_impl(const float *x, const float *y, uint32_t m, con
     float *H1 = buf, *G1 = H1 + (size_t)m * SJ_HID, *H2 = G1 + (size_t)m * SJ_HID, *G2 = H2 + (size_t)m * SJ_HID,
           *G3 = G2 + (size_t)m * SJ_HID;
     cudaMemsetAsync(lossOut, 0, sizeof(float), s);
-    k_mlp_backprop<<<(m + 127) / 128, 128, 0, s>>>(x, y, m, w, H1, G1, H2, G2, G3, lossOut);
-    k_mlp_wgrad<<<(NP + 255) / 256, 256, 0, s>>>(x, H1, H2, G1, G2, G3, m, grad);
+    k_mlp_backprop<<<(m + 127) / 128, 128, 0, s>>>(x, y, m, w, H1, G1, H2, G2, G3, lossOut); sj_note_launch();
+    k_mlp_wgrad<<<(NP + 255) / 256, 256, 0, s>>>(x, H1, H2, G1, G2, G3, m, grad); sj_note_launch();
     e = cudaGetLastError();
     cudaFreeAsync(buf, s);
     return e;
@@ -240,6 +240,6 @@ cudaError_t sj_launch_mlp_train_step(const float *x, const float *y, uint32_t m,
 {
     cudaError_t e = mlp_grad_impl(x, y, m, weights, grad, lossOut, s);
     if (e != cudaSuccess) return e;
-    k_adam<<<(NP + 255) / 256, 256, 0, s>>>(weights, grad, adamM, adamV, step, lr);
+    k_adam<<<(NP + 255) / 256, 256, 0, s>>>(weights, grad, adamM, adamV, step, lr); sj_note_launch();
     return cudaGetLastError();
 }

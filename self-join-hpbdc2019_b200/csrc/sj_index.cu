@@ -144,39 +144,39 @@ inline unsigned blocks_for(uint64_t n, unsigned t) { return (unsigned)((n + t - 
 cudaError_t sj_launch_minmax(const double *pts, uint64_t n, int D, double *minmax_dev, cudaStream_t s)
 {
     unsigned long long *mm = (unsigned long long *)minmax_dev;
-    k_minmax_init<<<1, 64, 0, s>>>(mm, D);
+    k_minmax_init<<<1, 64, 0, s>>>(mm, D); sj_note_launch();
     uint64_t blocks = (n + 255) / 256;
     if (blocks > 148 * 8) blocks = 148 * 8;
     if (blocks == 0) blocks = 1;
-    k_minmax<<<(unsigned)blocks, 256, 0, s>>>(pts, n, D, mm);
-    k_minmax_decode<<<1, 64, 0, s>>>(mm, D);
+    k_minmax<<<(unsigned)blocks, 256, 0, s>>>(pts, n, D, mm); sj_note_launch();
+    k_minmax_decode<<<1, 64, 0, s>>>(mm, D); sj_note_launch();
     return cudaGetLastError();
 }
 
 cudaError_t sj_launch_cell_keys(const double *pts, uint64_t n, sj_grid_dev g, uint64_t *keys, uint32_t *vals,
                                 cudaStream_t s)
 {
-    k_cell_keys<<<blocks_for(n, 256), 256, 0, s>>>(pts, n, g, keys, vals);
+    k_cell_keys<<<blocks_for(n, 256), 256, 0, s>>>(pts, n, g, keys, vals); sj_note_launch();
     return cudaGetLastError();
 }
 
 cudaError_t sj_launch_cell_flags(const uint64_t *keys, uint64_t n, uint32_t *flags, cudaStream_t s)
 {
-    k_cell_flags<<<blocks_for(n, 256), 256, 0, s>>>(keys, n, flags);
+    k_cell_flags<<<blocks_for(n, 256), 256, 0, s>>>(keys, n, flags); sj_note_launch();
     return cudaGetLastError();
 }
 
 cudaError_t sj_launch_cell_build(const uint64_t *keys, const uint32_t *cellIdxExcl, uint64_t n, uint32_t *cellStart,
                                  uint64_t *cellLid, cudaStream_t s)
 {
-    k_cell_build<<<blocks_for(n, 256), 256, 0, s>>>(keys, cellIdxExcl, n, cellStart, cellLid);
+    k_cell_build<<<blocks_for(n, 256), 256, 0, s>>>(keys, cellIdxExcl, n, cellStart, cellLid); sj_note_launch();
     return cudaGetLastError();
 }
 
 cudaError_t sj_launch_gather(const double *pts, const uint32_t *ids, uint64_t n, int D, int Dp, double *xs,
                              cudaStream_t s)
 {
-    k_gather<<<blocks_for(n * (uint64_t)Dp, 256), 256, 0, s>>>(pts, ids, n, D, Dp, xs);
+    k_gather<<<blocks_for(n * (uint64_t)Dp, 256), 256, 0, s>>>(pts, ids, n, D, Dp, xs); sj_note_launch();
     return cudaGetLastError();
 }
 
@@ -184,6 +184,6 @@ cudaError_t sj_launch_cell_coords(const uint64_t *cellLid, uint32_t nCells, sj_g
                                   cudaStream_t s)
 {
     if (nCells == 0) return cudaSuccess;
-    k_cell_coords<<<blocks_for(nCells, 256), 256, 0, s>>>(cellLid, nCells, g, coord);
+    k_cell_coords<<<blocks_for(nCells, 256), 256, 0, s>>>(cellLid, nCells, g, coord); sj_note_launch();
     return cudaGetLastError();
 }

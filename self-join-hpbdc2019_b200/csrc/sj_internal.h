@@ -69,6 +69,11 @@ struct sj_join_args {
     double margin;              // FP32 filter half-band on the squared distance
 };
 
+// Kernel launches made by this library since load (every launcher calls
+// sj_note_launch() after each <<<...>>>; bench and tests read the total).
+void sj_note_launch();
+unsigned long long sj_launch_total();
+
 // ---------------------------------------------------------------- launchers
 // primitives (sj_prims.cu)
 size_t sj_scan_temp_bytes(uint64_t n);

@@ -394,6 +394,7 @@ cudaError_t launch_dp(const sj_join_args &a, const sj_grid_dev &g, int fill, int
         if (fill) k_join<DP, false, true><<<grid, SJ_CTA, 0, s>>>(a, g, queue);
         else k_join<DP, false, false><<<grid, SJ_CTA, 0, s>>>(a, g, queue);
     }
+    sj_note_launch();
     return cudaGetLastError();
 }
 

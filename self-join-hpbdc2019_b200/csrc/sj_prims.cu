@@ -1,4 +1,6 @@
 // Device primitives: exclusive scan (u32), stable LSD radix sort, pair-set hash.
+#include <atomic>
+
 #include "sj_internal.h"
 
 namespace {
@@ -107,16 +109,19 @@ cudaError_t scan_rec(const uint32_t *in, uint32_t *out, uint64_t n, uint32_t *te
         return cudaSuccess;
     }
     if (n <= (uint64_t)SCAN_TILE) {
-        k_scan_tile<<<1, SCAN_THREADS, 0, s>>>(in, out, n, nullptr, total_dev);
+        k_scan_tile<<<1, SCAN_THREADS, 0, s>>>(in, out, n, nullptr, total_dev); sj_note_launch();
         return cudaGetLastError();
     }
     uint64_t nb = ceil_div(n, SCAN_TILE);
     uint32_t *sums = temp, *scanned = temp + nb;
-    k_scan_reduce<<<(unsigned)nb, SCAN_THREADS, 0, s>>>(in, n, sums);
+    k_scan_reduce<<<(unsigned)nb, SCAN_THREADS, 0, s>>>(in, n, sums); sj_note_launch();
     cudaError_t e = scan_rec(sums, scanned, nb, temp + 2 * nb, nullptr, s);
     if (e != cudaSuccess) return e;
-    if (total_dev) k_scan_total<<<1, 32, 0, s>>>(scanned, sums, nb, total_dev);
-    k_scan_tile<<<(unsigned)nb, SCAN_THREADS, 0, s>>>(in, out, n, scanned, nullptr);
+    if (total_dev) {
+        k_scan_total<<<1, 32, 0, s>>>(scanned, sums, nb, total_dev);
+        sj_note_launch();
+    }
+    k_scan_tile<<<(unsigned)nb, SCAN_THREADS, 0, s>>>(in, out, n, scanned, nullptr); sj_note_launch();
     return cudaGetLastError();
 }
 
@@ -201,10 +206,10 @@ cudaError_t radix_sort(K *keys, uint32_t *vals, K *keysAlt, uint32_t *valsAlt, u
     uint32_t *vin = vals, *vout = valsAlt;
     int alt = 0;
     for (int shift = 0; shift < bits; shift += 8) {
-        k_radix_hist<K><<<nb, RS_THREADS, 0, s>>>(kin, n, shift, hist, nb);
+        k_radix_hist<K><<<nb, RS_THREADS, 0, s>>>(kin, n, shift, hist, nb); sj_note_launch();
         cudaError_t e = scan_rec(hist, hist, (uint64_t)256 * nb, scanTemp, nullptr, s);
         if (e != cudaSuccess) return e;
-        k_radix_scatter<K><<<nb, RS_THREADS, 0, s>>>(kin, vin, kout, vout, n, shift, hist, nb);
+        k_radix_scatter<K><<<nb, RS_THREADS, 0, s>>>(kin, vin, kout, vout, n, shift, hist, nb); sj_note_launch();
         e = cudaGetLastError();
         if (e != cudaSuccess) return e;
         K *tk = kin; kin = kout; kout = tk;
@@ -246,6 +251,10 @@ __global__ void __launch_bounds__(256) k_hash_pairs(const int32_t *__restrict__ 
 
 }  // namespace
 
+static std::atomic<unsigned long long> g_launches{0};
+void sj_note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+unsigned long long sj_launch_total() { return g_launches.load(std::memory_order_relaxed); }
+
 size_t sj_scan_temp_bytes(uint64_t n) { return scan_temp_elems(n) * sizeof(uint32_t); }
 
 cudaError_t sj_exclusive_scan_u32(const uint32_t *in, uint32_t *out, uint64_t n, void *temp, uint32_t *total_dev,
@@ -278,6 +287,6 @@ cudaError_t sj_hash_pairs(const int32_t *key, const int32_t *val, uint64_t m, un
     if (m == 0) return cudaSuccess;
     uint64_t blocks = ceil_div(m, 256 * 16);
     if (blocks > 148 * 16) blocks = 148 * 16;
-    k_hash_pairs<<<(unsigned)blocks, 256, 0, s>>>(key, val, m, hashOut);
+    k_hash_pairs<<<(unsigned)blocks, 256, 0, s>>>(key, val, m, hashOut); sj_note_launch();
     return cudaGetLastError();
 }

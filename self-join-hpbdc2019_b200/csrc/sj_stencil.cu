@@ -161,6 +161,6 @@ cudaError_t sj_launch_neighbours(const uint64_t *cellLid, const uint32_t *cellCo
 {
     if (nCells == 0) return cudaSuccess;
     k_neighbours<<<(nCells + 127) / 128, 128, 0, s>>>(cellLid, cellCoord, cellStart, nCells, g, pattern, nbrStart,
-                                                      nbrCountOrCell, candFull, feat, pass);
+                                                      nbrCountOrCell, candFull, feat, pass); sj_note_launch();
     return cudaGetLastError();
 }

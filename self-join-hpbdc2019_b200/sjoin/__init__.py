@@ -29,9 +29,9 @@ DELIVER_DEVICE, DELIVER_HOST, DELIVER_NONE = 0, 1, 2
 EXPORTS = [
     "sj_params_default", "sj_create", "sj_destroy", "sj_import_csv", "sj_read_csv", "sj_set_points", "sj_build_index",
     "sj_index_sizes", "sj_index_export", "sj_join", "sj_degrees", "sj_neighbor_table", "sj_free",
-    "sj_get_stats", "sj_mlp_num_params", "sj_set_estimator_weights", "sj_load_estimator",
+    "sj_get_stats", "sj_get_stream", "sj_mlp_num_params", "sj_set_estimator_weights", "sj_load_estimator",
     "sj_cell_features", "sj_mlp_train", "sj_mlp_loss_grad", "sj_mlp_forward", "sj_status_string",
-    "sj_last_error", "sj_version",
+    "sj_last_error", "sj_version", "sj_kernel_launch_count",
 ]
 
 
@@ -56,6 +56,7 @@ class Stats(C.Structure):
         ("ms_upload", C.c_float), ("ms_index", C.c_float), ("ms_tasks", C.c_float), ("ms_estimate", C.c_float),
         ("ms_count", C.c_float), ("ms_scan", C.c_float), ("ms_fill", C.c_float), ("ms_deliver", C.c_float),
         ("ms_total", C.c_float), ("ms_join_kernels", C.c_float), ("ms_fill_kernel", C.c_float),
+        ("kernel_launches", C.c_uint64),
     ]
 
     def as_dict(self) -> dict:
@@ -116,6 +117,7 @@ def load() -> C.CDLL:
     L.sj_free.argtypes = [vp]
     L.sj_free.restype = None
     L.sj_get_stats.argtypes = [vp, C.POINTER(Stats)]
+    L.sj_get_stream.argtypes = [vp, C.POINTER(vp)]
     L.sj_mlp_num_params.restype = u32
     L.sj_set_estimator_weights.argtypes = [vp, vp, u32]
     L.sj_load_estimator.argtypes = [vp, C.c_char_p]
@@ -127,6 +129,7 @@ def load() -> C.CDLL:
     L.sj_status_string.argtypes = [i32]
     L.sj_last_error.restype = C.c_char_p
     L.sj_version.restype = C.c_char_p
+    L.sj_kernel_launch_count.restype = C.c_uint64
     for name in EXPORTS:
         if not hasattr(L, name):
             raise RuntimeError(f"libsj.so lacks {name}")
@@ -152,6 +155,11 @@ def read_csv(path: str, dim: int) -> np.ndarray:
     out = np.zeros((n.value, dim), np.float64)
     _check(L.sj_read_csv(path.encode(), int(dim), _ptr(out), n.value, C.byref(n)))
     return out
+
+
+def kernel_launch_count() -> int:
+    """Kernels libsj has launched since it was loaded."""
+    return int(load().sj_kernel_launch_count())
 
 
 def mlp_num_params() -> int:
@@ -316,6 +324,12 @@ class SelfJoin:
         finally:
             L.sj_free(C.cast(vals, C.c_void_p))
         return rows, v
+
+    def stream(self) -> int:
+        """cudaStream_t of this context (for CUDA events around its work)."""
+        s = C.c_void_p()
+        _check(load().sj_get_stream(self._h, C.byref(s)))
+        return int(s.value or 0)
 
     def stats(self) -> Stats:
         s = Stats()

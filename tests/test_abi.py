@@ -12,7 +12,7 @@ from conftest import REPO, has_gpu
 
 def _declared():
     text = open(os.path.join(REPO, "include", "sj.h")).read()
-    return sorted(set(re.findall(r"^\s*(?:sj_status|void|uint32_t|const char \*)\s*\*?\s*(sj_[a-z0-9_]+)\s*\(",
+    return sorted(set(re.findall(r"^\s*(?:sj_status|void|uint32_t|uint64_t|const char \*)\s*\*?\s*(sj_[a-z0-9_]+)\s*\(",
                                  text, re.M)))
 
 
