@@ -260,9 +260,18 @@ def run_ours(args):
         return
     peak, peak_kind = _peaks()
     s = stats[-1]
-    fill_ms = s["ms_fill_kernel"]
-    achieved = (pairs * 8) / (fill_ms / 1e3) / 1e9 if fill_ms > 0 else None
-    traffic = FILL_TRAFFIC_BYTES_PER_PAIR * pairs / max(1, s["num_batches"]) if FILL_TRAFFIC_BYTES_PER_PAIR else None
+    nb = max(1, s["num_batches"])
+    # per-stage device time (CUDA events around every launch) and algorithmic bytes
+    stages = {
+        "fill": (s["ms_fill_kernel"], 4 * pairs, "k_join fill pass: pair values to their row slots"),
+        "expand": (s["ms_expand"], 4 * pairs + 12 * spec["n"] * nb, "k_expand_keys: key array from row offsets"),
+        "hash": (s["ms_deliver"], 8 * pairs, "k_hash_pairs_dev: consumer fold of every batch"),
+        "count": (s["ms_count"], 0, "k_join count pass"),
+    }
+    top = max(("fill", "expand", "hash"), key=lambda k2: stages[k2][0])
+    t_ms, algo_bytes, kdesc = stages[top]
+    achieved = algo_bytes / (t_ms / 1e3) / 1e9 if t_ms > 0 else None
+    traffic = (FILL_TRAFFIC_BYTES_PER_PAIR * pairs / nb) if (FILL_TRAFFIC_BYTES_PER_PAIR and top == "fill") else None
     cpu = None
     if not args.no_cpu:
         rate, cores, sample, _ = cpu_oracle_rate(pts, eps, k, target_s=args.cpu_seconds)
@@ -273,13 +282,13 @@ def run_ours(args):
         "scaling": "weak", "vs_baseline": None, "dtype": "f64" if prec == 0 else "f32+f64",
         "data": "synthetic (seeded generator, same shapes and distributions)", "config": _config(args, spec),
         "time_s": job_ms / 1e3, "pairs_per_step": pairs, "pair_hash": s["pair_hash"],
-        "roofline": {"bound": "hbm", "kernel": "k_join fill pass (pair writes)", "achieved": achieved,
-                     "peak": peak, "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
-                     "peak_kind": peak_kind, "algorithmic_bytes_per_pair": 8,
-                     "traffic": traffic, "launches": s["num_batches"]},
+        "roofline": {"bound": "hbm", "kernel": kdesc, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": (achieved / peak) if achieved else None, "peak_kind": peak_kind,
+                     "algorithmic_bytes_per_launch": algo_bytes / nb, "launches": nb, "traffic": traffic,
+                     "stage_ms": {k2: round(v[0], 3) for k2, v in stages.items()}},
         "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clocks,
         "phases_ms": {k2: round(s[k2], 3) for k2 in ("ms_index", "ms_tasks", "ms_estimate", "ms_count", "ms_scan",
-                                                     "ms_fill", "ms_deliver", "ms_total")},
+                                                     "ms_fill", "ms_expand", "ms_deliver", "ms_total")},
         "batches": s["num_batches"], "overflow_retries": s["overflow_retries"],
         "distance_calcs": s["distance_calcs"], "full_stencil_calcs": s["full_stencil_calcs"],
         "refined_pairs": s["refined_pairs"], "step_ms": step_ms,

@@ -106,6 +106,7 @@ typedef struct {
     float ms_join_kernels;      /* count + fill kernel time */
     float ms_fill_kernel;       /* fill kernel time alone */
     uint64_t kernel_launches;   /* this library's kernel launches during the last join */
+    float ms_expand;            /* key-array expansion from the batch row structure */
 } sj_stats;
 
 /* Fill `p` with params.h defaults: D=k=2, BLOCKSIZE 256, THREADPERPOINT 1,

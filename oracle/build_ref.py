@@ -8,9 +8,18 @@ generated params.h: the compiler resolves quoted includes relative to the
 link's directory and therefore picks up that params.h.
 
 Per configuration (GPUNUMDIM, NUMINDEXEDDIM, SORT_BY_WORKLOAD) it produces
-  _ref/ref_dump_D{D}_K{k}_S{s}      one reference kernel, single batch, raw pairs
-  _ref/ref_pipeline_D{D}_K{k}_S{s}  the reference's batched pipeline, timed
-  _ref/ref_import_D{D}              the reference's CSV import (CPU only)
+  _ref/ref_dump_D{D}_K{k}_S{s}{v}      one reference kernel, single batch, raw pairs
+  _ref/ref_pipeline_D{D}_K{k}_S{s}{v}  the reference's batched pipeline, timed
+  _ref/ref_import_D{D}                 the reference's CSV import (CPU only)
+
+Variant v = "" is the reference exactly as shipped.  With nvcc 12.9 its device
+code finds no grid cell at all: every cell lookup is a thrust::binary_search
+whose comparison calls gridCellLookup::operator< (structs.h:91), a host-only
+member, so on the device every kernel emits zero pairs (measured on a B200).
+Variant v = "_hd" differs in that one declaration only: its structs.h is
+generated here from the original with `__host__ __device__` added to that
+operator, which is what the device code needs to compare cells.  Every other
+file is the original, linked in place.
 Flags follow the reference makefile (makefile:13) with the architecture set
 to sm_100a.  The reference cannot run without a GPU; the binaries travel to
 the GPU box with the repository snapshot.
@@ -28,8 +37,11 @@ REFERENCE = os.environ.get("SJ_REFERENCE", "/root/reference")
 NVCC = os.path.join(os.environ.get("CUDA_HOME", "/usr/local/cuda"), "bin", "nvcc")
 REF_FILES = ["GPU.cu", "GPU.h", "import_dataset.cpp", "kernel.cu", "kernel.h", "kernelloops.h", "main.cu",
              "stamploops.h", "stamploopsV2.h", "stamploopsSortingCells.h", "structs.h"]
-# (GPUNUMDIM, NUMINDEXEDDIM, SORT_BY_WORKLOAD)
-CONFIGS = [(2, 2, 0), (2, 2, 1), (3, 3, 0), (4, 4, 0), (6, 6, 0), (16, 6, 0), (5, 3, 0)]
+# (GPUNUMDIM, NUMINDEXEDDIM, SORT_BY_WORKLOAD, variant)
+CONFIGS = [(2, 2, 0, ""), (2, 2, 0, "_hd"), (2, 2, 1, "_hd"), (3, 3, 0, "_hd"), (4, 4, 0, "_hd"),
+           (6, 6, 0, "_hd"), (16, 6, 0, "_hd"), (5, 3, 0, "_hd")]
+HD_FROM = "bool operator<(const gridCellLookup & other) const"
+HD_TO = "__host__ __device__ bool operator<(const gridCellLookup & other) const"
 FLAGS = ["-std=c++14", "-O3", "-Xcompiler", "-fopenmp", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo",
          "-D_MWAITXINTRIN_H_INCLUDED", "-D_FORCE_INLINES", "-w"]
 
@@ -55,11 +67,22 @@ def _run(cmd):
         raise RuntimeError("failed: " + " ".join(cmd) + "\n" + r.stderr[-3000:])
 
 
-def _farm(d, k, s) -> str:
-    src = os.path.join(OUT, f"src_D{d}_K{k}_S{s}")
+def _farm(d, k, s, v="") -> str:
+    src = os.path.join(OUT, f"src_D{d}_K{k}_S{s}{v}")
     os.makedirs(src, exist_ok=True)
     for f in REF_FILES:
         link = os.path.join(src, f)
+        if v == "_hd" and f == "structs.h":
+            text = open(os.path.join(REFERENCE, f)).read()
+            if text.count(HD_FROM) != 1:
+                raise RuntimeError("structs.h: comparison operator not found")
+            text = text.replace(HD_FROM, HD_TO)
+            if os.path.islink(link):
+                os.remove(link)
+            if not os.path.exists(link) or open(link).read() != text:
+                with open(link, "w") as fh:
+                    fh.write(text)
+            continue
         if not os.path.islink(link):
             if os.path.exists(link):
                 os.remove(link)
@@ -76,9 +99,9 @@ def _stale(target, deps):
     return not os.path.exists(target) or any(os.path.getmtime(x) > os.path.getmtime(target) for x in deps)
 
 
-def build_config(d, k, s, force=False):
-    src = _farm(d, k, s)
-    tag = f"D{d}_K{k}_S{s}"
+def build_config(d, k, s, v="", force=False):
+    src = _farm(d, k, s, v)
+    tag = f"D{d}_K{k}_S{s}{v}"
     objs = {}
     deps = [os.path.join(src, f) for f in REF_FILES] + [os.path.join(src, "params.h")]
     for name, extra in (("kernel.cu", []), ("GPU.cu", []), ("main.cu", ["-Dmain=sjref_reference_main"]),
@@ -113,10 +136,10 @@ def build(force=False, configs=None) -> bool:
     return True
 
 
-def binary(kind: str, d: int, k: int, s: int = 0) -> str:
+def binary(kind: str, d: int, k: int, s: int = 0, variant: str = "_hd") -> str:
     if kind == "import":
         return os.path.join(OUT, f"ref_import_D{d}")
-    return os.path.join(OUT, f"ref_{kind}_D{d}_K{k}_S{s}")
+    return os.path.join(OUT, f"ref_{kind}_D{d}_K{k}_S{s}{variant}")
 
 
 if __name__ == "__main__":

@@ -194,6 +194,8 @@ struct Ctx {
     DevBuf<unsigned long long> stat;   // evals, refined, pairs, overflow, hash
     DevBuf<uint32_t> queueHead;
     DevBuf<uint32_t> taskHits;
+    DevBuf<unsigned long long> batchTot;
+    std::vector<cudaEvent_t> events;   // per-batch stage boundaries of the asynchronous phase
     PinBuf pinTotal, pinKey[2], pinVal[2];
     // estimator
     std::vector<float> mlpW;
@@ -244,6 +246,10 @@ sj_status check_params(const sj_params &p)
     }
     if (!(p.sample_rate > 0.0 && p.sample_rate <= 1.0)) {
         set_error("sample_rate must be in (0, 1]");
+        return SJ_ERR_BAD_INPUT;
+    }
+    if (p.batch_capacity_pairs != 0 && p.batch_capacity_pairs < 65536) {
+        set_error("batch_capacity_pairs must be 0 (automatic) or at least 65536");
         return SJ_ERR_BAD_INPUT;
     }
     if (p.alpha < 0.0) {
@@ -493,11 +499,11 @@ sj_status estimate_rates(Ctx &c)
 // indices 0..q-1: only candidates at stream offset >= query index count.
 double diag_evals(uint64_t s0, uint64_t s1, uint64_t q)
 {
-    double e = 0;
-    for (uint64_t i = 0; i < q; i++) {
-        uint64_t lo = std::max(s0, i);
-        if (s1 > lo) e += (double)(s1 - lo);
-    }
+    // sum over i in [0, q) of max(0, s1 - max(s0, i))
+    if (s1 <= s0) return 0.0;
+    double e = (double)std::min(q, s0) * (double)(s1 - s0);
+    const uint64_t a = s0, b = std::min(q, s1);
+    if (b > a) e += (double)(b - a) * (double)s1 - 0.5 * (double)(a + b - 1) * (double)(b - a);
     return e;
 }
 
@@ -519,11 +525,15 @@ sj_status build_tasks(Ctx &c, int pattern, uint64_t cap)
         for (uint32_t q0 = 0; q0 < occ; q0 += SJ_CTA) {
             const uint32_t qc = std::min<uint32_t>(SJ_CTA, occ - q0);
             const uint32_t qBegin = aStart + q0;
-            // chunk length from the predicted pair density of this cell
+            // chunk length from the predicted pair density of this cell, and
+            // never more candidates than keep the worst case (every candidate a
+            // hit, both directions) inside one batch
             double perEval = std::max(rate, 1e-6) * (sym ? 2.0 : 1.0);
             double chunk = pairsPerTask / (perEval * qc);
             uint32_t sChunk = (uint32_t)std::min(65536.0, std::max(256.0, chunk));
-            sChunk = (sChunk / 32) * 32;
+            const uint64_t worst = (uint64_t)cap / ((sym ? 2ULL : 1ULL) * qc);
+            if (sChunk > worst) sChunk = (uint32_t)worst;
+            sChunk = std::max<uint32_t>(32, (sChunk / 32) * 32);
             for (uint32_t g0 = 0; g0 < nSegAll; g0 += SJ_MAX_SEG) {
                 const uint32_t gc = std::min<uint32_t>(SJ_MAX_SEG, nSegAll - g0);
                 uint64_t homeLen = 0, L = 0;
@@ -663,6 +673,7 @@ sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
     CK(c.stat.ensure(8));
     CK(c.queueHead.ensure(1));
     CK(c.taskHits.ensure(nt ? nt : 1));
+    CK(cudaMemsetAsync(c.taskHits.p, 0, sizeof(uint32_t) * (nt ? nt : 1), c.s));
     CK(c.pinTotal.ensure(64));
     CK(cudaMemsetAsync(c.stat.p, 0, sizeof(unsigned long long) * 8, c.s));
     double predTotal = 0;
@@ -704,71 +715,158 @@ sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
     std::vector<uint32_t> hTaskHits(nt);
     uint64_t pairsTotal = 0, batches = 0, retries = 0;
     double relErrSum = 0;
-    float msCount = 0, msScan = 0, msFill = 0, msDeliver = 0;
-    Timer tb;
+    float msCount = 0, msScan = 0, msFill = 0, msDeliver = 0, msExpand = 0;
     int pinSel = 0;
     sj_status result = SJ_OK;
-    while (!plan.empty()) {
-        BatchRange br = plan.back();
-        plan.pop_back();
+    CK(c.batchTot.ensure(plan.size() + 1));
+    CK(cudaMemsetAsync(c.batchTot.p, 0, sizeof(unsigned long long) * (plan.size() + 1), c.s));
+    CK(cudaMemsetAsync(c.keyCount.p, 0, sizeof(uint32_t) * n, c.s));   // expand_keys re-zeroes it per batch
+    auto predOf = [&](const BatchRange &br) {
+        double p = 0;
+        for (uint32_t t = br.t0; t < br.t1; t++) p += c.taskPred[t];
+        return p;
+    };
+
+    // ---- asynchronous phase: batches folded on the device (no host delivery).
+    // Every batch runs count -> scan -> fill -> key expansion -> hash without
+    // a host round trip; a batch whose count exceeds the output buffer skips
+    // its fill and is re-run below, split.
+    std::vector<BatchRange> stack;
+    if (delivery == SJ_DELIVER_NONE && !plan.empty()) {
+        double maxPred = 0;
+        for (const BatchRange &br : plan) maxPred = std::max(maxPred, predOf(br) * (1.0 + c.p.alpha));
+        uint64_t bufCap = std::min<uint64_t>(cap, (uint64_t)(1.25 * maxPred) + 65536);
+        if (bufCap > c.outKey.n) {
+            CK(c.outKey.ensure(bufCap));
+            CK(c.outVal.ensure(bufCap));
+        }
+        bufCap = c.outKey.n;
+        a.outKey = c.outKey.p;
+        a.outVal = c.outVal.p;
+        a.capacity = bufCap;
+        const size_t nplan = plan.size();
+        while (c.events.size() < 6 * nplan) {
+            cudaEvent_t e;
+            CK(cudaEventCreate(&e));
+            c.events.push_back(e);
+        }
+        cudaEvent_t *ev = c.events.data();
+        for (size_t i = 0; i < nplan; i++) {
+            const BatchRange &br = plan[nplan - 1 - i];   // plan is stored as a stack
+            a.taskBegin = br.t0;
+            a.taskEnd = br.t1;
+            a.batchPairs = c.batchTot.p + i;
+            CK(cudaEventRecord(ev[6 * i + 0], c.s));
+            CKS(run_pass(c, a, false, queue));
+            CK(cudaEventRecord(ev[6 * i + 1], c.s));
+            CK(sj_exclusive_scan_u32(c.keyCount.p, c.keyCursor.p, n, c.scanTemp.p, c.total.p, c.s));
+            CK(cudaEventRecord(ev[6 * i + 2], c.s));
+            CKS(run_pass(c, a, true, queue));
+            CK(cudaEventRecord(ev[6 * i + 3], c.s));
+            CK(sj_expand_keys(c.keyCount.p, c.keyCursor.p, n, c.outKey.p, a.batchPairs, bufCap, c.s));
+            CK(cudaEventRecord(ev[6 * i + 4], c.s));
+            CK(sj_hash_pairs_dev(c.outKey.p, c.outVal.p, a.batchPairs, bufCap, bufCap, c.stat.p + 4, c.s));
+            CK(cudaEventRecord(ev[6 * i + 5], c.s));
+        }
+        std::vector<unsigned long long> tot(nplan);
+        CK(cudaMemcpyAsync(tot.data(), c.batchTot.p, sizeof(unsigned long long) * nplan, cudaMemcpyDeviceToHost,
+                           c.s));
+        CK(cudaMemcpyAsync(hTaskHits.data(), c.taskHits.p, sizeof(uint32_t) * nt, cudaMemcpyDeviceToHost, c.s));
+        CK(cudaStreamSynchronize(c.s));
+        for (size_t i = 0; i < nplan; i++) {
+            float t01, t12, t23, t34, t45;
+            cudaEventElapsedTime(&t01, ev[6 * i + 0], ev[6 * i + 1]);
+            cudaEventElapsedTime(&t12, ev[6 * i + 1], ev[6 * i + 2]);
+            cudaEventElapsedTime(&t23, ev[6 * i + 2], ev[6 * i + 3]);
+            cudaEventElapsedTime(&t34, ev[6 * i + 3], ev[6 * i + 4]);
+            cudaEventElapsedTime(&t45, ev[6 * i + 4], ev[6 * i + 5]);
+            msCount += t01;
+            msScan += t12;
+            msFill += t23;
+            msExpand += t34;
+            msDeliver += t45;
+        }
+        for (size_t i = 0; i < nplan; i++) {
+            const BatchRange &br = plan[nplan - 1 - i];
+            if (tot[i] > bufCap) {
+                stack.push_back(br);
+                retries++;
+                continue;
+            }
+            if (tot[i] > 0) relErrSum += std::fabs(predOf(br) - (double)tot[i]) / (double)tot[i];
+            pairsTotal += tot[i];
+            batches++;
+        }
+        std::reverse(stack.begin(), stack.end());
+    } else {
+        stack = plan;
+    }
+
+    // ---- synchronous phase: host / device delivery, and batches to re-plan
+    Timer tb;
+    unsigned long long *slot = c.batchTot.p + plan.size();
+    while (!stack.empty() && result == SJ_OK) {
+        BatchRange br = stack.back();
+        stack.pop_back();
         a.taskBegin = br.t0;
         a.taskEnd = br.t1;
-        // count pass
+        a.batchPairs = slot;
+        a.capacity = c.outKey.n;
+        CK(cudaMemsetAsync(slot, 0, sizeof(unsigned long long), c.s));
         tb.start(c.s);
-        CK(cudaMemsetAsync(c.keyCount.p, 0, sizeof(uint32_t) * n, c.s));
         CKS(run_pass(c, a, false, queue));
         msCount += tb.stop(c.s);
         tb.start(c.s);
         CK(sj_exclusive_scan_u32(c.keyCount.p, c.keyCursor.p, n, c.scanTemp.p, c.total.p, c.s));
-        CK(cudaMemcpyAsync(c.pinTotal.p, c.total.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, c.s));
-        msScan += tb.stop(c.s);
-        // scan totals wrap at 2^32: recompute from the exact per-task counts
+        unsigned long long cnt = 0;
+        CK(cudaMemcpyAsync(c.pinTotal.p, slot, sizeof(unsigned long long), cudaMemcpyDeviceToHost, c.s));
         CK(cudaMemcpyAsync(hTaskHits.data() + br.t0, c.taskHits.p + br.t0, sizeof(uint32_t) * (br.t1 - br.t0),
                            cudaMemcpyDeviceToHost, c.s));
-        CK(cudaStreamSynchronize(c.s));
-        uint64_t cnt = 0;
-        for (uint32_t t = br.t0; t < br.t1; t++) cnt += hTaskHits[t];
+        msScan += tb.stop(c.s);
+        memcpy(&cnt, c.pinTotal.p, sizeof(cnt));
         if (cnt > cap) {
+            // estimate too low: clear the counts and split the batch
+            CK(sj_expand_keys(c.keyCount.p, c.keyCursor.p, n, c.outKey.p, slot, 0, c.s));
             if (br.t1 - br.t0 <= 1) {
                 set_error("a single task produces %llu pairs, more than the batch capacity %llu",
                           (unsigned long long)cnt, (unsigned long long)cap);
                 return SJ_ERR_INTERNAL;
             }
             uint32_t mid = br.t0 + (br.t1 - br.t0) / 2;
-            plan.push_back({mid, br.t1});
-            plan.push_back({br.t0, mid});
+            stack.push_back({mid, br.t1});
+            stack.push_back({br.t0, mid});
             retries++;
             continue;
         }
-        double pred = 0;
-        for (uint32_t t = br.t0; t < br.t1; t++) pred += c.taskPred[t];
-        if (cnt > 0) relErrSum += std::fabs(pred - (double)cnt) / (double)cnt;
+        if (cnt > 0) relErrSum += std::fabs(predOf(br) - (double)cnt) / (double)cnt;
         // output buffers follow the exact batch size (grow-only, 25% headroom, <= capacity)
         if (cnt > c.outKey.n) {
             uint64_t want = std::min<uint64_t>(cap, std::max<uint64_t>(cnt, (uint64_t)(1.25 * (double)c.outKey.n)));
             CK(c.outKey.ensure(want));
             CK(c.outVal.ensure(want));
         }
-        if (delivery == SJ_DELIVER_HOST && cnt * sizeof(int32_t) > c.pinKey[pinSel].bytes) {
-            size_t want = std::max<size_t>(cnt * sizeof(int32_t), (size_t)(1.25 * (double)c.pinKey[pinSel].bytes));
-            want = std::min<size_t>(want, cap * sizeof(int32_t));
-            CK(c.pinKey[pinSel].ensure(want));
-            CK(c.pinVal[pinSel].ensure(want));
-        }
         a.outKey = c.outKey.p;
         a.outVal = c.outVal.p;
         a.capacity = c.outKey.n;
-        // fill pass
         tb.start(c.s);
         CKS(run_pass(c, a, true, queue));
         msFill += tb.stop(c.s);
+        tb.start(c.s);
+        CK(sj_expand_keys(c.keyCount.p, c.keyCursor.p, n, c.outKey.p, slot, a.capacity, c.s));
+        msExpand += tb.stop(c.s);
         tb.start(c.s);
         CK(sj_hash_pairs(c.outKey.p, c.outVal.p, cnt, c.stat.p + 4, c.s));
         if (delivery == SJ_DELIVER_DEVICE && cb) {
             CK(cudaStreamSynchronize(c.s));
             sj_batch b{batches, cnt, c.outKey.p, c.outVal.p, 1};
-            if (cb(&b, user)) { result = SJ_ERR_ABORTED; }
+            if (cb(&b, user)) result = SJ_ERR_ABORTED;
         } else if (delivery == SJ_DELIVER_HOST) {
+            if (cnt * sizeof(int32_t) > c.pinKey[pinSel].bytes) {
+                size_t want = std::max<size_t>(cnt * sizeof(int32_t), (size_t)(1.25 * (double)c.pinKey[pinSel].bytes));
+                want = std::min<size_t>(want, cap * sizeof(int32_t));
+                CK(c.pinKey[pinSel].ensure(want));
+                CK(c.pinVal[pinSel].ensure(want));
+            }
             int32_t *hk = (int32_t *)c.pinKey[pinSel].p, *hv = (int32_t *)c.pinVal[pinSel].p;
             if (cnt) {
                 CK(cudaMemcpyAsync(hk, c.outKey.p, cnt * sizeof(int32_t), cudaMemcpyDeviceToHost, c.s));
@@ -777,14 +875,13 @@ sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
             CK(cudaStreamSynchronize(c.s));
             if (cb) {
                 sj_batch b{batches, cnt, hk, hv, 0};
-                if (cb(&b, user)) { result = SJ_ERR_ABORTED; }
+                if (cb(&b, user)) result = SJ_ERR_ABORTED;
             }
             pinSel ^= 1;
         }
         msDeliver += tb.stop(c.s);
         pairsTotal += cnt;
         batches++;
-        if (result != SJ_OK) break;
     }
     unsigned long long hs[8];
     CK(cudaMemcpyAsync(hs, c.stat.p, sizeof(hs), cudaMemcpyDeviceToHost, c.s));
@@ -795,8 +892,8 @@ sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
     }
     c.st.total_pairs = pairsTotal;
     c.st.pair_hash = hs[4];
-    c.st.distance_calcs = hs[0] / 2;   // count + fill passes evaluate the same candidates
-    c.st.refined_pairs = hs[1] / 2;
+    c.st.distance_calcs = hs[0];
+    c.st.refined_pairs = hs[1];
     c.st.num_batches = batches;
     c.st.overflow_retries = retries;
     c.st.estimator_mean_abs_rel_err = batches ? relErrSum / (double)batches : 0.0;
@@ -814,6 +911,7 @@ sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
     c.st.ms_deliver = msDeliver;
     c.st.ms_join_kernels = msCount + msFill;
     c.st.ms_fill_kernel = msFill;
+    c.st.ms_expand = msExpand;
     c.st.ms_total = total.stop(c.s);
     c.st.kernel_launches = sj_launch_total() - launches0;
     return result;
@@ -968,6 +1066,7 @@ sj_status sj_destroy(void *ctx)
     cudaSetDevice(c->dev);
     cudaStreamSynchronize(c->s);
     cudaStream_t s = c->s;
+    for (cudaEvent_t e : c->events) cudaEventDestroy(e);
     delete c;
     if (s) cudaStreamDestroy(s);
     return SJ_OK;

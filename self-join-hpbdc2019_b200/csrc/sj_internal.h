@@ -64,7 +64,9 @@ struct sj_join_args {
     uint32_t *keyCursor;        // fill pass: per point-id write cursors (exclusive offsets)
     int32_t *outKey, *outVal;   // fill pass output
     uint64_t capacity;          // pairs the output buffers hold
-    unsigned long long *stat;   // [0] evals, [1] refined, [2] hits(count pass), [3] overflow flag
+    unsigned long long *stat;   // [0] evals, [1] refined, [2] pairs (count pass), [3] run past capacity,
+                                // [4] set hash, [5] batches skipped for overflow
+    unsigned long long *batchPairs;  // this batch's pair total (count pass adds, later passes read)
     uint32_t *taskHits;         // optional per-task measured pairs (count pass)
     double margin;              // FP32 filter half-band on the squared distance
 };
@@ -86,6 +88,13 @@ cudaError_t sj_radix_sort_u32_u32(uint32_t *keys, uint32_t *vals, uint32_t *keys
                                   uint64_t n, int bits, void *temp, int *resultInAlt, cudaStream_t s);
 cudaError_t sj_hash_pairs(const int32_t *key, const int32_t *val, uint64_t m,
                           unsigned long long *hashOut, cudaStream_t s);
+// same, with the pair count read on the device (skipped when it exceeds cap)
+cudaError_t sj_hash_pairs_dev(const int32_t *key, const int32_t *val, const unsigned long long *count, uint64_t cap,
+                              uint64_t gridHint, unsigned long long *hashOut, cudaStream_t s);
+// keys of a batch from its row structure: rows are [cursor-count, cursor) after
+// the fill pass; also clears `count` for the next batch
+cudaError_t sj_expand_keys(uint32_t *count, const uint32_t *cursor, uint64_t n, int32_t *outKey,
+                           const unsigned long long *batchPairs, uint64_t cap, cudaStream_t s);
 
 // index build (sj_index.cu)
 cudaError_t sj_launch_minmax(const double *pts, uint64_t n, int D, double *minmax_dev, cudaStream_t s);

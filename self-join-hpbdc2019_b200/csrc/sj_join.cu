@@ -87,7 +87,6 @@ __global__ void __launch_bounds__(SJ_CTA) k_join(sj_join_args a, sj_grid_dev g, 
     __shared__ uint32_t segStart[SJ_MAX_SEG];
     __shared__ uint32_t segPre[SJ_MAX_SEG + 1];
     __shared__ uint32_t colCnt[FILL ? 1 : NW][FILL ? 1 : S];
-    __shared__ uint32_t qIdS[SJ_CTA];
     __shared__ uint32_t scanTmp[NW];
     __shared__ uint32_t curTask;
     __shared__ unsigned long long taskPairs;
@@ -95,7 +94,14 @@ __global__ void __launch_bounds__(SJ_CTA) k_join(sj_join_args a, sj_grid_dev g, 
     const uint32_t tid = threadIdx.x;
     const uint32_t lane = tid & 31u;
     const uint32_t warp = tid >> 5;
+    const uint32_t ltmask = (1u << lane) - 1u;
     const int D = g.D;
+    // fill pass of a batch whose count exceeded the output buffer: skip it
+    // (the host re-plans it); the count pass always runs
+    if (FILL && a.batchPairs && *a.batchPairs > a.capacity) {
+        if (tid == 0 && blockIdx.x == 0) atomicMax(&a.stat[5], 1ULL);
+        return;
+    }
     const double T = g.thresh;
 
     if (!FILL) {
@@ -175,7 +181,6 @@ __global__ void __launch_bounds__(SJ_CTA) k_join(sj_join_args a, sj_grid_dev g, 
         const bool qValid = qi < task.qCount;
         const uint32_t qpos = task.qBegin + (qValid ? qi : 0u);
         const uint32_t qid = a.ids[qpos];
-        qIdS[tid] = qid;
         double q64[F32 ? 1 : DP];
         float q2[F32 ? DP : 1];
         float thrLo = 0.f, thrHi = 0.f;
@@ -299,45 +304,49 @@ __global__ void __launch_bounds__(SJ_CTA) k_join(sj_join_args a, sj_grid_dev g, 
                     }
                 }
                 evals += __popc(rowValid);
-                const uint32_t rowMask = hits & rowValid;
-                const uint32_t mirMask = transpose32(hits & mirValid, lane);
+                const uint32_t rowMask = hits & rowValid;   // lane = query, bit = candidate
+                const uint32_t mirRow = hits & mirValid;    // pairs also emitted with the candidate as key
                 if (FILL) {
-                    uint32_t n = __popc(rowMask);
-                    if (n) {
-                        uint32_t p = atomicAdd(&a.keyCursor[qid], n);
-                        if ((uint64_t)p + n <= a.capacity) {
-                            uint32_t m = rowMask;
-                            while (m) {
-                                int b = __ffs(m) - 1;
-                                m &= m - 1;
-                                a.outKey[p] = (int32_t)qid;
-                                a.outVal[p] = (int32_t)candId[jb + b];
-                                p++;
-                            }
-                        } else {
-                            atomicMax(&a.stat[3], 1ULL);
-                        }
+                    // rowT / mirT: lane j holds, for candidate jb+j, the bit mask of
+                    // this warp's queries it pairs with (one transpose suffices
+                    // outside the home diagonal, where both masks agree)
+                    const bool diag = sym && (blk < homeEnd);
+                    const uint32_t rowT = transpose32(rowMask, lane);
+                    const uint32_t mirT = sym ? (diag ? transpose32(mirRow, lane) : rowT) : 0u;
+                    const uint32_t cidL = candId[jb + lane];
+                    const uint32_t nRow = __popc(rowMask), nCol = __popc(mirT);
+                    uint32_t pRow = 0, pCol = 0;
+                    if (nRow) pRow = atomicAdd(&a.keyCursor[qid], nRow);
+                    if (nCol) pCol = atomicAdd(&a.keyCursor[cidL], nCol);
+                    // positions come from the counted offsets; a run past the end
+                    // would mean the two passes disagree
+                    const bool okRow = (uint64_t)pRow + nRow <= a.capacity;
+                    const bool okCol = (uint64_t)pCol + nCol <= a.capacity;
+                    if (!okRow || !okCol) atomicMax(&a.stat[3], 1ULL);
+                    // one coalesced run per key: row runs (key = query L, values =
+                    // candidates in lane order), then column runs (key = candidate j,
+                    // values = queries in lane order)
+                    uint32_t live = __ballot_sync(0xffffffffu, nRow != 0 && okRow);
+                    while (live) {
+                        const int L = __ffs(live) - 1;
+                        live &= live - 1;
+                        const uint32_t base = __shfl_sync(0xffffffffu, pRow, L);
+                        const bool h = (rowT >> L) & 1u;
+                        const uint32_t b = __ballot_sync(0xffffffffu, h);
+                        if (h) a.outVal[base + __popc(b & ltmask)] = (int32_t)cidL;
                     }
-                    uint32_t nm = __popc(mirMask);
-                    if (nm) {
-                        uint32_t cid = candId[jb + lane];
-                        uint32_t p = atomicAdd(&a.keyCursor[cid], nm);
-                        if ((uint64_t)p + nm <= a.capacity) {
-                            uint32_t m = mirMask;
-                            while (m) {
-                                int b = __ffs(m) - 1;
-                                m &= m - 1;
-                                a.outKey[p] = (int32_t)cid;
-                                a.outVal[p] = (int32_t)qIdS[warp * 32 + b];
-                                p++;
-                            }
-                        } else {
-                            atomicMax(&a.stat[3], 1ULL);
-                        }
+                    live = __ballot_sync(0xffffffffu, nCol != 0 && okCol);
+                    while (live) {
+                        const int j = __ffs(live) - 1;
+                        live &= live - 1;
+                        const uint32_t base = __shfl_sync(0xffffffffu, pCol, j);
+                        const bool h = (mirRow >> j) & 1u;
+                        const uint32_t b = __ballot_sync(0xffffffffu, h);
+                        if (h) a.outVal[base + __popc(b & ltmask)] = (int32_t)qid;
                     }
                 } else {
                     rowCount += __popc(rowMask);
-                    if (sym) colCnt[warp][jb + lane] += __popc(mirMask);
+                    if (sym) colCnt[warp][jb + lane] += __popc(transpose32(mirRow, lane));
                 }
             }
             if (!FILL && sym) {
@@ -365,14 +374,17 @@ __global__ void __launch_bounds__(SJ_CTA) k_join(sj_join_args a, sj_grid_dev g, 
             e += __shfl_xor_sync(0xffffffffu, e, o);
             r += __shfl_xor_sync(0xffffffffu, r, o);
         }
-        if (lane == 0) {
+        if (FILL && lane == 0) {   // each task is filled exactly once
             if (e) atomicAdd(&a.stat[0], e);
             if (r) atomicAdd(&a.stat[1], r);
         }
         if (!FILL) {
             __syncthreads();
             if (tid == 0) {
-                if (taskPairs) atomicAdd(&a.stat[2], taskPairs);
+                if (taskPairs) {
+                    atomicAdd(&a.stat[2], taskPairs);
+                    if (a.batchPairs) atomicAdd(a.batchPairs, taskPairs);
+                }
                 if (a.taskHits) a.taskHits[t] = (uint32_t)min(taskPairs, 0xffffffffULL);
             }
         }

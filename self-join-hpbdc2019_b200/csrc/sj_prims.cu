@@ -249,7 +249,86 @@ __global__ void __launch_bounds__(256) k_hash_pairs(const int32_t *__restrict__ 
     }
 }
 
+__global__ void __launch_bounds__(256) k_hash_pairs_dev(const int32_t *__restrict__ key,
+                                                        const int32_t *__restrict__ val,
+                                                        const unsigned long long *__restrict__ count, uint64_t cap,
+                                                        unsigned long long *out)
+{
+    const unsigned long long m = *count;
+    if (m > cap) return;
+    unsigned long long h = 0;
+    uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += stride) {
+        unsigned long long z = ((unsigned long long)(uint32_t)key[i] << 32) | (uint32_t)val[i];
+        h += splitmix64(z);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) h += __shfl_xor_sync(0xffffffffu, h, o);
+    __shared__ unsigned long long ws[8];
+    if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = h;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long t = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += ws[w];
+        if (t) atomicAdd(out, t);
+    }
+}
+
+// Block per 256 keys: the keys' rows are consecutive in the batch (their
+// offsets came from one exclusive scan over ascending ids), so the block
+// writes the key of every position in its span, coalesced.
+__global__ void __launch_bounds__(256) k_expand_keys(uint32_t *__restrict__ count, const uint32_t *__restrict__ cursor,
+                                                     uint64_t n, int32_t *__restrict__ outKey,
+                                                     const unsigned long long *__restrict__ batchPairs, uint64_t cap)
+{
+    __shared__ uint32_t sStart[256];
+    __shared__ uint32_t sEnd[256];
+    const uint64_t k = (uint64_t)blockIdx.x * 256 + threadIdx.x;
+    uint32_t c = 0, e = 0;
+    if (k < n) {
+        c = count[k];
+        e = cursor[k];
+        count[k] = 0;
+    }
+    const bool write = *batchPairs <= cap;
+    sStart[threadIdx.x] = e - c;
+    sEnd[threadIdx.x] = e;
+    __syncthreads();
+    if (!write) return;
+    const uint64_t left = n - (uint64_t)blockIdx.x * 256;
+    const int nk = left < 256 ? (int)left : 256;
+    const uint32_t lo = sStart[0], hi = sEnd[nk - 1];
+    for (uint32_t pos = lo + threadIdx.x; pos < hi; pos += 256) {
+        int a = 0, b = nk - 1;        // last key whose row starts at or before pos
+        while (a < b) {
+            int mid = (a + b + 1) >> 1;
+            if (sStart[mid] <= pos) a = mid; else b = mid - 1;
+        }
+        outKey[pos] = (int32_t)((uint64_t)blockIdx.x * 256 + a);
+    }
+}
+
 }  // namespace
+
+cudaError_t sj_hash_pairs_dev(const int32_t *key, const int32_t *val, const unsigned long long *count, uint64_t cap,
+                              uint64_t gridHint, unsigned long long *hashOut, cudaStream_t s)
+{
+    uint64_t blocks = ceil_div(gridHint ? gridHint : 1, 256 * 16);
+    if (blocks > 148 * 16) blocks = 148 * 16;
+    if (blocks == 0) blocks = 1;
+    k_hash_pairs_dev<<<(unsigned)blocks, 256, 0, s>>>(key, val, count, cap, hashOut);
+    sj_note_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t sj_expand_keys(uint32_t *count, const uint32_t *cursor, uint64_t n, int32_t *outKey,
+                           const unsigned long long *batchPairs, uint64_t cap, cudaStream_t s)
+{
+    if (n == 0) return cudaSuccess;
+    k_expand_keys<<<(unsigned)ceil_div(n, 256), 256, 0, s>>>(count, cursor, n, outKey, batchPairs, cap);
+    sj_note_launch();
+    return cudaGetLastError();
+}
 
 static std::atomic<unsigned long long> g_launches{0};
 void sj_note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }

@@ -2,8 +2,10 @@
 
 For each small seeded case this writes the dataset as CSV, runs the reference's
 own import (oracle/_ref/ref_import_D*) to get its point order, then runs the
-reference's own join kernels (oracle/_ref/ref_dump_*; modes 3 full stencil,
-4 Unicomp, 5 B-Unicomp, 6 linear-ID Unicomp, single batch, SORT_BY_WORKLOAD 0)
+reference's own join kernels (oracle/_ref/ref_dump_*_hd; modes 3 full stencil,
+4 Unicomp, 5 B-Unicomp, 6 linear-ID Unicomp, single batch, SORT_BY_WORKLOAD 0;
+the _hd build is the reference with its cell comparison operator made callable
+on the device, see oracle/build_ref.py)
 and stores, per case, an .npz with
     pts      the points in the reference's id order (float64)
     eps, k   search radius and indexed dimensions
@@ -71,6 +73,13 @@ def run_case(name, out_dir, tmp):
     n = struct.unpack("<Q", raw[:8])[0]
     ref_pts = np.frombuffer(raw[8:], np.float64).reshape(n, D).copy()
     rec = dict(pts=ref_pts, eps=np.float64(eps), k=np.int64(k))
+    if D == 2 and k == 2:
+        # the reference exactly as shipped: record what it emits (zero pairs
+        # with nvcc 12.9, its device cell lookups never match)
+        exe = build_ref.binary("dump", D, k, 0, variant="")
+        out = os.path.join(tmp, f"{name}_asis.bin")
+        subprocess.check_call([exe, csv, repr(eps), "3", out], stdout=subprocess.DEVNULL)
+        rec["asis_mode3_count"] = np.int64(struct.unpack("<Q", open(out, "rb").read()[:8])[0])
     for m in modes:
         exe = build_ref.binary("dump", D, k, 0)
         out = os.path.join(tmp, f"{name}_{m}.bin")

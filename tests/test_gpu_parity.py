@@ -91,7 +91,7 @@ def test_all_modes_match_oracle(name, prec):
 @pytest.mark.parametrize("mode", [3, 5, 6, 10])
 def test_multi_batch_with_overflow_retries(mode, prec):
     pts, eps, k, ix, (ok, ov) = _oracle_pairs("exp2d_dense")
-    cap = 20000
+    cap = 65536
     # alpha 0 and a tiny sample make underestimates (and so retries) likely
     batches, st = _run(pts, eps, k, mode, prec, capacity=cap, alpha=0.0, sample_rate=0.002)
     _check_batches(batches, cap)
@@ -105,7 +105,7 @@ def test_full_stencil_batches_hold_complete_rows():
     # with the full stencil every key is produced by one task's query tile, and
     # the count pass places all of a key's values together
     pts, eps, k, ix, (ok, ov) = _oracle_pairs("uniform2d")
-    batches, _ = _run(pts, eps, k, 3, sjoin.PREC_FP64, capacity=50000)
+    batches, _ = _run(pts, eps, k, 3, sjoin.PREC_FP64, capacity=65536)
     seen = set()
     for key, val in batches:
         ks = set(np.unique(key).tolist())
@@ -132,7 +132,7 @@ def test_degrees_match_oracle(mode):
 
 def test_neighbor_table_rows():
     pts, eps, k, ix, (ok, ov) = _oracle_pairs("exp2d_dense")
-    with sjoin.SelfJoin(2, eps, mode=10, capacity=30000) as sj:
+    with sjoin.SelfJoin(2, eps, mode=10, capacity=65536) as sj:
         sj.set_points(pts)
         sj.build_index()
         rows, vals = sj.neighbor_table()
