@@ -24,8 +24,8 @@
  *                                          filter only drops coordinates that no point
  *                                          occupies, so it never changes the pair set.
  *   distance             kernel.cu:344-349  acc += (cand[l]-query[l])^2 over all GPUNUMDIM
- *                                          dims, in dim order; nvcc contracts the update to
- *                                          acc = fma(d, d, acc) (fma_mode=1, the default);
+ *                                          dims, in dim order, in the exact rounding order
+ *                                          of the reference's nvcc build (orc_dist2);
  *                                          emit (query, cand) iff sqrt(acc) <= eps.
  *   output               (key = query id, value = candidate id), self pairs included,
  *                        both orders present; canonical form sorted by (key, value).
@@ -88,13 +88,31 @@ uint64_t orc_hash_pairs(const int32_t *keys, const int32_t *vals, int64_t m)
 
 /* ------------------------------------------------------------- predicate -- */
 
-/* kernel.cu:344-349.  fma_mode 1: acc = fma(d,d,acc) (nvcc default contraction);
- * fma_mode 0: acc = acc + d*d with two roundings (kept to pin the contraction
- * question against the reference's own outputs). */
+/* kernel.cu:344-349: runningTotalDist += (cand[l] - query[l])^2 over l, from 0.
+ * fma_mode 1 (default) is the arithmetic the reference's nvcc build performs,
+ * pinned against its own outputs (tests/golden): the compiler drops the
+ * initial "0 +" and fuses the FIRST product of the first addition,
+ *     acc = fma(d0, d0, d1*d1),  then  acc = fma(dl, dl, acc) for l >= 2
+ * (D == 1: acc = d0*d0).  fma_mode 0 rounds every product and sum separately;
+ * fma_mode 2 is the plain chain acc = fma(dl, dl, acc) from acc = 0.  Both are
+ * kept only to show that the fixtures discriminate between the variants. */
 static inline double orc_dist2(const double *cand, const double *query, int D, int fma_mode)
 {
     double acc = 0.0;
-    if (fma_mode) {
+    if (fma_mode == 1) {
+        double d0 = cand[0] - query[0];
+        if (D == 1) {
+            volatile double sq = d0 * d0;
+            return sq;
+        }
+        double d1 = cand[1] - query[1];
+        volatile double sq1 = d1 * d1;
+        acc = fma(d0, d0, sq1);
+        for (int l = 2; l < D; l++) {
+            double d = cand[l] - query[l];
+            acc = fma(d, d, acc);
+        }
+    } else if (fma_mode == 2) {
         for (int l = 0; l < D; l++) {
             double d = cand[l] - query[l];
             acc = fma(d, d, acc);

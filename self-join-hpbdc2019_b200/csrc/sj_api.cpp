@@ -515,7 +515,7 @@ sj_status build_tasks(Ctx &c, int pattern, uint64_t cap)
     c.tasks.clear();
     c.taskPred.clear();
     c.taskEvals.clear();
-    const double pairsPerTask = std::max(4096.0, (double)cap / 1024.0);
+    const double pairsPerTask = std::max(4096.0, (double)cap / 4096.0);
     for (uint32_t A = 0; A < c.nCells; A++) {
         const uint32_t aStart = c.hCellStart[A], aEnd = c.hCellStart[A + 1];
         const uint32_t occ = aEnd - aStart;
@@ -720,7 +720,7 @@ sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
     sj_status result = SJ_OK;
     CK(c.batchTot.ensure(plan.size() + 1));
     CK(cudaMemsetAsync(c.batchTot.p, 0, sizeof(unsigned long long) * (plan.size() + 1), c.s));
-    CK(cudaMemsetAsync(c.keyCount.p, 0, sizeof(uint32_t) * n, c.s));   // expand_keys re-zeroes it per batch
+    CK(cudaMemsetAsync(c.keyCount.p, 0, sizeof(uint32_t) * n, c.s));   // each scan clears it again
     auto predOf = [&](const BatchRange &br) {
         double p = 0;
         for (uint32_t t = br.t0; t < br.t1; t++) p += c.taskPred[t];
@@ -759,11 +759,10 @@ sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
             CK(cudaEventRecord(ev[6 * i + 0], c.s));
             CKS(run_pass(c, a, false, queue));
             CK(cudaEventRecord(ev[6 * i + 1], c.s));
-            CK(sj_exclusive_scan_u32(c.keyCount.p, c.keyCursor.p, n, c.scanTemp.p, c.total.p, c.s));
+            CK(sj_exclusive_scan_u32_clear(c.keyCount.p, c.keyCursor.p, n, c.scanTemp.p, c.total.p, c.s));
             CK(cudaEventRecord(ev[6 * i + 2], c.s));
             CKS(run_pass(c, a, true, queue));
             CK(cudaEventRecord(ev[6 * i + 3], c.s));
-            CK(sj_expand_keys(c.keyCount.p, c.keyCursor.p, n, c.outKey.p, a.batchPairs, bufCap, c.s));
             CK(cudaEventRecord(ev[6 * i + 4], c.s));
             CK(sj_hash_pairs_dev(c.outKey.p, c.outVal.p, a.batchPairs, bufCap, bufCap, c.stat.p + 4, c.s));
             CK(cudaEventRecord(ev[6 * i + 5], c.s));
@@ -817,7 +816,7 @@ sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
         CKS(run_pass(c, a, false, queue));
         msCount += tb.stop(c.s);
         tb.start(c.s);
-        CK(sj_exclusive_scan_u32(c.keyCount.p, c.keyCursor.p, n, c.scanTemp.p, c.total.p, c.s));
+        CK(sj_exclusive_scan_u32_clear(c.keyCount.p, c.keyCursor.p, n, c.scanTemp.p, c.total.p, c.s));
         unsigned long long cnt = 0;
         CK(cudaMemcpyAsync(c.pinTotal.p, slot, sizeof(unsigned long long), cudaMemcpyDeviceToHost, c.s));
         CK(cudaMemcpyAsync(hTaskHits.data() + br.t0, c.taskHits.p + br.t0, sizeof(uint32_t) * (br.t1 - br.t0),
@@ -825,8 +824,7 @@ sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
         msScan += tb.stop(c.s);
         memcpy(&cnt, c.pinTotal.p, sizeof(cnt));
         if (cnt > cap) {
-            // estimate too low: clear the counts and split the batch
-            CK(sj_expand_keys(c.keyCount.p, c.keyCursor.p, n, c.outKey.p, slot, 0, c.s));
+            // estimate too low: split the batch (the scan already cleared the counts)
             if (br.t1 - br.t0 <= 1) {
                 set_error("a single task produces %llu pairs, more than the batch capacity %llu",
                           (unsigned long long)cnt, (unsigned long long)cap);
@@ -851,9 +849,6 @@ sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
         tb.start(c.s);
         CKS(run_pass(c, a, true, queue));
         msFill += tb.stop(c.s);
-        tb.start(c.s);
-        CK(sj_expand_keys(c.keyCount.p, c.keyCursor.p, n, c.outKey.p, slot, a.capacity, c.s));
-        msExpand += tb.stop(c.s);
         tb.start(c.s);
         CK(sj_hash_pairs(c.outKey.p, c.outVal.p, cnt, c.stat.p + 4, c.s));
         if (delivery == SJ_DELIVER_DEVICE && cb) {

@@ -40,7 +40,7 @@ __global__ void __launch_bounds__(256) k_sample(sj_join_args a, sj_grid_dev g, u
         uint32_t b0 = a.cellStart[B], b1 = a.cellStart[B + 1];
         for (uint32_t c = b0 + lane; c < b1; c += 32) {
             const double *x = a.xs + (uint64_t)c * g.Dp;
-            double acc = 0.0;
+            double acc = 0.0;   // estimate only: plain fma chain
             for (int l = 0; l < g.Dp; l++) {
                 double d = __dsub_rn(x[l], q[l]);
                 acc = __fma_rn(d, d, acc);

@@ -81,6 +81,9 @@ unsigned long long sj_launch_total();
 size_t sj_scan_temp_bytes(uint64_t n);
 cudaError_t sj_exclusive_scan_u32(const uint32_t *in, uint32_t *out, uint64_t n, void *temp,
                                   uint32_t *total_dev, cudaStream_t s);
+// same, and sets every input element to zero after reading it
+cudaError_t sj_exclusive_scan_u32_clear(uint32_t *in, uint32_t *out, uint64_t n, void *temp, uint32_t *total_dev,
+                                        cudaStream_t s);
 size_t sj_radix_temp_bytes(uint64_t n);
 cudaError_t sj_radix_sort_u64_u32(uint64_t *keys, uint32_t *vals, uint64_t *keysAlt, uint32_t *valsAlt,
                                   uint64_t n, int bits, void *temp, int *resultInAlt, cudaStream_t s);

@@ -13,11 +13,13 @@
 // fill pass : keys are placed at exclusive offsets of those counts, so every
 //             key's values land contiguously and keys come out ascending --
 //             the order thrust::sort_by_key gives the reference (GPU.cu:2336)
-//             without sorting.
+//             without sorting.  Each key's share of a 32x32 block is written as
+//             one run by the whole warp (ballot rank -> consecutive addresses).
 //
-// Predicate (kernel.cu:344-349): acc = sum over dims of fma(d,d,acc) with
-// d = cand - query, hit iff sqrt(acc) <= eps, evaluated as acc <= T with T the
-// largest double whose rounded sqrt is <= eps (identical by monotonicity).
+// Predicate (kernel.cu:344-349): the squared distance in the reference build's
+// rounding order (ref_dist2), hit iff sqrt(acc) <= eps, evaluated as acc <= T
+// with T the largest double whose rounded sqrt is <= eps (identical by
+// monotonicity of the correctly rounded square root).
 // FP32 filter: acc32 = |b|^2 + sum(-2 a_l b_l) in local coordinates around the
 // home cell's centre; pairs inside a proven error band of the threshold are
 // re-evaluated with the exact FP64 chain above, so the pair set is the FP64 set.
@@ -44,19 +46,30 @@ __device__ __forceinline__ uint32_t transpose32(uint32_t x, uint32_t lane)
     return x;
 }
 
+// Squared distance in the reference build's exact rounding order (pinned by
+// its own outputs): the first addition fuses the FIRST product,
+//     acc = fma(d0, d0, d1*d1),  then  acc = fma(dl, dl, acc) for l >= 2,
+// with d = cand - query (kernel.cu:344-347).  Padded dimensions hold 0 in both
+// points and fma(0, 0, acc) == acc, so padding never changes the result.
+template <int DP>
+__device__ __forceinline__ double ref_dist2(const double *c, const double *q)
+{
+    const double d0 = __dsub_rn(c[0], q[0]);
+    if (DP == 1) return __dmul_rn(d0, d0);
+    const double d1 = __dsub_rn(c[1], q[1]);
+    double acc = __fma_rn(d0, d0, __dmul_rn(d1, d1));
+#pragma unroll
+    for (int l = 2; l < DP; l++) {
+        const double d = __dsub_rn(c[l], q[l]);
+        acc = __fma_rn(d, d, acc);
+    }
+    return acc;
+}
+
 template <int DP>
 __device__ __forceinline__ bool exact_hit(const double *__restrict__ xs, uint32_t cpos, uint32_t qpos, double T)
 {
-    const double *c = xs + (uint64_t)cpos * DP;
-    const double *q = xs + (uint64_t)qpos * DP;
-    double acc = 0.0;
-    // padded dimensions hold 0 in both points: fma(0,0,acc) == acc exactly
-#pragma unroll
-    for (int l = 0; l < DP; l++) {
-        double d = __dsub_rn(c[l], q[l]);
-        acc = __fma_rn(d, d, acc);
-    }
-    return acc <= T;
+    return ref_dist2<DP>(xs + (uint64_t)cpos * DP, xs + (uint64_t)qpos * DP) <= T;
 }
 
 template <int DP>
@@ -261,13 +274,7 @@ __global__ void __launch_bounds__(SJ_CTA) k_join(sj_join_args a, sj_grid_dev g, 
                                 else if (acc <= thrHi) border |= 1u << jj;
                             } else {
                                 const double *cb = reinterpret_cast<const double *>(&st.c[j][0]);
-                                double acc = 0.0;
-#pragma unroll
-                                for (int l = 0; l < DP; l++) {
-                                    double d = __dsub_rn(cb[l], q64[l]);
-                                    acc = __fma_rn(d, d, acc);
-                                }
-                                if (acc <= T) hits |= 1u << jj;
+                                if (ref_dist2<DP>(cb, q64) <= T) hits |= 1u << jj;
                             }
                         }
                     }
@@ -331,18 +338,28 @@ __global__ void __launch_bounds__(SJ_CTA) k_join(sj_join_args a, sj_grid_dev g, 
                         const int L = __ffs(live) - 1;
                         live &= live - 1;
                         const uint32_t base = __shfl_sync(0xffffffffu, pRow, L);
+                        const uint32_t key = __shfl_sync(0xffffffffu, qid, L);
                         const bool h = (rowT >> L) & 1u;
                         const uint32_t b = __ballot_sync(0xffffffffu, h);
-                        if (h) a.outVal[base + __popc(b & ltmask)] = (int32_t)cidL;
+                        if (h) {
+                            const uint32_t at = base + __popc(b & ltmask);
+                            a.outKey[at] = (int32_t)key;
+                            a.outVal[at] = (int32_t)cidL;
+                        }
                     }
                     live = __ballot_sync(0xffffffffu, nCol != 0 && okCol);
                     while (live) {
                         const int j = __ffs(live) - 1;
                         live &= live - 1;
                         const uint32_t base = __shfl_sync(0xffffffffu, pCol, j);
+                        const uint32_t key = __shfl_sync(0xffffffffu, cidL, j);
                         const bool h = (mirRow >> j) & 1u;
                         const uint32_t b = __ballot_sync(0xffffffffu, h);
-                        if (h) a.outVal[base + __popc(b & ltmask)] = (int32_t)qid;
+                        if (h) {
+                            const uint32_t at = base + __popc(b & ltmask);
+                            a.outKey[at] = (int32_t)key;
+                            a.outVal[at] = (int32_t)qid;
+                        }
                     }
                 } else {
                     rowCount += __popc(rowMask);
@@ -397,7 +414,21 @@ cudaError_t launch_dp(const sj_join_args &a, const sj_grid_dev &g, int fill, int
 {
     uint32_t nt = a.taskEnd - a.taskBegin;
     if (nt == 0) return cudaSuccess;
-    unsigned grid = queue ? (unsigned)(numSM * 8) : nt;
+    // persistent queue: one full wave of resident CTAs
+    static int perSM[2][2] = {{0, 0}, {0, 0}};
+    int &occ = perSM[fp32 ? 1 : 0][fill ? 1 : 0];
+    if (queue && occ == 0) {
+        int b = 0;
+        if (fp32) {
+            if (fill) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_join<DP, true, true>, SJ_CTA, 0);
+            else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_join<DP, true, false>, SJ_CTA, 0);
+        } else {
+            if (fill) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_join<DP, false, true>, SJ_CTA, 0);
+            else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_join<DP, false, false>, SJ_CTA, 0);
+        }
+        occ = b > 0 ? b : 4;
+    }
+    unsigned grid = queue ? (unsigned)(numSM * occ) : nt;
     if (queue && grid > nt) grid = nt;
     if (fp32) {
         if (fill) k_join<DP, true, true><<<grid, SJ_CTA, 0, s>>>(a, g, queue);

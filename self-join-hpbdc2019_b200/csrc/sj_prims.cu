@@ -60,7 +60,7 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan_reduce(const uint32_t *__
 // (nullptr for a single-block scan, which also writes the grand total).
 __global__ void __launch_bounds__(SCAN_THREADS) k_scan_tile(const uint32_t *in, uint32_t *out, uint64_t n,
                                                             const uint32_t *__restrict__ blockOffsets,
-                                                            uint32_t *total_dev)
+                                                            uint32_t *total_dev, uint32_t *zeroIn)
 {
     uint64_t base = (uint64_t)blockIdx.x * SCAN_TILE + (uint64_t)threadIdx.x * SCAN_ITEMS;
     uint32_t v[SCAN_ITEMS];
@@ -70,6 +70,11 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan_tile(const uint32_t *in, 
         uint64_t idx = base + i;
         v[i] = (idx < n) ? in[idx] : 0u;
         s += v[i];
+    }
+    if (zeroIn) {
+#pragma unroll
+        for (int i = 0; i < SCAN_ITEMS; i++)
+            if (base + i < n) zeroIn[base + i] = 0u;
     }
     uint32_t tot;
     uint32_t pre = block_exclusive_scan(s, &tot);
@@ -102,14 +107,14 @@ size_t scan_temp_elems(uint64_t n)
 }
 
 cudaError_t scan_rec(const uint32_t *in, uint32_t *out, uint64_t n, uint32_t *temp, uint32_t *total_dev,
-                     cudaStream_t s)
+                     cudaStream_t s, uint32_t *zeroIn = nullptr)
 {
     if (n == 0) {
         if (total_dev) return cudaMemsetAsync(total_dev, 0, sizeof(uint32_t), s);
         return cudaSuccess;
     }
     if (n <= (uint64_t)SCAN_TILE) {
-        k_scan_tile<<<1, SCAN_THREADS, 0, s>>>(in, out, n, nullptr, total_dev); sj_note_launch();
+        k_scan_tile<<<1, SCAN_THREADS, 0, s>>>(in, out, n, nullptr, total_dev, zeroIn); sj_note_launch();
         return cudaGetLastError();
     }
     uint64_t nb = ceil_div(n, SCAN_TILE);
@@ -121,7 +126,7 @@ cudaError_t scan_rec(const uint32_t *in, uint32_t *out, uint64_t n, uint32_t *te
         k_scan_total<<<1, 32, 0, s>>>(scanned, sums, nb, total_dev);
         sj_note_launch();
     }
-    k_scan_tile<<<(unsigned)nb, SCAN_THREADS, 0, s>>>(in, out, n, scanned, nullptr); sj_note_launch();
+    k_scan_tile<<<(unsigned)nb, SCAN_THREADS, 0, s>>>(in, out, n, scanned, nullptr, zeroIn); sj_note_launch();
     return cudaGetLastError();
 }
 
@@ -257,11 +262,19 @@ __global__ void __launch_bounds__(256) k_hash_pairs_dev(const int32_t *__restric
     const unsigned long long m = *count;
     if (m > cap) return;
     unsigned long long h = 0;
-    uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += stride) {
-        unsigned long long z = ((unsigned long long)(uint32_t)key[i] << 32) | (uint32_t)val[i];
-        h += splitmix64(z);
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    const uint64_t m4 = m / 4;
+    const int4 *k4 = reinterpret_cast<const int4 *>(key);
+    const int4 *v4 = reinterpret_cast<const int4 *>(val);
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m4; i += stride) {
+        const int4 a = __ldcs(k4 + i), b = __ldcs(v4 + i);
+        h += splitmix64(((unsigned long long)(uint32_t)a.x << 32) | (uint32_t)b.x);
+        h += splitmix64(((unsigned long long)(uint32_t)a.y << 32) | (uint32_t)b.y);
+        h += splitmix64(((unsigned long long)(uint32_t)a.z << 32) | (uint32_t)b.z);
+        h += splitmix64(((unsigned long long)(uint32_t)a.w << 32) | (uint32_t)b.w);
     }
+    for (uint64_t i = 4 * m4 + (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += stride)
+        h += splitmix64(((unsigned long long)(uint32_t)key[i] << 32) | (uint32_t)val[i]);
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) h += __shfl_xor_sync(0xffffffffu, h, o);
     __shared__ unsigned long long ws[8];
@@ -314,7 +327,7 @@ cudaError_t sj_hash_pairs_dev(const int32_t *key, const int32_t *val, const unsi
                               uint64_t gridHint, unsigned long long *hashOut, cudaStream_t s)
 {
     uint64_t blocks = ceil_div(gridHint ? gridHint : 1, 256 * 16);
-    if (blocks > 148 * 16) blocks = 148 * 16;
+    if (blocks > 148 * 8) blocks = 148 * 8;
     if (blocks == 0) blocks = 1;
     k_hash_pairs_dev<<<(unsigned)blocks, 256, 0, s>>>(key, val, count, cap, hashOut);
     sj_note_launch();
@@ -340,6 +353,12 @@ cudaError_t sj_exclusive_scan_u32(const uint32_t *in, uint32_t *out, uint64_t n,
                                   cudaStream_t s)
 {
     return scan_rec(in, out, n, (uint32_t *)temp, total_dev, s);
+}
+
+cudaError_t sj_exclusive_scan_u32_clear(uint32_t *in, uint32_t *out, uint64_t n, void *temp, uint32_t *total_dev,
+                                        cudaStream_t s)
+{
+    return scan_rec(in, out, n, (uint32_t *)temp, total_dev, s, in);
 }
 
 size_t sj_radix_temp_bytes(uint64_t n)

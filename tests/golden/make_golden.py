@@ -59,6 +59,9 @@ CASES = {
     "shell6d": (lambda: shell(3000, 6, 0.1, 16), 0.1, 6, 6, [3, 6]),
     "gauss16": (lambda: datasets.gaussian_mixture(2000, 16, 17), 0.3, 16, 6, [3, 6]),
     "uni5d_k3": (lambda: np.random.default_rng(18).random((2000, 5)), 0.12, 5, 3, [3, 5, 6]),
+    "shell4d": (lambda: shell(4000, 4, 0.05, 19), 0.05, 4, 4, [3, 6]),
+    "shell5d_k3": (lambda: shell(4000, 5, 0.08, 20), 0.08, 5, 3, [3, 5, 6]),
+    "shell16d_k6": (lambda: shell(3000, 16, 0.3, 21), 0.3, 16, 6, [3, 6]),
 }
 
 

@@ -141,7 +141,8 @@ def test_neighbor_table_rows():
     starts = np.concatenate([[0], np.cumsum(deg)[:-1]])
     for p in np.random.default_rng(0).choice(len(pts), 300, replace=False):
         got = np.sort(vals[rows[p, 0]:rows[p, 1] + 1])
-        assert np.array_equal(got, ov[starts[p]:starts[p] + deg[p]])
+        s0 = int(starts[p])
+        assert np.array_equal(got, ov[s0:s0 + int(deg[p])])
 
 
 @pytest.mark.parametrize("name", ["exp4d", "gauss16_k6", "duplicates", "uniform5d_k3"])
