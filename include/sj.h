@@ -191,6 +191,28 @@ sj_status sj_mlp_loss_grad(const float *x, const float *y, uint32_t m, const flo
 /* Forward pass only: out m x 2. */
 sj_status sj_mlp_forward(const float *x, uint32_t m, const float *w, float *out, int device);
 
+/* Loss and gradient of the estimator MLP, like sj_mlp_loss_grad, for callers
+ * that cannot allocate device memory: code that runs while its stream is being
+ * captured into a CUDA graph (where cudaMalloc and cudaFree are not allowed),
+ * and services that reserve all of their GPU memory up front and must not grow
+ * the device heap afterwards.  No counterpart in the reference.
+ *
+ * Every pointer is DEVICE memory owned by the caller: x (m x 16), y (m x 2),
+ * w (SJ_MLP_NPARAM), loss (1 float, overwritten), grad (SJ_MLP_NPARAM).  The
+ * per-sample activations live in a fixed array inside the library sized for
+ * SJ_MLP_NOALLOC_MAX_SAMPLES samples (about 8.5 MB, held by every device that
+ * loads the library until the process exits); larger m is rejected with
+ * SJ_ERR_BAD_INPUT.  Work is queued on `stream` (a cudaStream_t; NULL = the
+ * default stream) and the call returns without synchronising.  The first call
+ * on each device looks up the array's device address; make that first call
+ * before any stream capture begins.  All calls on a device share the one
+ * array: calls whose work overlaps on the GPU (different streams, or
+ * different threads on one device) race and corrupt each other's results, so
+ * order them on one stream or serialise them. */
+#define SJ_MLP_NOALLOC_MAX_SAMPLES 8192
+sj_status sj_mlp_loss_grad_noalloc(const float *x, const float *y, uint32_t m, const float *w, float *loss,
+                                   float *grad, void *stream);
+
 /* Kernels this library has launched since it was loaded (all contexts). */
 uint64_t sj_kernel_launch_count(void);
 

@@ -996,6 +996,8 @@ sj_status bind(Ctx &c)
 
 }  // namespace
 
+void sj_set_error_message(const char *msg) { g_lastError = msg ? msg : ""; }
+
 // =================================================================== C ABI
 extern "C" {
 

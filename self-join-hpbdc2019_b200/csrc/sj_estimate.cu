@@ -10,6 +10,8 @@
 // Learned estimator: a 16 -> 64 -> 64 -> 2 ReLU MLP on per-cell features
 // predicts log2(1 + distance calcs) and log2(1 + hits) of a cell.  Forward,
 // backward and Adam are plain FP32 CUDA-core kernels (the network is tiny).
+#include <mutex>
+
 #include "sj_internal.h"
 
 namespace {
@@ -242,4 +244,71 @@ cudaError_t sj_launch_mlp_train_step(const float *x, const float *y, uint32_t m,
     if (e != cudaSuccess) return e;
     k_adam<<<(NP + 255) / 256, 256, 0, s>>>(weights, grad, adamM, adamV, step, lr); sj_note_launch();
     return cudaGetLastError();
+}
+
+// ------------------------------------------------- allocation-free gradient --
+// Fixed scratch for sj_mlp_loss_grad_noalloc: the per-sample activations and
+// gradients (H1, G1, H2, G2 of SJ_HID floats and G3 of SJ_NOUT floats) of at
+// most SJ_MLP_NOALLOC_MAX_SAMPLES samples.  Every device that loads this
+// library holds it (about 8.5 MB) until the process exits.
+static __device__ __align__(256) float g_mlpNoallocScratch[SJ_MLP_NOALLOC_MAX_SAMPLES * (4 * SJ_HID + SJ_NOUT)];
+
+namespace {
+constexpr int kMaxDevices = 64;
+std::mutex g_noallocMutex;
+float *g_noallocScratchPtr[kMaxDevices] = {nullptr};
+}  // namespace
+
+extern "C" sj_status sj_mlp_loss_grad_noalloc(const float *x, const float *y, uint32_t m, const float *w, float *loss,
+                                              float *grad, void *stream)
+{
+    if (!x || !y || !w || !loss || !grad || m == 0) {
+        sj_set_error_message("sj_mlp_loss_grad_noalloc: null pointer or zero samples");
+        return SJ_ERR_BAD_INPUT;
+    }
+    if (m > SJ_MLP_NOALLOC_MAX_SAMPLES) {
+        sj_set_error_message("sj_mlp_loss_grad_noalloc: more samples than the fixed scratch holds "
+                             "(limit SJ_MLP_NOALLOC_MAX_SAMPLES = 8192); split the batch");
+        return SJ_ERR_BAD_INPUT;
+    }
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
+        sj_set_error_message("sj_mlp_loss_grad_noalloc: no usable current device");
+        return SJ_ERR_CUDA;
+    }
+    float *scratch;
+    {
+        // first call on a device: resolve the device address of the scratch
+        // array (a host-side name of a __device__ array is not a device pointer)
+        std::lock_guard<std::mutex> lock(g_noallocMutex);
+        if (!g_noallocScratchPtr[dev]) {
+            void *ptr = nullptr;
+            e = cudaGetSymbolAddress(&ptr, g_mlpNoallocScratch);
+            if (e != cudaSuccess || !ptr) {
+                sj_set_error_message("sj_mlp_loss_grad_noalloc: cudaGetSymbolAddress failed");
+                return SJ_ERR_CUDA;
+            }
+            g_noallocScratchPtr[dev] = (float *)ptr;
+        }
+        scratch = g_noallocScratchPtr[dev];
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    float *H1 = scratch, *G1 = H1 + (size_t)m * SJ_HID, *H2 = G1 + (size_t)m * SJ_HID, *G2 = H2 + (size_t)m * SJ_HID,
+          *G3 = G2 + (size_t)m * SJ_HID;
+    // the loss is accumulated with atomics: it must start at zero; the scratch
+    // rows are fully overwritten by every call
+    e = cudaMemsetAsync(loss, 0, sizeof(float), s);
+    if (e == cudaSuccess) {
+        k_mlp_backprop<<<(m + 127) / 128, 128, 0, s>>>(x, y, m, w, H1, G1, H2, G2, G3, loss);
+        sj_note_launch();
+        k_mlp_wgrad<<<(NP + 255) / 256, 256, 0, s>>>(x, H1, H2, G1, G2, G3, m, grad);
+        sj_note_launch();
+        e = cudaGetLastError();
+    }
+    if (e != cudaSuccess) {
+        sj_set_error_message(cudaGetErrorString(e));
+        return SJ_ERR_CUDA;
+    }
+    return SJ_OK;
 }

@@ -75,6 +75,8 @@ struct sj_join_args {
 // sj_note_launch() after each <<<...>>>; bench and tests read the total).
 void sj_note_launch();
 unsigned long long sj_launch_total();
+// sets the text returned by sj_last_error() for this thread
+void sj_set_error_message(const char *msg);
 
 // ---------------------------------------------------------------- launchers
 // primitives (sj_prims.cu)

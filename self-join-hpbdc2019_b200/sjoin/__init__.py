@@ -30,7 +30,8 @@ EXPORTS = [
     "sj_params_default", "sj_create", "sj_destroy", "sj_import_csv", "sj_read_csv", "sj_set_points", "sj_build_index",
     "sj_index_sizes", "sj_index_export", "sj_join", "sj_degrees", "sj_neighbor_table", "sj_free",
     "sj_get_stats", "sj_get_stream", "sj_mlp_num_params", "sj_set_estimator_weights", "sj_load_estimator",
-    "sj_cell_features", "sj_mlp_train", "sj_mlp_loss_grad", "sj_mlp_forward", "sj_status_string",
+    "sj_cell_features", "sj_mlp_train", "sj_mlp_loss_grad", "sj_mlp_forward", "sj_mlp_loss_grad_noalloc",
+    "sj_status_string",
     "sj_last_error", "sj_version", "sj_kernel_launch_count",
 ]
 
@@ -125,6 +126,7 @@ def load() -> C.CDLL:
     L.sj_mlp_train.argtypes = [vp, vp, u32, vp, i32, C.c_float, u32, u64, C.POINTER(C.c_float), i32]
     L.sj_mlp_loss_grad.argtypes = [vp, vp, u32, vp, C.POINTER(C.c_float), vp, i32]
     L.sj_mlp_forward.argtypes = [vp, u32, vp, vp, i32]
+    L.sj_mlp_loss_grad_noalloc.argtypes = [vp, vp, u32, vp, vp, vp, vp]
     L.sj_status_string.restype = C.c_char_p
     L.sj_status_string.argtypes = [i32]
     L.sj_last_error.restype = C.c_char_p
@@ -362,6 +364,17 @@ def mlp_loss_grad(x: np.ndarray, y: np.ndarray, w: np.ndarray, device: int = 0):
     loss = C.c_float()
     _check(L.sj_mlp_loss_grad(_ptr(x), _ptr(y), x.shape[0], _ptr(w), C.byref(loss), _ptr(g), device))
     return float(loss.value), g
+
+
+MLP_NOALLOC_MAX_SAMPLES = 8192
+
+
+def mlp_loss_grad_noalloc(x_ptr: int, y_ptr: int, m: int, w_ptr: int, loss_ptr: int, grad_ptr: int,
+                          stream: int = 0):
+    """Allocation-free loss/gradient on caller-owned device buffers (see sj.h).
+    Queues the work on `stream` and returns without synchronising."""
+    _check(load().sj_mlp_loss_grad_noalloc(C.c_void_p(x_ptr), C.c_void_p(y_ptr), int(m), C.c_void_p(w_ptr),
+                                           C.c_void_p(loss_ptr), C.c_void_p(grad_ptr), C.c_void_p(stream or None)))
 
 
 def mlp_forward(x: np.ndarray, w: np.ndarray, device: int = 0) -> np.ndarray:
