@@ -200,6 +200,13 @@ struct Ctx {
     // estimator
     std::vector<float> mlpW;
     DevBuf<float> dMlpW;
+    // grow-only scratch reused by every index build / join (no per-call allocation)
+    DevBuf<double> sMinMax;
+    DevBuf<uint64_t> sKeys, sKeysAlt;
+    DevBuf<uint32_t> sValsAlt, sFlags, sOne, sCnt;
+    DevBuf<uint8_t> sTemp;
+    DevBuf<float> sMlpOut;
+    DevBuf<unsigned long long> sHits, sCands;
     std::vector<double> cellRate;      // predicted hits per evaluation, per cell
     std::vector<double> measCellHits;  // from the last degrees/join run (full-stencil semantics)
     bool haveMeas = false;
@@ -271,7 +278,7 @@ sj_status build_index(Ctx &c)
     const int D = c.p.gpunumdim, k = c.p.numindexeddim;
     const uint64_t n = c.n;
     // 1. min / max of every dimension
-    DevBuf<double> mm;
+    DevBuf<double> &mm = c.sMinMax;
     CK(mm.ensure(2 * D + 1));
     CK(sj_launch_minmax(c.pts.p, n, D, mm.p, c.s));
     std::vector<double> hmm(2 * D + 1);
@@ -320,9 +327,9 @@ sj_status build_index(Ctx &c)
     int bits = 1;
     while (bits < 64 && (1ULL << bits) < mul) bits++;
     // 3. keys, stable sort, run-length cells
-    DevBuf<uint64_t> keys, keysAlt;
-    DevBuf<uint32_t> valsAlt, flags;
-    DevBuf<uint8_t> tmp;
+    DevBuf<uint64_t> &keys = c.sKeys, &keysAlt = c.sKeysAlt;
+    DevBuf<uint32_t> &valsAlt = c.sValsAlt, &flags = c.sFlags;
+    DevBuf<uint8_t> &tmp = c.sTemp;
     CK(keys.ensure(n));
     CK(keysAlt.ensure(n));
     CK(c.ids.ensure(n));
@@ -335,7 +342,7 @@ sj_status build_index(Ctx &c)
     uint64_t *sk = inAlt ? keysAlt.p : keys.p;
     if (inAlt) CK(cudaMemcpyAsync(c.ids.p, valsAlt.p, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, c.s));
     CK(sj_launch_cell_flags(sk, n, flags.p, c.s));
-    DevBuf<uint32_t> nne;
+    DevBuf<uint32_t> &nne = c.sOne;
     CK(nne.ensure(1));
     CK(sj_exclusive_scan_u32(flags.p, flags.p, n, tmp.p, nne.p, c.s));
     uint32_t nCells = 0;
@@ -384,12 +391,12 @@ sj_status build_neighbours(Ctx &c, int pattern)
     CK(c.nbrStart.ensure(nc + 1));
     CK(c.candFull.ensure(nc));
     CK(c.feat.ensure((size_t)nc * SJ_NFEAT));
-    DevBuf<uint32_t> cnt;
+    DevBuf<uint32_t> &cnt = c.sCnt;
     CK(cnt.ensure(nc + 1));
     CK(sj_launch_neighbours(c.cellLid.p, c.cellCoord.p, c.cellStart.p, nc, c.g, pattern, nullptr, cnt.p,
                             c.candFull.p, c.feat.p, 0, c.s));
-    DevBuf<uint8_t> tmp;
-    DevBuf<uint32_t> tot;
+    DevBuf<uint8_t> &tmp = c.sTemp;
+    DevBuf<uint32_t> &tot = c.sOne;
     CK(tot.ensure(1));
     CK(tmp.ensure(sj_scan_temp_bytes(nc)));
     CK(sj_exclusive_scan_u32(cnt.p, c.nbrStart.p, nc, tmp.p, tot.p, c.s));
@@ -456,7 +463,7 @@ sj_status estimate_rates(Ctx &c)
     const uint32_t nc = c.nCells;
     c.cellRate.assign(nc, 0.0);
     if (c.p.scheduler == SJ_SCHED_LEARNED && !c.mlpW.empty()) {
-        DevBuf<float> out;
+        DevBuf<float> &out = c.sMlpOut;
         CK(out.ensure((size_t)nc * SJ_NOUT));
         CK(c.dMlpW.ensure(SJ_MLP_NPARAM));
         CK(cudaMemcpyAsync(c.dMlpW.p, c.mlpW.data(), sizeof(float) * SJ_MLP_NPARAM, cudaMemcpyHostToDevice, c.s));
@@ -471,7 +478,7 @@ sj_status estimate_rates(Ctx &c)
             c.cellRate[i] = std::min(1.0, std::max(r, 0.0));
         }
     } else {
-        DevBuf<unsigned long long> hits, cands;
+        DevBuf<unsigned long long> &hits = c.sHits, &cands = c.sCands;
         CK(hits.ensure(nc));
         CK(cands.ensure(nc));
         CK(cudaMemsetAsync(hits.p, 0, sizeof(unsigned long long) * nc, c.s));
@@ -507,71 +514,132 @@ double diag_evals(uint64_t s0, uint64_t s1, uint64_t q)
     return e;
 }
 
-sj_status build_tasks(Ctx &c, int pattern, uint64_t cap)
+// Tasks of one cell: query tiles of <= SJ_CTA points x chunks of the cell's
+// candidate stream (home segment + owned neighbours, <= SJ_MAX_SEG segments per
+// group).  With emit == nullptr only counts them.  Returns the number of tasks
+// and adds their evaluations / predicted pairs to *evals / *pred.
+template <class Emit>
+uint32_t cell_tasks(const Ctx &c, uint32_t A, bool sym, uint64_t cap, double pairsPerTask, Emit emit)
+{
+    const uint32_t aStart = c.hCellStart[A], aEnd = c.hCellStart[A + 1];
+    const uint32_t occ = aEnd - aStart;
+    const uint32_t nb0 = c.hNbrStart[A], nb1 = c.hNbrStart[A + 1];
+    const uint32_t nSegAll = 1 + (nb1 - nb0);
+    const double rate = c.cellRate.empty() ? 0.0 : c.cellRate[A];
+    uint32_t made = 0;
+    for (uint32_t q0 = 0; q0 < occ; q0 += SJ_CTA) {
+        const uint32_t qc = std::min<uint32_t>(SJ_CTA, occ - q0);
+        const uint32_t qBegin = aStart + q0;
+        // chunk length from the predicted pair density of this cell, and never
+        // more candidates than keep the worst case (every candidate a hit, both
+        // directions) inside one batch
+        const double perEval = std::max(rate, 1e-6) * (sym ? 2.0 : 1.0);
+        const double chunk = pairsPerTask / (perEval * qc);
+        uint32_t sChunk = (uint32_t)std::min(65536.0, std::max(256.0, chunk));
+        const uint64_t worst = cap / ((sym ? 2ULL : 1ULL) * qc);
+        if (sChunk > worst) sChunk = (uint32_t)worst;
+        sChunk = std::max<uint32_t>(32, (sChunk / 32) * 32);
+        for (uint32_t g0 = 0; g0 < nSegAll; g0 += SJ_MAX_SEG) {
+            const uint32_t gc = std::min<uint32_t>(SJ_MAX_SEG, nSegAll - g0);
+            uint64_t homeLen = 0, L = 0;
+            for (uint32_t sgi = 0; sgi < gc; sgi++) {
+                const uint32_t gs = g0 + sgi;
+                uint64_t len;
+                if (gs == 0) {
+                    len = sym ? (aEnd - qBegin) : occ;
+                    homeLen = len;
+                } else {
+                    const uint32_t B = c.hNbrCell[nb0 + gs - 1];
+                    len = c.hCellStart[B + 1] - c.hCellStart[B];
+                }
+                L += len;
+            }
+            for (uint64_t s0 = 0; s0 < L; s0 += sChunk) {
+                const uint64_t s1 = std::min<uint64_t>(L, s0 + sChunk);
+                double ev;
+                if (sym && g0 == 0 && s0 < homeLen) {
+                    const uint64_t h1 = std::min<uint64_t>(s1, homeLen);
+                    ev = diag_evals(s0, h1, qc) + (double)qc * (double)(s1 - h1);
+                } else {
+                    ev = (double)qc * (double)(s1 - s0);
+                }
+                sj_task t;
+                t.cell = A;
+                t.qBegin = qBegin;
+                t.qCount = qc;
+                t.segBase = g0;
+                t.segCount = gc;
+                t.sBegin = (uint32_t)s0;
+                t.sEnd = (uint32_t)s1;
+                t.flags = (sym ? SJ_TASK_SYM : 0u) | (g0 == 0 ? SJ_TASK_HOME : 0u);
+                emit(made, t, ev, ev * rate * (sym ? 2.0 : 1.0));
+                made++;
+            }
+        }
+    }
+    return made;
+}
+
+// Builds the task list in queue order.  With byCost the cells are ordered by
+// their mean predicted task cost (evaluations + a write cost per predicted
+// pair), heaviest first, and each cell's tasks stay together; otherwise cells
+// keep linear-id order.  Cells are processed in parallel on the host.
+sj_status build_tasks(Ctx &c, int pattern, uint64_t cap, bool byCost)
 {
     Timer tm;
     tm.start(c.s);
     const bool sym = pattern != SJ_PAT_FULL;
-    c.tasks.clear();
-    c.taskPred.clear();
-    c.taskEvals.clear();
+    const uint32_t nc = c.nCells;
     const double pairsPerTask = std::max(4096.0, (double)cap / 4096.0);
-    for (uint32_t A = 0; A < c.nCells; A++) {
-        const uint32_t aStart = c.hCellStart[A], aEnd = c.hCellStart[A + 1];
-        const uint32_t occ = aEnd - aStart;
-        const uint32_t nb0 = c.hNbrStart[A], nb1 = c.hNbrStart[A + 1];
-        const uint32_t nSegAll = 1 + (nb1 - nb0);
-        const double rate = c.cellRate.empty() ? 0.0 : c.cellRate[A];
-        for (uint32_t q0 = 0; q0 < occ; q0 += SJ_CTA) {
-            const uint32_t qc = std::min<uint32_t>(SJ_CTA, occ - q0);
-            const uint32_t qBegin = aStart + q0;
-            // chunk length from the predicted pair density of this cell, and
-            // never more candidates than keep the worst case (every candidate a
-            // hit, both directions) inside one batch
-            double perEval = std::max(rate, 1e-6) * (sym ? 2.0 : 1.0);
-            double chunk = pairsPerTask / (perEval * qc);
-            uint32_t sChunk = (uint32_t)std::min(65536.0, std::max(256.0, chunk));
-            const uint64_t worst = (uint64_t)cap / ((sym ? 2ULL : 1ULL) * qc);
-            if (sChunk > worst) sChunk = (uint32_t)worst;
-            sChunk = std::max<uint32_t>(32, (sChunk / 32) * 32);
-            for (uint32_t g0 = 0; g0 < nSegAll; g0 += SJ_MAX_SEG) {
-                const uint32_t gc = std::min<uint32_t>(SJ_MAX_SEG, nSegAll - g0);
-                uint64_t homeLen = 0, L = 0;
-                for (uint32_t sgi = 0; sgi < gc; sgi++) {
-                    uint32_t gs = g0 + sgi;
-                    uint64_t len;
-                    if (gs == 0) len = sym ? (aEnd - qBegin) : occ;
-                    else {
-                        uint32_t B = c.hNbrCell[nb0 + gs - 1];
-                        len = c.hCellStart[B + 1] - c.hCellStart[B];
-                    }
-                    if (gs == 0) homeLen = len;
-                    L += len;
-                }
-                for (uint64_t s0 = 0; s0 < L; s0 += sChunk) {
-                    uint64_t s1 = std::min<uint64_t>(L, s0 + sChunk);
-                    sj_task t;
-                    t.cell = A;
-                    t.qBegin = qBegin;
-                    t.qCount = qc;
-                    t.segBase = g0;
-                    t.segCount = gc;
-                    t.sBegin = (uint32_t)s0;
-                    t.sEnd = (uint32_t)s1;
-                    t.flags = (sym ? SJ_TASK_SYM : 0u) | (g0 == 0 ? SJ_TASK_HOME : 0u);
-                    double ev;
-                    if (sym && g0 == 0 && s0 < homeLen) {
-                        uint64_t h1 = std::min<uint64_t>(s1, homeLen);
-                        ev = diag_evals(s0, h1, qc) + (double)qc * (double)(s1 - h1);
-                    } else {
-                        ev = (double)qc * (double)(s1 - s0);
-                    }
-                    c.tasks.push_back(t);
-                    c.taskEvals.push_back(ev);
-                    c.taskPred.push_back(ev * rate * (sym ? 2.0 : 1.0));
-                }
+    std::vector<uint32_t> cnt(nc);
+    std::vector<double> cellCost(nc);
+#pragma omp parallel for schedule(dynamic, 64)
+    for (int64_t Ai = 0; Ai < (int64_t)nc; Ai++) {
+        const uint32_t A = (uint32_t)Ai;
+        double ev = 0, pr = 0;
+        cnt[A] = cell_tasks(c, A, sym, cap, pairsPerTask, [&](uint32_t, const sj_task &, double e, double p) {
+            ev += e;
+            pr += p;
+        });
+        cellCost[A] = cnt[A] ? (ev + 4.0 * pr) / cnt[A] : 0.0;
+    }
+    std::vector<uint32_t> order(nc);
+    std::iota(order.begin(), order.end(), 0u);
+    if (byCost)
+        std::stable_sort(order.begin(), order.end(),
+                         [&](uint32_t x, uint32_t y) { return cellCost[x] > cellCost[y]; });
+    std::vector<uint64_t> off(nc + 1, 0);
+    for (uint32_t i = 0; i < nc; i++) off[i + 1] = off[i] + cnt[order[i]];
+    const uint64_t nt = off[nc];
+    if (nt > 0xffffffffULL) {
+        set_error("%llu tasks exceed the 32-bit task index", (unsigned long long)nt);
+        return SJ_ERR_BAD_INPUT;
+    }
+    c.tasks.resize(nt);
+    c.taskEvals.resize(nt);
+    c.taskPred.resize(nt);
+#pragma omp parallel for schedule(dynamic, 64)
+    for (int64_t i = 0; i < (int64_t)nc; i++) {
+        const uint64_t base = off[i];
+        cell_tasks(c, order[i], sym, cap, pairsPerTask, [&](uint32_t j, const sj_task &t, double e, double p) {
+            c.tasks[base + j] = t;
+            c.taskEvals[base + j] = e;
+            c.taskPred[base + j] = p;
+        });
+    }
+    if (c.p.shard_count > 1) {
+        // round-robin over the ordered list: each shard gets a similar cost mix
+        size_t w = 0;
+        for (size_t i = 0; i < c.tasks.size(); i++)
+            if ((int)(i % (size_t)c.p.shard_count) == c.p.shard_index) {
+                c.tasks[w] = c.tasks[i];
+                c.taskEvals[w] = c.taskEvals[i];
+                c.taskPred[w] = c.taskPred[i];
+                w++;
             }
-        }
+        c.tasks.resize(w);
+        c.taskEvals.resize(w);
+        c.taskPred.resize(w);
     }
     c.st.ms_tasks += tm.stop(c.s);
     return SJ_OK;
@@ -616,32 +684,6 @@ uint64_t auto_capacity(Ctx &c)
     return std::max<uint64_t>(1 << 20, std::min<uint64_t>(byMem, 2000000000ULL));
 }
 
-void order_tasks(Ctx &c)
-{
-    const bool byCost = c.p.sort_by_workload || c.p.search_mode == 7 || c.p.search_mode == 9 ||
-                        c.p.search_mode == 10;
-    std::vector<uint32_t> order(c.tasks.size());
-    std::iota(order.begin(), order.end(), 0u);
-    if (byCost) {
-        // cost: distance evaluations plus a write cost per predicted pair
-        std::vector<double> cost(c.tasks.size());
-        for (size_t i = 0; i < cost.size(); i++) cost[i] = c.taskEvals[i] + 4.0 * c.taskPred[i];
-        std::stable_sort(order.begin(), order.end(), [&](uint32_t x, uint32_t y) { return cost[x] > cost[y]; });
-    }
-    std::vector<sj_task> t2;
-    std::vector<double> p2, e2;
-    t2.reserve(order.size());
-    for (size_t i = 0; i < order.size(); i++) {
-        if (c.p.shard_count > 1 && (int)(i % (size_t)c.p.shard_count) != c.p.shard_index) continue;
-        t2.push_back(c.tasks[order[i]]);
-        p2.push_back(c.taskPred[order[i]]);
-        e2.push_back(c.taskEvals[order[i]]);
-    }
-    c.tasks.swap(t2);
-    c.taskPred.swap(p2);
-    c.taskEvals.swap(e2);
-}
-
 sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
 {
     const unsigned long long launches0 = sj_launch_total();
@@ -656,8 +698,9 @@ sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
     {
         Timer tm;
         tm.start(c.s);
-        CKS(build_tasks(c, pattern, cap));
-        order_tasks(c);
+        const bool byCost = c.p.sort_by_workload || c.p.search_mode == 7 || c.p.search_mode == 9 ||
+                            c.p.search_mode == 10;
+        CKS(build_tasks(c, pattern, cap, byCost));
         CK(c.dTasks.ensure(c.tasks.size()));
         if (!c.tasks.empty())
             CK(cudaMemcpyAsync(c.dTasks.p, c.tasks.data(), sizeof(sj_task) * c.tasks.size(), cudaMemcpyHostToDevice,
@@ -735,7 +778,8 @@ sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
     if (delivery == SJ_DELIVER_NONE && !plan.empty()) {
         double maxPred = 0;
         for (const BatchRange &br : plan) maxPred = std::max(maxPred, predOf(br) * (1.0 + c.p.alpha));
-        uint64_t bufCap = std::min<uint64_t>(cap, (uint64_t)(1.25 * maxPred) + 65536);
+        uint64_t bufCap = c.p.batch_capacity_pairs ? cap
+                                                   : std::min<uint64_t>(cap, (uint64_t)(1.25 * maxPred) + 65536);
         if (bufCap > c.outKey.n) {
             CK(c.outKey.ensure(bufCap));
             CK(c.outVal.ensure(bufCap));
@@ -919,7 +963,7 @@ sj_status run_degrees(Ctx &c, uint32_t *degHost)
     bool queue;
     CKS(prepare_join(c, pattern, queue));
     const uint64_t n = c.n;
-    CKS(build_tasks(c, pattern, 0xffffffffULL));
+    CKS(build_tasks(c, pattern, 0xffffffffULL, false));
     const uint32_t nt = (uint32_t)c.tasks.size();
     CK(c.dTasks.ensure(nt));
     if (nt) CK(cudaMemcpyAsync(c.dTasks.p, c.tasks.data(), sizeof(sj_task) * nt, cudaMemcpyHostToDevice, c.s));

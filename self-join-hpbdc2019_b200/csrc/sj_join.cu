@@ -28,6 +28,7 @@
 namespace {
 
 constexpr int NW = SJ_CTA / 32;
+constexpr int EMIT_STAGE = 256;   // staged emissions per warp and direction (sparse blocks)
 
 __device__ __forceinline__ uint32_t transpose32(uint32_t x, uint32_t lane)
 {
@@ -100,6 +101,11 @@ __global__ void __launch_bounds__(SJ_CTA) k_join(sj_join_args a, sj_grid_dev g, 
     __shared__ uint32_t segStart[SJ_MAX_SEG];
     __shared__ uint32_t segPre[SJ_MAX_SEG + 1];
     __shared__ uint32_t colCnt[FILL ? 1 : NW][FILL ? 1 : S];
+    // fill pass, sparse blocks: per-warp staging of (slot, key, value)
+    __shared__ uint32_t stSlot[FILL ? NW : 1][FILL ? EMIT_STAGE : 1];
+    __shared__ uint32_t stKey[FILL ? NW : 1][FILL ? EMIT_STAGE : 1];
+    __shared__ uint32_t stVal[FILL ? NW : 1][FILL ? EMIT_STAGE : 1];
+    __shared__ uint32_t qIdS[FILL ? SJ_CTA : 1];
     __shared__ uint32_t scanTmp[NW];
     __shared__ uint32_t curTask;
     __shared__ unsigned long long taskPairs;
@@ -194,6 +200,7 @@ __global__ void __launch_bounds__(SJ_CTA) k_join(sj_join_args a, sj_grid_dev g, 
         const bool qValid = qi < task.qCount;
         const uint32_t qpos = task.qBegin + (qValid ? qi : 0u);
         const uint32_t qid = a.ids[qpos];
+        if (FILL) qIdS[tid] = qid;
         double q64[F32 ? 1 : DP];
         float q2[F32 ? DP : 1];
         float thrLo = 0.f, thrHi = 0.f;
@@ -330,35 +337,88 @@ __global__ void __launch_bounds__(SJ_CTA) k_join(sj_join_args a, sj_grid_dev g, 
                     const bool okRow = (uint64_t)pRow + nRow <= a.capacity;
                     const bool okCol = (uint64_t)pCol + nCol <= a.capacity;
                     if (!okRow || !okCol) atomicMax(&a.stat[3], 1ULL);
-                    // one coalesced run per key: row runs (key = query L, values =
-                    // candidates in lane order), then column runs (key = candidate j,
-                    // values = queries in lane order)
-                    uint32_t live = __ballot_sync(0xffffffffu, nRow != 0 && okRow);
-                    while (live) {
-                        const int L = __ffs(live) - 1;
-                        live &= live - 1;
-                        const uint32_t base = __shfl_sync(0xffffffffu, pRow, L);
-                        const uint32_t key = __shfl_sync(0xffffffffu, qid, L);
-                        const bool h = (rowT >> L) & 1u;
-                        const uint32_t b = __ballot_sync(0xffffffffu, h);
-                        if (h) {
-                            const uint32_t at = base + __popc(b & ltmask);
-                            a.outKey[at] = (int32_t)key;
-                            a.outVal[at] = (int32_t)cidL;
+                    // Two ways to write a block's pairs, chosen per direction:
+                    // dense blocks: one warp iteration per non-empty run (the
+                    // run is written coalesced by the lanes holding its members);
+                    // sparse blocks: every lane stages its own short run in shared
+                    // memory, then the warp copies the staged pairs out in order.
+                    const uint32_t nr = okRow ? nRow : 0u, nc = okCol ? nCol : 0u;
+                    uint32_t incR = nr, incC = nc;
+#pragma unroll
+                    for (int o = 1; o < 32; o <<= 1) {
+                        const uint32_t yr = __shfl_up_sync(0xffffffffu, incR, o);
+                        const uint32_t yc = __shfl_up_sync(0xffffffffu, incC, o);
+                        if (lane >= (uint32_t)o) { incR += yr; incC += yc; }
+                    }
+                    const uint32_t totR = __shfl_sync(0xffffffffu, incR, 31);
+                    const uint32_t totC = __shfl_sync(0xffffffffu, incC, 31);
+                    uint32_t* const sS = stSlot[FILL ? warp : 0];
+                    uint32_t* const sK = stKey[FILL ? warp : 0];
+                    uint32_t* const sV = stVal[FILL ? warp : 0];
+                    // row direction: key = this lane's query, values = candidates
+                    if (totR <= EMIT_STAGE) {
+                        uint32_t m = okRow ? rowMask : 0u, at = incR - nr, slot = pRow;
+                        while (m) {
+                            const int b = __ffs(m) - 1;
+                            m &= m - 1;
+                            sS[at] = slot++;
+                            sK[at] = qid;
+                            sV[at] = candId[jb + b];
+                            at++;
+                        }
+                        __syncwarp();
+                        for (uint32_t e = lane; e < totR; e += 32) {
+                            a.outKey[sS[e]] = (int32_t)sK[e];
+                            a.outVal[sS[e]] = (int32_t)sV[e];
+                        }
+                        __syncwarp();
+                    } else {
+                        uint32_t live = __ballot_sync(0xffffffffu, nr != 0);
+                        while (live) {
+                            const int L = __ffs(live) - 1;
+                            live &= live - 1;
+                            const uint32_t base = __shfl_sync(0xffffffffu, pRow, L);
+                            const uint32_t key = __shfl_sync(0xffffffffu, qid, L);
+                            const bool h = (rowT >> L) & 1u;
+                            const uint32_t b = __ballot_sync(0xffffffffu, h);
+                            if (h) {
+                                const uint32_t at = base + __popc(b & ltmask);
+                                a.outKey[at] = (int32_t)key;
+                                a.outVal[at] = (int32_t)cidL;
+                            }
                         }
                     }
-                    live = __ballot_sync(0xffffffffu, nCol != 0 && okCol);
-                    while (live) {
-                        const int j = __ffs(live) - 1;
-                        live &= live - 1;
-                        const uint32_t base = __shfl_sync(0xffffffffu, pCol, j);
-                        const uint32_t key = __shfl_sync(0xffffffffu, cidL, j);
-                        const bool h = (mirRow >> j) & 1u;
-                        const uint32_t b = __ballot_sync(0xffffffffu, h);
-                        if (h) {
-                            const uint32_t at = base + __popc(b & ltmask);
-                            a.outKey[at] = (int32_t)key;
-                            a.outVal[at] = (int32_t)qid;
+                    // column direction: key = this lane's candidate, values = queries
+                    if (totC <= EMIT_STAGE) {
+                        uint32_t m = okCol ? mirT : 0u, at = incC - nc, slot = pCol;
+                        while (m) {
+                            const int b = __ffs(m) - 1;
+                            m &= m - 1;
+                            sS[at] = slot++;
+                            sK[at] = cidL;
+                            sV[at] = qIdS[warp * 32 + b];
+                            at++;
+                        }
+                        __syncwarp();
+                        for (uint32_t e = lane; e < totC; e += 32) {
+                            a.outKey[sS[e]] = (int32_t)sK[e];
+                            a.outVal[sS[e]] = (int32_t)sV[e];
+                        }
+                        __syncwarp();
+                    } else {
+                        uint32_t live = __ballot_sync(0xffffffffu, nc != 0);
+                        while (live) {
+                            const int j = __ffs(live) - 1;
+                            live &= live - 1;
+                            const uint32_t base = __shfl_sync(0xffffffffu, pCol, j);
+                            const uint32_t key = __shfl_sync(0xffffffffu, cidL, j);
+                            const bool h = (mirRow >> j) & 1u;
+                            const uint32_t b = __ballot_sync(0xffffffffu, h);
+                            if (h) {
+                                const uint32_t at = base + __popc(b & ltmask);
+                                a.outKey[at] = (int32_t)key;
+                                a.outVal[at] = (int32_t)qid;
+                            }
                         }
                     }
                 } else {

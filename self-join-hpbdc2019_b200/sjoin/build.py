@@ -47,7 +47,7 @@ def _compile(src: str, force: bool) -> str:
         cmd = [NVCC, "-O3", "-std=c++17", *ARCH, "-lineinfo", "-Xcompiler", "-fPIC",
                "-I", CSRC, "-I", INCLUDE, "-c", src, "-o", obj]
     else:
-        cmd = ["g++", "-O3", "-std=c++17", "-fPIC", "-I", CSRC, "-I", INCLUDE,
+        cmd = ["g++", "-O3", "-std=c++17", "-fPIC", "-fopenmp", "-I", CSRC, "-I", INCLUDE,
                "-I", os.path.join(CUDA, "include"), "-c", src, "-o", obj]
     subprocess.check_call(cmd)
     return obj
@@ -60,7 +60,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
         objs = list(ex.map(lambda s: _compile(s, force), srcs))
     if force or _newer(LIB, objs):
         subprocess.check_call([NVCC, "-shared", *ARCH, "-cudart", "static", "-o", LIB, *objs,
-                               "-Xlinker", "--no-undefined", "-lpthread", "-ldl", "-lrt"])
+                               "-Xlinker", "--no-undefined", "-lgomp", "-lpthread", "-ldl", "-lrt"])
     cli_src = os.path.join(CSRC, "sj_cli.cpp")
     if os.path.exists(cli_src) and (force or _newer(CLI, [cli_src, LIB] + _headers())):
         subprocess.check_call(["g++", "-O2", "-std=c++17", "-I", INCLUDE, cli_src, "-o", CLI,

@@ -1,0 +1,103 @@
+"""Trains the learned batch estimator on counts the engine itself measures.
+
+Data: seeded runs of the 6-D exponential(40) generator (the c4 workload's
+distribution) with eps drawn uniformly from [0.01, 0.05].  For each run the
+engine builds its index, computes every cell's 16 features and full-stencil
+distance-calculation count, and measures every point's neighbour count with
+its count pass (sj_degrees); a cell's target is (log2(1+calcs), log2(1+hits)).
+The point count of a run is shrunk until the run's full-stencil work stays
+under a budget, so the collection takes minutes, not hours.
+
+Training: the 16 -> 64 -> 64 -> 2 MLP is trained with the engine's own FP32
+forward / backward / Adam kernels (sj_mlp_train).  Weights are written as raw
+float32 in the engine's layout (sj_mlp_num_params() values).
+
+usage: python -m sjoin.train_estimator [--runs 50] [--out sjoin/estimator_c4.bin]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import time
+
+import numpy as np
+
+from . import PREC_FP32_REFINE, SelfJoin, datasets, mlp_init, mlp_loss_grad, mlp_train
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+DEFAULT_OUT = os.path.join(PKG, "estimator_c4.bin")
+
+
+def cell_table(pts: np.ndarray, eps: float, k: int, with_hits: bool = True):
+    """(features, calcs, hits) of every non-empty cell, measured by the engine."""
+    D = pts.shape[1]
+    with SelfJoin(D, eps, indexed_dims=k, mode=10, precision=PREC_FP32_REFINE) as sj:
+        sj.set_points(pts)
+        sj.build_index()
+        if with_hits:
+            sj.degrees()
+        feat, hits, calcs = sj.cell_features(with_hits=with_hits)
+    return feat, calcs, hits
+
+
+def targets(calcs: np.ndarray, hits: np.ndarray) -> np.ndarray:
+    return np.stack([np.log2(1.0 + calcs), np.log2(1.0 + hits)], 1).astype(np.float32)
+
+
+def collect(runs: int = 50, seed0: int = 7000, n_max: int = 1_000_000, n_min: int = 50_000,
+            work_budget: float = 4e11, D: int = 6, log=print):
+    rng = np.random.default_rng(seed0)
+    xs, ys, meta = [], [], []
+    for r in range(runs):
+        eps = float(rng.uniform(0.01, 0.05))
+        n = int(10 ** rng.uniform(math.log10(n_min), math.log10(n_max)))
+        seed = seed0 + r
+        while True:
+            pts = datasets.exponential(n, D, 40.0, seed)
+            feat, calcs, _ = cell_table(pts, eps, D, with_hits=False)
+            work = float(calcs.sum())
+            if work <= work_budget or n <= n_min:
+                break
+            n = max(n_min, int(n * math.sqrt(work_budget / work) * 0.9))
+        t0 = time.time()
+        feat, calcs, hits = cell_table(pts, eps, D, with_hits=True)
+        xs.append(feat)
+        ys.append(targets(calcs, hits))
+        meta.append(dict(run=r, seed=seed, n=n, eps=eps, cells=len(feat), calcs=float(calcs.sum()),
+                         hits=float(hits.sum()), s=round(time.time() - t0, 2)))
+        log(json.dumps(meta[-1]))
+    return np.concatenate(xs), np.concatenate(ys), meta
+
+
+def train(x: np.ndarray, y: np.ndarray, steps: int = 6000, lr: float = 2e-3, batch: int = 4096, seed: int = 1):
+    w0 = mlp_init(seed)
+    # step-wise learning-rate decay: three stages
+    w = w0
+    for frac, scale in ((0.5, 1.0), (0.3, 0.3), (0.2, 0.1)):
+        w, loss = mlp_train(x, y, w, steps=max(1, int(steps * frac)), lr=lr * scale, batch=batch, seed=seed)
+    return w, loss
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--runs", type=int, default=50)
+    ap.add_argument("--steps", type=int, default=6000)
+    ap.add_argument("--out", default=DEFAULT_OUT)
+    ap.add_argument("--data-out", default=None, help="optional .npz of the collected training set")
+    args = ap.parse_args()
+    t0 = time.time()
+    x, y, meta = collect(args.runs)
+    print(f"collected {len(x)} cells from {len(meta)} runs in {time.time() - t0:.1f} s", flush=True)
+    if args.data_out:
+        np.savez_compressed(args.data_out, x=x, y=y)
+    w, loss = train(x, y, steps=args.steps)
+    full, _ = mlp_loss_grad(x, y, w)
+    w.astype(np.float32).tofile(args.out)
+    print(json.dumps({"cells": int(len(x)), "final_loss": full, "out": args.out,
+                      "seconds": round(time.time() - t0, 1)}), flush=True)
+
+
+if __name__ == "__main__":
+    main()
