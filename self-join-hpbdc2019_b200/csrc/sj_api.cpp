@@ -436,7 +436,24 @@ void join_args_base(Ctx &c, sj_join_args &a)
 // FP32 filter half-band: bound on |(acc32 - thr32) - (S64 - T)| for local
 // coordinates measured from the home cell's centre (indexed dims) or the data
 // centre (other dims).  |a_l| <= 0.5 eps, |b_l| <= 1.5 eps on indexed dims.
-double filter_margin(const Ctx &c)
+// FP32 filter bounds.  Queries are taken relative to their home cell's centre
+// (indexed dims) or the data centre (others): |a| <= Ra; candidates lie in the
+// home cell or a neighbour: |b| <= Rb.  The kernel evaluates in FP32
+//     y = fl(|b|^2 - tLo) + sum_l fl(-2 a_l) b_l     (D+2 roundings),
+// with tLo = RD(T - |a|^2 - M).  With u = 2^-24 and r = Ra + Rb:
+//   * chain rounding <= (D+2) u (r^2 + T + M),
+//   * rounding the local coordinates moves |b - a|^2 by <= 2 u r^2,
+//   * the FP64 predicate's own rounding (d2 vs the exact |dx|^2) <= 2^-49 r^2,
+// so M = 2 (D+4) u (r^2 + T) + 2^-39 (r^2 + T) exceeds their sum: y <= 0 proves
+// d2 <= T.  y >= delta proves d2 > T when delta >= 2M + 2u (T + Ra^2 + M) (the
+// second term covers rounding tLo down).  Pairs with 0 < y < delta are
+// re-evaluated in FP64.
+struct FilterBounds {
+    double margin;
+    float delta;
+};
+
+FilterBounds filter_bounds(const Ctx &c)
 {
     const sj_grid_dev &g = c.g;
     double ra2 = 0, rb2 = 0;
@@ -450,9 +467,16 @@ double filter_margin(const Ctx &c)
             rb2 += h * h;
         }
     }
-    double r = std::sqrt(ra2) + std::sqrt(rb2);
+    const double r = std::sqrt(ra2) + std::sqrt(rb2);
     const double u = std::ldexp(1.0, -24);
-    return 2.0 * r * r * u * (g.D + 4) + g.thresh * std::ldexp(1.0, -40);
+    const double T = g.thresh;
+    FilterBounds b;
+    b.margin = 2.0 * (g.D + 4) * u * (r * r + T) + std::ldexp(r * r + T, -39);
+    const double d = (2.0 * b.margin + 2.0 * u * (T + ra2 + b.margin)) * (1.0 + std::ldexp(1.0, -20));
+    float df = (float)d;
+    if ((double)df < d) df = std::nextafter(df, INFINITY);
+    b.delta = df;
+    return b;
 }
 
 // ------------------------------------------------------------ estimate --
@@ -514,7 +538,8 @@ double diag_evals(uint64_t s0, uint64_t s1, uint64_t q)
     return e;
 }
 
-// Tasks of one cell: query tiles of <= SJ_CTA points x chunks of the cell's
+// Tasks of one cell: query tiles of <= SJ_CTA * R points (R query slots per
+// join thread, sj_query_slots) x chunks of the cell's
 // candidate stream (home segment + owned neighbours, <= SJ_MAX_SEG segments per
 // group).  With emit == nullptr only counts them.  Returns the number of tasks
 // and adds their evaluations / predicted pairs to *evals / *pred.
@@ -526,9 +551,10 @@ uint32_t cell_tasks(const Ctx &c, uint32_t A, bool sym, uint64_t cap, double pai
     const uint32_t nb0 = c.hNbrStart[A], nb1 = c.hNbrStart[A + 1];
     const uint32_t nSegAll = 1 + (nb1 - nb0);
     const double rate = c.cellRate.empty() ? 0.0 : c.cellRate[A];
+    const uint32_t tile = SJ_CTA * (uint32_t)sj_query_slots(c.g.Dp, c.p.precision == SJ_PREC_FP32_REFINE);
     uint32_t made = 0;
-    for (uint32_t q0 = 0; q0 < occ; q0 += SJ_CTA) {
-        const uint32_t qc = std::min<uint32_t>(SJ_CTA, occ - q0);
+    for (uint32_t q0 = 0; q0 < occ; q0 += tile) {
+        const uint32_t qc = std::min<uint32_t>(tile, occ - q0);
         const uint32_t qBegin = aStart + q0;
         // chunk length from the predicted pair density of this cell, and never
         // more candidates than keep the worst case (every candidate a hit, both
@@ -753,7 +779,11 @@ sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
     a.capacity = cap;
     a.stat = c.stat.p;
     a.taskHits = c.taskHits.p;
-    a.margin = filter_margin(c);
+    {
+        const FilterBounds fb = filter_bounds(c);
+        a.margin = fb.margin;
+        a.delta = fb.delta;
+    }
 
     std::vector<uint32_t> hTaskHits(nt);
     uint64_t pairsTotal = 0, batches = 0, retries = 0;
@@ -978,7 +1008,11 @@ sj_status run_degrees(Ctx &c, uint32_t *degHost)
     a.queueHead = c.queueHead.p;
     a.keyCount = c.keyCount.p;
     a.stat = c.stat.p;
-    a.margin = filter_margin(c);
+    {
+        const FilterBounds fb = filter_bounds(c);
+        a.margin = fb.margin;
+        a.delta = fb.delta;
+    }
     a.taskBegin = 0;
     a.taskEnd = nt;
     CKS(run_pass(c, a, false, true));

@@ -15,6 +15,15 @@
 #define SJ_HID 64            // learned-estimator hidden width
 #define SJ_NOUT 2            // learned-estimator outputs (log distance calcs, log hits)
 
+// Query slots per join thread: a join task covers up to SJ_CTA * slots query
+// points of one cell (each thread evaluates every staged candidate against
+// `slots` queries held in registers).
+constexpr int sj_query_slots(int Dp, bool fp32)
+{
+    (void)fp32;
+    return Dp <= 8 ? 4 : 2;
+}
+
 // Traversal (neighbour ownership) patterns, mapped from the reference's search modes.
 enum sj_pattern { SJ_PAT_FULL = 0, SJ_PAT_UNICOMP = 1, SJ_PAT_BUNICOMP = 2, SJ_PAT_LID = 3 };
 
@@ -68,7 +77,8 @@ struct sj_join_args {
                                 // [4] set hash, [5] batches skipped for overflow
     unsigned long long *batchPairs;  // this batch's pair total (count pass adds, later passes read)
     uint32_t *taskHits;         // optional per-task measured pairs (count pass)
-    double margin;              // FP32 filter half-band on the squared distance
+    double margin;              // FP32 filter: bound M on |FP32 estimate - (FP64 d2 - T)|
+    float delta;                // FP32 filter: width of the borderline band (>= 2M plus threshold rounding)
 };
 
 // Kernel launches made by this library since load (every launcher calls

@@ -1,20 +1,23 @@
 // The distance join: count pass and fill pass over cell tasks.
 //
-// One CTA of 128 threads takes a task: up to 128 query points of one cell
-// (one per thread, coordinates in registers) against a stretch of that cell's
-// candidate stream (home cell + owned neighbour cells, kernel.cu:1403-1538 in
-// the reference).  Candidates are staged in shared memory in steps of
-// SJ_STAGE and read by every thread as broadcasts.  Each thread builds a
-// 32-bit hit mask per block of 32 candidates; a 5-step butterfly transposes the
-// warp's 32x32 mask so that lane L holds candidate L's hits for the mirrored
-// direction (symmetric traversals emit (p,q) and (q,p) from one evaluation).
+// One CTA of 128 threads takes a task: up to 128*R query points of one cell
+// (R query "slots" of 128; thread t holds queries t, t+128, ... in registers)
+// against a stretch of that cell's candidate stream (home cell + owned
+// neighbour cells, kernel.cu:1403-1538 in the reference).  Candidates are
+// staged in shared memory in steps of SJ_STAGE and read as broadcasts; each
+// staged candidate is loaded once per thread and evaluated against all R of
+// its queries.  Per block of 32 candidates each thread builds a 32-bit hit mask
+// per slot; a 5-step butterfly transposes a warp's 32x32 mask so that lane L
+// holds candidate L's hits for the mirrored direction (symmetric traversals
+// emit (p,q) and (q,p) from one evaluation).
 //
 // count pass: per-key pair counts (the row lengths of this batch).
 // fill pass : keys are placed at exclusive offsets of those counts, so every
 //             key's values land contiguously and keys come out ascending --
 //             the order thrust::sort_by_key gives the reference (GPU.cu:2336)
-//             without sorting.  Each key's share of a 32x32 block is written as
-//             one run by the whole warp (ballot rank -> consecutive addresses).
+//             without sorting.  Dense blocks write each key's share as one run
+//             by the whole warp (ballot rank -> consecutive addresses); sparse
+//             blocks stage their short runs in shared memory and copy them out.
 //
 // Predicate (kernel.cu:344-349): the squared distance in the reference build's
 // rounding order (ref_dist2), hit iff sqrt(acc) <= eps, evaluated as acc <= T
@@ -22,7 +25,7 @@
 // monotonicity of the correctly rounded square root).
 // FP32 filter: acc32 = |b|^2 + sum(-2 a_l b_l) in local coordinates around the
 // home cell's centre; pairs inside a proven error band of the threshold are
-// re-evaluated with the exact FP64 chain above, so the pair set is the FP64 set.
+// re-evaluated with the exact FP64 arithmetic, so the pair set is the FP64 set.
 #include "sj_internal.h"
 
 namespace {
@@ -74,16 +77,19 @@ __device__ __forceinline__ bool exact_hit(const double *__restrict__ xs, uint32_
 }
 
 template <int DP>
-struct Stage64 {
+struct __align__(16) Stage64 {
     static constexpr int S = (DP <= 8) ? SJ_STAGE : ((SJ_STAGE * 8 / DP) / 32) * 32;
     double c[S][DP];
 };
 
+// FP32 stage: candidates in pairs (2p, 2p+1) so that one packed f32x2
+// instruction evaluates a query against both; per pair, float2 0 holds the
+// two |b|^2 and float2 1+l the two local coordinates l.
 template <int DP>
-struct Stage32 {
-    static constexpr int CW = ((DP + 1 + 3) / 4) * 4;
+struct __align__(16) Stage32 {
+    static constexpr int CW2 = ((DP + 1) + 1) / 2 * 2;   // float2 per pair, even (16-byte rows)
     static constexpr int S = SJ_STAGE;
-    float c[S][CW];   // local coordinates, then |b|^2 at [DP]
+    float2 c[S / 2][CW2];
 };
 
 template <int DP, bool F32>
@@ -91,7 +97,160 @@ struct StageOf { using T = Stage64<DP>; };
 template <int DP>
 struct StageOf<DP, true> { using T = Stage32<DP>; };
 
-template <int DP, bool F32, bool FILL>
+// FP32 filter over one block of 32 staged candidates for slots 0..RR-1.
+//   y = (|b|^2 - tLo) + sum_l (-2 a_l) b_l      (packed f32x2: two candidates per op)
+//   z = y - delta
+// hit bit  <- sign(y): y <= 0 proves the FP64 predicate true;
+// near bit <- sign(z): z >= 0 proves it false; near & ~hit is the borderline band.
+// Bits are shifted in from candidate 31 down to 0, so bit i is candidate i.
+template <int DP, int RR, int R>
+__device__ __forceinline__ void eval_block_f32(const Stage32<DP> &st, uint32_t pb, const float2 (&qa)[R][DP],
+                                               const float2 (&nt)[R], float2 nd, uint32_t (&hit)[R],
+                                               uint32_t (&near)[R])
+{
+    constexpr int CW2 = Stage32<DP>::CW2;
+#pragma unroll
+    for (int p = 15; p >= 0; p--) {
+        const float4 *row = reinterpret_cast<const float4 *>(&st.c[pb + p][0]);
+        float2 y[RR];
+        {
+            const float4 v = row[0];
+            const float2 nb = make_float2(v.x, v.y);
+#pragma unroll
+            for (int r = 0; r < RR; r++) y[r] = __fadd2_rn(nb, nt[r]);
+            if (DP >= 1) {
+                const float2 b = make_float2(v.z, v.w);
+#pragma unroll
+                for (int r = 0; r < RR; r++) y[r] = __ffma2_rn(qa[r][0], b, y[r]);
+            }
+        }
+#pragma unroll
+        for (int h = 1; h < CW2 / 2; h++) {
+            const float4 v = row[h];
+            if (2 * h - 1 < DP) {
+                const float2 b = make_float2(v.x, v.y);
+#pragma unroll
+                for (int r = 0; r < RR; r++) y[r] = __ffma2_rn(qa[r][2 * h - 1], b, y[r]);
+            }
+            if (2 * h < DP) {
+                const float2 b = make_float2(v.z, v.w);
+#pragma unroll
+                for (int r = 0; r < RR; r++) y[r] = __ffma2_rn(qa[r][2 * h], b, y[r]);
+            }
+        }
+#pragma unroll
+        for (int r = 0; r < RR; r++) {
+            const float2 z = __fadd2_rn(y[r], nd);
+            hit[r] = __funnelshift_l(__float_as_uint(y[r].y), hit[r], 1);
+            hit[r] = __funnelshift_l(__float_as_uint(y[r].x), hit[r], 1);
+            near[r] = __funnelshift_l(__float_as_uint(z.y), near[r], 1);
+            near[r] = __funnelshift_l(__float_as_uint(z.x), near[r], 1);
+        }
+    }
+}
+
+// FP64 predicate over one block of 32 staged candidates for slots 0..RR-1, in
+// the reference's rounding order (ref_dist2).  acc >= 0, so acc <= T is the
+// sign of bits(acc) - (bits(T) + 1) as 64-bit integers.
+template <int DP, int RR, int R>
+__device__ __forceinline__ void eval_block_f64(const Stage64<DP> &st, uint32_t jb, const double (&q)[R][DP],
+                                               long long T1, uint32_t (&hit)[R])
+{
+#pragma unroll
+    for (int jj = 31; jj >= 0; jj--) {
+        const double *cb = &st.c[jb + jj][0];
+        double acc[RR];
+        {
+            const double c0 = cb[0];
+            if (DP == 1) {
+#pragma unroll
+                for (int r = 0; r < RR; r++) {
+                    const double d0 = __dsub_rn(c0, q[r][0]);
+                    acc[r] = __dmul_rn(d0, d0);
+                }
+            } else {
+                const double c1 = cb[DP > 1 ? 1 : 0];
+#pragma unroll
+                for (int r = 0; r < RR; r++) {
+                    const double d0 = __dsub_rn(c0, q[r][0]);
+                    const double d1 = __dsub_rn(c1, q[r][DP > 1 ? 1 : 0]);
+                    acc[r] = __fma_rn(d0, d0, __dmul_rn(d1, d1));
+                }
+            }
+        }
+#pragma unroll
+        for (int l = 2; l < DP; l++) {
+            const double cl = cb[l];
+#pragma unroll
+            for (int r = 0; r < RR; r++) {
+                const double d = __dsub_rn(cl, q[r][l]);
+                acc[r] = __fma_rn(d, d, acc[r]);
+            }
+        }
+#pragma unroll
+        for (int r = 0; r < RR; r++) {
+            const long long diff = __double_as_longlong(acc[r]) - T1;
+            hit[r] = __funnelshift_l((uint32_t)((unsigned long long)diff >> 32), hit[r], 1);
+        }
+    }
+}
+
+// Writes one direction of a block's pairs.  Lane x owns `mask` (bits = the
+// partner lanes of its key), a run of n slots reserved at `pos`, and its key;
+// partnerOf(b) is the value partner lane b contributes and myPartnerVal this
+// lane's own contribution.  maskT (lane b: bits = keys it partners) serves the
+// dense path.  Sparse blocks (<= EMIT_STAGE pairs) stage every lane's run in
+// shared memory and copy them out with all lanes; dense blocks take one warp
+// iteration per non-empty run, written coalesced by the partner lanes.
+template <class Partner>
+__device__ __forceinline__ void emit_block(uint32_t mask, uint32_t maskT, uint32_t n, uint32_t pos, uint32_t key,
+                                           uint32_t myPartnerVal, Partner partnerOf, int32_t *__restrict__ outKey,
+                                           int32_t *__restrict__ outVal, uint32_t *sS, uint32_t *sK, uint32_t *sV,
+                                           uint32_t lane, uint32_t ltmask)
+{
+    uint32_t inc = n;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= (uint32_t)o) inc += y;
+    }
+    const uint32_t tot = __shfl_sync(0xffffffffu, inc, 31);
+    if (tot == 0) return;
+    if (tot <= EMIT_STAGE) {
+        uint32_t m = n ? mask : 0u, at = inc - n, slot = pos;
+        while (m) {
+            const int b = __ffs(m) - 1;
+            m &= m - 1;
+            sS[at] = slot++;
+            sK[at] = key;
+            sV[at] = partnerOf(b);
+            at++;
+        }
+        __syncwarp();
+        for (uint32_t e = lane; e < tot; e += 32) {
+            outKey[sS[e]] = (int32_t)sK[e];
+            outVal[sS[e]] = (int32_t)sV[e];
+        }
+        __syncwarp();
+    } else {
+        uint32_t live = __ballot_sync(0xffffffffu, n != 0);
+        while (live) {
+            const int L = __ffs(live) - 1;
+            live &= live - 1;
+            const uint32_t base = __shfl_sync(0xffffffffu, pos, L);
+            const uint32_t k = __shfl_sync(0xffffffffu, key, L);
+            const bool h = (maskT >> L) & 1u;
+            const uint32_t b = __ballot_sync(0xffffffffu, h);
+            if (h) {
+                const uint32_t at = base + __popc(b & ltmask);
+                outKey[at] = (int32_t)k;
+                outVal[at] = (int32_t)myPartnerVal;
+            }
+        }
+    }
+}
+
+template <int DP, bool F32, bool FILL, int R>
 __global__ void __launch_bounds__(SJ_CTA) k_join(sj_join_args a, sj_grid_dev g, int queue)
 {
     using Stage = typename StageOf<DP, F32>::T;
@@ -105,7 +264,8 @@ __global__ void __launch_bounds__(SJ_CTA) k_join(sj_join_args a, sj_grid_dev g, 
     __shared__ uint32_t stSlot[FILL ? NW : 1][FILL ? EMIT_STAGE : 1];
     __shared__ uint32_t stKey[FILL ? NW : 1][FILL ? EMIT_STAGE : 1];
     __shared__ uint32_t stVal[FILL ? NW : 1][FILL ? EMIT_STAGE : 1];
-    __shared__ uint32_t qIdS[FILL ? SJ_CTA : 1];
+    __shared__ uint32_t qIdS[FILL ? R : 1][FILL ? SJ_CTA : 1];
+    __shared__ double originS[F32 ? DP : 1];
     __shared__ uint32_t scanTmp[NW];
     __shared__ uint32_t curTask;
     __shared__ unsigned long long taskPairs;
@@ -171,6 +331,14 @@ __global__ void __launch_bounds__(SJ_CTA) k_join(sj_join_args a, sj_grid_dev g, 
             locLen[r] = len;
             mySum += len;
         }
+        if (F32 && (int)tid < DP) {
+            // local-coordinate origin: home cell centre (indexed dims), data centre (others)
+            double o;
+            if ((int)tid < g.k) o = g.minArr[tid] + ((double)a.cellCoord[(uint64_t)cellA * g.k + tid] + 0.5) * g.eps;
+            else if ((int)tid < D) o = g.center[tid];
+            else o = 0.0;
+            originS[F32 ? tid : 0] = o;
+        }
         {
             // block exclusive scan of mySum
             uint32_t x = mySum;
@@ -195,39 +363,47 @@ __global__ void __launch_bounds__(SJ_CTA) k_join(sj_join_args a, sj_grid_dev g, 
         __syncthreads();
         const uint32_t homeEnd = (task.segBase == 0 && (task.flags & SJ_TASK_HOME)) ? segPre[1] : 0u;
 
-        // ---- query point of this thread
-        const uint32_t qi = tid;
-        const bool qValid = qi < task.qCount;
-        const uint32_t qpos = task.qBegin + (qValid ? qi : 0u);
-        const uint32_t qid = a.ids[qpos];
-        if (FILL) qIdS[tid] = qid;
-        double q64[F32 ? 1 : DP];
-        float q2[F32 ? DP : 1];
-        float thrLo = 0.f, thrHi = 0.f;
-        double origin[F32 ? DP : 1];
-        if (F32) {
-            double na = 0.0;
+        // ---- query points of this thread: slot r holds query r*128 + tid
+        // nAct: slots with at least one valid query in this warp (warp-uniform)
+        const uint32_t nAct = task.qCount > warp * 32
+                                  ? min((uint32_t)R, (task.qCount - warp * 32 + SJ_CTA - 1) / SJ_CTA)
+                                  : 0u;
+        uint32_t qid[R];
+        double q64[F32 ? 1 : R][F32 ? 1 : DP];
+        float2 qa[F32 ? R : 1][F32 ? DP : 1];   // (-2 a_l, -2 a_l)
+        float2 nt[R];                           // (-tLo, -tLo)
 #pragma unroll
-            for (int l = 0; l < DP; l++) {
-                double o;
-                if (l < g.k) o = g.minArr[l] + ((double)a.cellCoord[(uint64_t)cellA * g.k + l] + 0.5) * g.eps;
-                else if (l < D) o = g.center[l];
-                else o = 0.0;
-                origin[l] = o;
-                float qa = (l < D) ? __double2float_rn(a.xs[(uint64_t)qpos * DP + l] - o) : 0.0f;
-                q2[l] = -2.0f * qa;
-                na += (double)qa * (double)qa;
+        for (int r = 0; r < R; r++) {
+            const uint32_t qi = (uint32_t)r * SJ_CTA + tid;
+            const bool v = qi < task.qCount;
+            const uint32_t qpos = task.qBegin + (v ? qi : 0u);
+            qid[r] = a.ids[qpos];
+            if (FILL) qIdS[FILL ? r : 0][tid] = qid[r];
+            const double *src = a.xs + (uint64_t)qpos * DP;
+            if (F32) {
+                double na = 0.0;
+#pragma unroll
+                for (int l = 0; l < DP; l++) {
+                    const float ql = (l < D) ? __double2float_rn(src[l] - originS[F32 ? l : 0]) : 0.0f;
+                    qa[F32 ? r : 0][F32 ? l : 0] = make_float2(-2.0f * ql, -2.0f * ql);
+                    na += (double)ql * (double)ql;
+                }
+                const float tLo = __double2float_rd(T - na - a.margin);
+                nt[r] = make_float2(-tLo, -tLo);
+            } else {
+#pragma unroll
+                for (int l = 0; l < DP; l++) q64[F32 ? 0 : r][F32 ? 0 : l] = src[l];
+                nt[r] = make_float2(0.f, 0.f);
             }
-            thrLo = __double2float_rd(T - na - a.margin);
-            thrHi = __double2float_ru(T - na + a.margin);
-        } else {
-#pragma unroll
-            for (int l = 0; l < DP; l++) q64[l] = a.xs[(uint64_t)qpos * DP + l];
         }
+        const float2 nd = make_float2(-a.delta, -a.delta);
+        const long long T1 = __double_as_longlong(T) + 1;
 
-        uint32_t rowCount = 0;       // count pass: pairs keyed by this query
-        uint32_t evals = 0;          // candidate evaluations
-        uint32_t refined = 0;        // FP32 borderline re-evaluations
+        uint32_t rowCount[R];   // count pass: pairs keyed by each query
+        uint32_t evals = 0;     // candidate evaluations
+        uint32_t refined = 0;   // FP32 borderline re-evaluations
+#pragma unroll
+        for (int r = 0; r < R; r++) rowCount[r] = 0;
 
         // the stream can never extend past the segments actually present
         const uint32_t sEnd = min(task.sEnd, segPre[nSeg]);
@@ -245,16 +421,16 @@ __global__ void __launch_bounds__(SJ_CTA) k_join(sj_join_args a, sj_grid_dev g, 
                 uint32_t pos = segStart[lo] + (s - segPre[lo]);
                 candId[j] = a.ids[pos];
                 const double *src = a.xs + (uint64_t)pos * DP;
-                if (F32) {
-                    float *dst = reinterpret_cast<float *>(&st.c[j][0]);
+                if constexpr (F32) {
+                    float *dst = reinterpret_cast<float *>(&st.c[j >> 1][0]) + (j & 1);
                     double nb = 0.0;
 #pragma unroll
                     for (int l = 0; l < DP; l++) {
-                        float b = (l < D) ? __double2float_rn(src[l] - origin[l]) : 0.0f;
-                        dst[l] = b;
+                        float b = (l < D) ? __double2float_rn(src[l] - originS[F32 ? l : 0]) : 0.0f;
+                        dst[2 * (1 + l)] = b;
                         nb += (double)b * (double)b;
                     }
-                    dst[DP] = __double2float_rn(nb);
+                    dst[0] = __double2float_rn(nb);
                 } else {
                     double *dst = reinterpret_cast<double *>(&st.c[j][0]);
 #pragma unroll
@@ -262,168 +438,95 @@ __global__ void __launch_bounds__(SJ_CTA) k_join(sj_join_args a, sj_grid_dev g, 
                 }
             }
             __syncthreads();
-
-            for (uint32_t jb = 0; jb < nIn; jb += 32) {
+            // a warp without queries skips the evaluation (but not the barriers below)
+            for (uint32_t jb = 0; nAct != 0 && jb < nIn; jb += 32) {
                 const uint32_t nb = min(32u, nIn - jb);
                 const uint32_t inRange = (nb == 32) ? 0xffffffffu : ((1u << nb) - 1u);
-                uint32_t hits = 0, border = 0;
-                if (qValid) {
+                uint32_t hits[R], near[R];
 #pragma unroll
-                    for (int jj = 0; jj < 32; jj++) {
-                        if (jj < (int)nb) {
-                            const int j = jb + jj;
-                            if (F32) {
-                                const float *cb = reinterpret_cast<const float *>(&st.c[j][0]);
-                                float acc = cb[DP];
-#pragma unroll
-                                for (int l = 0; l < DP; l++) acc = fmaf(q2[l], cb[l], acc);
-                                if (acc <= thrLo) hits |= 1u << jj;
-                                else if (acc <= thrHi) border |= 1u << jj;
-                            } else {
-                                const double *cb = reinterpret_cast<const double *>(&st.c[j][0]);
-                                if (ref_dist2<DP>(cb, q64) <= T) hits |= 1u << jj;
-                            }
-                        }
-                    }
+                for (int r = 0; r < R; r++) { hits[r] = 0; near[r] = 0; }
+                // branch-free evaluation of the warp's active slots (a partly
+                // active slot set rounds up; the extra slots are ignored below)
+                if constexpr (F32) {
+                    if (nAct == 1) eval_block_f32<DP, 1, R>(st, jb >> 1, qa, nt, nd, hits, near);
+                    else if (R == 2 || nAct == 2) eval_block_f32<DP, (R >= 2 ? 2 : 1), R>(st, jb >> 1, qa, nt, nd, hits, near);
+                    else eval_block_f32<DP, R, R>(st, jb >> 1, qa, nt, nd, hits, near);
+                } else {
+                    if (nAct == 1) eval_block_f64<DP, 1, R>(st, jb, q64, T1, hits);
+                    else if (R == 2 || nAct == 2) eval_block_f64<DP, (R >= 2 ? 2 : 1), R>(st, jb, q64, T1, hits);
+                    else eval_block_f64<DP, R, R>(st, jb, q64, T1, hits);
                 }
-                // validity: the symmetric home segment keeps only cand >= query
-                uint32_t rowValid = inRange, mirValid = sym ? inRange : 0u;
                 const uint32_t blk = sBase + jb;
-                if (blk < homeEnd) {
-                    uint32_t hn = homeEnd - blk;
-                    uint32_t homeBits = hn >= 32 ? 0xffffffffu : ((1u << hn) - 1u);
-                    if (sym) {
-                        int lo = (int)qi - (int)blk;     // home cand index >= query index
-                        uint32_t ge = lo <= 0 ? 0xffffffffu : (lo >= 32 ? 0u : (0xffffffffu << lo));
-                        uint32_t gt = (lo + 1) <= 0 ? 0xffffffffu : ((lo + 1) >= 32 ? 0u : (0xffffffffu << (lo + 1)));
+#pragma unroll
+                for (int r = 0; r < R; r++) {
+                    if ((uint32_t)r >= nAct) continue;   // warp-uniform
+                    const uint32_t qi = (uint32_t)r * SJ_CTA + tid;
+                    const bool qValid = qi < task.qCount;
+                    // validity: the symmetric home segment keeps only cand >= query
+                    uint32_t rowValid = inRange, mirValid = sym ? inRange : 0u;
+                    if (sym && blk < homeEnd) {
+                        const uint32_t hn = homeEnd - blk;
+                        const uint32_t homeBits = hn >= 32 ? 0xffffffffu : ((1u << hn) - 1u);
+                        const int lo = (int)qi - (int)blk;   // home cand index >= query index
+                        const uint32_t ge = lo <= 0 ? 0xffffffffu : (lo >= 32 ? 0u : (0xffffffffu << lo));
+                        const uint32_t gt = (lo + 1) <= 0 ? 0xffffffffu
+                                          : ((lo + 1) >= 32 ? 0u : (0xffffffffu << (lo + 1)));
                         rowValid &= (~homeBits) | (homeBits & ge);
                         mirValid &= (~homeBits) | (homeBits & gt);
                     }
-                }
-                if (!qValid) { rowValid = 0; mirValid = 0; }
-                if (F32) {
-                    uint32_t bm = border & rowValid;
-                    while (bm) {
-                        int jj = __ffs(bm) - 1;
-                        bm &= bm - 1;
-                        uint32_t s = blk + jj;
-                        uint32_t lo = 0, hi = nSeg;
-                        while (hi - lo > 1) {
-                            uint32_t mid = (lo + hi) >> 1;
-                            if (segPre[mid] <= s) lo = mid; else hi = mid;
-                        }
-                        uint32_t cpos = segStart[lo] + (s - segPre[lo]);
-                        refined++;
-                        if (exact_hit<DP>(a.xs, cpos, qpos, T)) hits |= 1u << jj;
-                    }
-                }
-                evals += __popc(rowValid);
-                const uint32_t rowMask = hits & rowValid;   // lane = query, bit = candidate
-                const uint32_t mirRow = hits & mirValid;    // pairs also emitted with the candidate as key
-                if (FILL) {
-                    // rowT / mirT: lane j holds, for candidate jb+j, the bit mask of
-                    // this warp's queries it pairs with (one transpose suffices
-                    // outside the home diagonal, where both masks agree)
-                    const bool diag = sym && (blk < homeEnd);
-                    const uint32_t rowT = transpose32(rowMask, lane);
-                    const uint32_t mirT = sym ? (diag ? transpose32(mirRow, lane) : rowT) : 0u;
-                    const uint32_t cidL = candId[jb + lane];
-                    const uint32_t nRow = __popc(rowMask), nCol = __popc(mirT);
-                    uint32_t pRow = 0, pCol = 0;
-                    if (nRow) pRow = atomicAdd(&a.keyCursor[qid], nRow);
-                    if (nCol) pCol = atomicAdd(&a.keyCursor[cidL], nCol);
-                    // positions come from the counted offsets; a run past the end
-                    // would mean the two passes disagree
-                    const bool okRow = (uint64_t)pRow + nRow <= a.capacity;
-                    const bool okCol = (uint64_t)pCol + nCol <= a.capacity;
-                    if (!okRow || !okCol) atomicMax(&a.stat[3], 1ULL);
-                    // Two ways to write a block's pairs, chosen per direction:
-                    // dense blocks: one warp iteration per non-empty run (the
-                    // run is written coalesced by the lanes holding its members);
-                    // sparse blocks: every lane stages its own short run in shared
-                    // memory, then the warp copies the staged pairs out in order.
-                    const uint32_t nr = okRow ? nRow : 0u, nc = okCol ? nCol : 0u;
-                    uint32_t incR = nr, incC = nc;
-#pragma unroll
-                    for (int o = 1; o < 32; o <<= 1) {
-                        const uint32_t yr = __shfl_up_sync(0xffffffffu, incR, o);
-                        const uint32_t yc = __shfl_up_sync(0xffffffffu, incC, o);
-                        if (lane >= (uint32_t)o) { incR += yr; incC += yc; }
-                    }
-                    const uint32_t totR = __shfl_sync(0xffffffffu, incR, 31);
-                    const uint32_t totC = __shfl_sync(0xffffffffu, incC, 31);
-                    uint32_t* const sS = stSlot[FILL ? warp : 0];
-                    uint32_t* const sK = stKey[FILL ? warp : 0];
-                    uint32_t* const sV = stVal[FILL ? warp : 0];
-                    // row direction: key = this lane's query, values = candidates
-                    if (totR <= EMIT_STAGE) {
-                        uint32_t m = okRow ? rowMask : 0u, at = incR - nr, slot = pRow;
-                        while (m) {
-                            const int b = __ffs(m) - 1;
-                            m &= m - 1;
-                            sS[at] = slot++;
-                            sK[at] = qid;
-                            sV[at] = candId[jb + b];
-                            at++;
-                        }
-                        __syncwarp();
-                        for (uint32_t e = lane; e < totR; e += 32) {
-                            a.outKey[sS[e]] = (int32_t)sK[e];
-                            a.outVal[sS[e]] = (int32_t)sV[e];
-                        }
-                        __syncwarp();
-                    } else {
-                        uint32_t live = __ballot_sync(0xffffffffu, nr != 0);
-                        while (live) {
-                            const int L = __ffs(live) - 1;
-                            live &= live - 1;
-                            const uint32_t base = __shfl_sync(0xffffffffu, pRow, L);
-                            const uint32_t key = __shfl_sync(0xffffffffu, qid, L);
-                            const bool h = (rowT >> L) & 1u;
-                            const uint32_t b = __ballot_sync(0xffffffffu, h);
-                            if (h) {
-                                const uint32_t at = base + __popc(b & ltmask);
-                                a.outKey[at] = (int32_t)key;
-                                a.outVal[at] = (int32_t)cidL;
+                    if (!qValid) { rowValid = 0; mirValid = 0; }
+                    uint32_t h = hits[r];
+                    if (F32) {
+                        uint32_t bm = near[r] & ~h & rowValid;
+                        while (bm) {
+                            const int jj = __ffs(bm) - 1;
+                            bm &= bm - 1;
+                            const uint32_t s = blk + jj;
+                            uint32_t lo = 0, hi = nSeg;
+                            while (hi - lo > 1) {
+                                const uint32_t mid = (lo + hi) >> 1;
+                                if (segPre[mid] <= s) lo = mid; else hi = mid;
                             }
+                            const uint32_t cpos = segStart[lo] + (s - segPre[lo]);
+                            refined++;
+                            if (exact_hit<DP>(a.xs, cpos, task.qBegin + qi, T)) h |= 1u << jj;
                         }
                     }
-                    // column direction: key = this lane's candidate, values = queries
-                    if (totC <= EMIT_STAGE) {
-                        uint32_t m = okCol ? mirT : 0u, at = incC - nc, slot = pCol;
-                        while (m) {
-                            const int b = __ffs(m) - 1;
-                            m &= m - 1;
-                            sS[at] = slot++;
-                            sK[at] = cidL;
-                            sV[at] = qIdS[warp * 32 + b];
-                            at++;
-                        }
-                        __syncwarp();
-                        for (uint32_t e = lane; e < totC; e += 32) {
-                            a.outKey[sS[e]] = (int32_t)sK[e];
-                            a.outVal[sS[e]] = (int32_t)sV[e];
-                        }
-                        __syncwarp();
+                    evals += __popc(rowValid);
+                    const uint32_t rowMask = h & rowValid;   // lane = query, bit = candidate
+                    const uint32_t mirRow = h & mirValid;    // pairs also emitted with the candidate as key
+                    if (FILL) {
+                        // rowT / mirT: lane j holds, for candidate jb+j, the mask of
+                        // this warp's queries it pairs with (one transpose suffices
+                        // outside the home diagonal, where both masks agree)
+                        const bool diag = sym && (blk < homeEnd);
+                        const uint32_t rowT = transpose32(rowMask, lane);
+                        const uint32_t mirT = sym ? (diag ? transpose32(mirRow, lane) : rowT) : 0u;
+                        const uint32_t cidL = candId[jb + lane];
+                        const uint32_t nRow = __popc(rowMask), nCol = __popc(mirT);
+                        uint32_t pRow = 0, pCol = 0;
+                        if (nRow) pRow = atomicAdd(&a.keyCursor[qid[r]], nRow);
+                        if (nCol) pCol = atomicAdd(&a.keyCursor[cidL], nCol);
+                        // positions come from the counted offsets; a run past the
+                        // end would mean the two passes disagree
+                        const bool okRow = (uint64_t)pRow + nRow <= a.capacity;
+                        const bool okCol = (uint64_t)pCol + nCol <= a.capacity;
+                        if (!okRow || !okCol) atomicMax(&a.stat[3], 1ULL);
+                        uint32_t *const sS = stSlot[FILL ? warp : 0];
+                        uint32_t *const sK = stKey[FILL ? warp : 0];
+                        uint32_t *const sV = stVal[FILL ? warp : 0];
+                        // rows: key = this lane's query, values = candidates
+                        emit_block(rowMask, rowT, okRow ? nRow : 0u, pRow, qid[r], cidL,
+                                   [&](int b) { return candId[jb + b]; }, a.outKey, a.outVal, sS, sK, sV, lane,
+                                   ltmask);
+                        // columns: key = this lane's candidate, values = queries
+                        const uint32_t *qrow = &qIdS[FILL ? r : 0][warp * 32];
+                        emit_block(mirT, mirRow, okCol ? nCol : 0u, pCol, cidL, qid[r],
+                                   [&](int b) { return qrow[b]; }, a.outKey, a.outVal, sS, sK, sV, lane, ltmask);
                     } else {
-                        uint32_t live = __ballot_sync(0xffffffffu, nc != 0);
-                        while (live) {
-                            const int j = __ffs(live) - 1;
-                            live &= live - 1;
-                            const uint32_t base = __shfl_sync(0xffffffffu, pCol, j);
-                            const uint32_t key = __shfl_sync(0xffffffffu, cidL, j);
-                            const bool h = (mirRow >> j) & 1u;
-                            const uint32_t b = __ballot_sync(0xffffffffu, h);
-                            if (h) {
-                                const uint32_t at = base + __popc(b & ltmask);
-                                a.outKey[at] = (int32_t)key;
-                                a.outVal[at] = (int32_t)qid;
-                            }
-                        }
+                        rowCount[r] += __popc(rowMask);
+                        if (sym) colCnt[warp][jb + lane] += __popc(transpose32(mirRow, lane));
                     }
-                } else {
-                    rowCount += __popc(rowMask);
-                    if (sym) colCnt[warp][jb + lane] += __popc(transpose32(mirRow, lane));
                 }
             }
             if (!FILL && sym) {
@@ -439,21 +542,25 @@ __global__ void __launch_bounds__(SJ_CTA) k_join(sj_join_args a, sj_grid_dev g, 
             }
         }
         if (!FILL) {
-            if (rowCount) {
-                atomicAdd(&a.keyCount[qid], rowCount);
-                atomicAdd(&taskPairs, (unsigned long long)rowCount);
-            }
+            uint32_t mine = 0;
+#pragma unroll
+            for (int r = 0; r < R; r++)
+                if (rowCount[r]) {
+                    atomicAdd(&a.keyCount[qid[r]], rowCount[r]);
+                    mine += rowCount[r];
+                }
+            if (mine) atomicAdd(&taskPairs, (unsigned long long)mine);
         }
         // ---- statistics
-        unsigned long long e = evals, r = refined;
+        unsigned long long e = evals, rf = refined;
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
             e += __shfl_xor_sync(0xffffffffu, e, o);
-            r += __shfl_xor_sync(0xffffffffu, r, o);
+            rf += __shfl_xor_sync(0xffffffffu, rf, o);
         }
         if (FILL && lane == 0) {   // each task is filled exactly once
             if (e) atomicAdd(&a.stat[0], e);
-            if (r) atomicAdd(&a.stat[1], r);
+            if (rf) atomicAdd(&a.stat[1], rf);
         }
         if (!FILL) {
             __syncthreads();
@@ -468,37 +575,41 @@ __global__ void __launch_bounds__(SJ_CTA) k_join(sj_join_args a, sj_grid_dev g, 
     }
 }
 
+template <int DP, bool F32, bool FILL>
+int occupancy_of()
+{
+    static int occ = 0;
+    if (occ == 0) {
+        int b = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_join<DP, F32, FILL, sj_query_slots(DP, F32)>, SJ_CTA,
+                                                      0);
+        occ = b > 0 ? b : 4;
+    }
+    return occ;
+}
+
+template <int DP, bool F32, bool FILL>
+cudaError_t launch_one(const sj_join_args &a, const sj_grid_dev &g, int queue, int numSM, cudaStream_t s)
+{
+    const uint32_t nt = a.taskEnd - a.taskBegin;
+    if (nt == 0) return cudaSuccess;
+    // persistent queue: one full wave of resident CTAs
+    unsigned grid = queue ? (unsigned)(numSM * occupancy_of<DP, F32, FILL>()) : nt;
+    if (queue && grid > nt) grid = nt;
+    k_join<DP, F32, FILL, sj_query_slots(DP, F32)><<<grid, SJ_CTA, 0, s>>>(a, g, queue);
+    sj_note_launch();
+    return cudaGetLastError();
+}
+
 template <int DP>
 cudaError_t launch_dp(const sj_join_args &a, const sj_grid_dev &g, int fill, int fp32, int queue, int numSM,
                       cudaStream_t s)
 {
-    uint32_t nt = a.taskEnd - a.taskBegin;
-    if (nt == 0) return cudaSuccess;
-    // persistent queue: one full wave of resident CTAs
-    static int perSM[2][2] = {{0, 0}, {0, 0}};
-    int &occ = perSM[fp32 ? 1 : 0][fill ? 1 : 0];
-    if (queue && occ == 0) {
-        int b = 0;
-        if (fp32) {
-            if (fill) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_join<DP, true, true>, SJ_CTA, 0);
-            else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_join<DP, true, false>, SJ_CTA, 0);
-        } else {
-            if (fill) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_join<DP, false, true>, SJ_CTA, 0);
-            else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_join<DP, false, false>, SJ_CTA, 0);
-        }
-        occ = b > 0 ? b : 4;
-    }
-    unsigned grid = queue ? (unsigned)(numSM * occ) : nt;
-    if (queue && grid > nt) grid = nt;
-    if (fp32) {
-        if (fill) k_join<DP, true, true><<<grid, SJ_CTA, 0, s>>>(a, g, queue);
-        else k_join<DP, true, false><<<grid, SJ_CTA, 0, s>>>(a, g, queue);
-    } else {
-        if (fill) k_join<DP, false, true><<<grid, SJ_CTA, 0, s>>>(a, g, queue);
-        else k_join<DP, false, false><<<grid, SJ_CTA, 0, s>>>(a, g, queue);
-    }
-    sj_note_launch();
-    return cudaGetLastError();
+    if (fp32)
+        return fill ? launch_one<DP, true, true>(a, g, queue, numSM, s)
+                    : launch_one<DP, true, false>(a, g, queue, numSM, s);
+    return fill ? launch_one<DP, false, true>(a, g, queue, numSM, s)
+                : launch_one<DP, false, false>(a, g, queue, numSM, s);
 }
 
 }  // namespace
