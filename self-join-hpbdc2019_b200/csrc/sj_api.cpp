@@ -191,9 +191,15 @@ struct Ctx {
     DevBuf<int32_t> outKey, outVal;
     DevBuf<uint8_t> scanTemp;
     DevBuf<uint32_t> total;
-    DevBuf<unsigned long long> stat;   // evals, refined, pairs, overflow, hash
+    DevBuf<unsigned long long> stat;   // see sj_join_args::stat
     DevBuf<uint32_t> queueHead;
     DevBuf<uint32_t> taskHits;
+    DevBuf<uint32_t> dTaskEvals, dTaskRefined;   // per task, written by the count pass
+    // count-pass records for the emission pass: per task, [block][query] hit
+    // masks and per-query row counts (offsets: prefix sums over all tasks)
+    std::vector<uint64_t> hMaskOff, hRowOff;
+    DevBuf<uint64_t> dMaskOff, dRowOff;
+    DevBuf<uint32_t> masks, rowCnt;
     DevBuf<unsigned long long> batchTot;
     std::vector<cudaEvent_t> events;   // per-batch stage boundaries of the asynchronous phase
     PinBuf pinTotal, pinKey[2], pinVal[2];
@@ -433,9 +439,6 @@ void join_args_base(Ctx &c, sj_join_args &a)
     a.cellCoord = c.cellCoord.p;
 }
 
-// FP32 filter half-band: bound on |(acc32 - thr32) - (S64 - T)| for local
-// coordinates measured from the home cell's centre (indexed dims) or the data
-// centre (other dims).  |a_l| <= 0.5 eps, |b_l| <= 1.5 eps on indexed dims.
 // FP32 filter bounds.  Queries are taken relative to their home cell's centre
 // (indexed dims) or the data centre (others): |a| <= Ra; candidates lie in the
 // home cell or a neighbour: |b| <= Rb.  The kernel evaluates in FP32
@@ -676,13 +679,36 @@ struct BatchRange {
     uint32_t t0, t1;
 };
 
-sj_status run_pass(Ctx &c, sj_join_args &a, bool fill, bool queue)
+sj_status run_count(Ctx &c, sj_join_args &a, bool queue)
 {
     if (queue) CK(cudaMemsetAsync(c.queueHead.p, 0, sizeof(uint32_t), c.s));
-    CK(sj_launch_join(a, c.g, fill ? 1 : 0, c.p.precision == SJ_PREC_FP32_REFINE ? 1 : 0, queue ? 1 : 0, c.numSM,
-                      c.s));
+    CK(sj_launch_join(a, c.g, c.p.precision == SJ_PREC_FP32_REFINE ? 1 : 0, queue ? 1 : 0, c.numSM, c.s));
     return SJ_OK;
 }
+
+// Per-task record offsets of the count pass: ceil(stream length / 32) mask
+// words per query, and one row count per query.
+sj_status task_offsets(Ctx &c)
+{
+    const size_t nt = c.tasks.size();
+    c.hMaskOff.assign(nt + 1, 0);
+    c.hRowOff.assign(nt + 1, 0);
+    for (size_t i = 0; i < nt; i++) {
+        const sj_task &t = c.tasks[i];
+        const uint64_t blocks = ((uint64_t)(t.sEnd - t.sBegin) + 31) / 32;
+        c.hMaskOff[i + 1] = c.hMaskOff[i] + blocks * t.qCount;
+        c.hRowOff[i + 1] = c.hRowOff[i] + t.qCount;
+    }
+    CK(c.dMaskOff.ensure(nt + 1));
+    CK(c.dRowOff.ensure(nt + 1));
+    CK(cudaMemcpyAsync(c.dMaskOff.p, c.hMaskOff.data(), sizeof(uint64_t) * (nt + 1), cudaMemcpyHostToDevice, c.s));
+    CK(cudaMemcpyAsync(c.dRowOff.p, c.hRowOff.data(), sizeof(uint64_t) * (nt + 1), cudaMemcpyHostToDevice, c.s));
+    return SJ_OK;
+}
+
+// Hit-mask words one batch may record (4 bytes each); a batch is also cut
+// when its masks would exceed this.
+constexpr uint64_t SJ_MASK_BATCH_WORDS = 1ULL << 29;
 
 sj_status prepare_join(Ctx &c, int &pattern, bool &queue)
 {
@@ -731,6 +757,7 @@ sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
         if (!c.tasks.empty())
             CK(cudaMemcpyAsync(c.dTasks.p, c.tasks.data(), sizeof(sj_task) * c.tasks.size(), cudaMemcpyHostToDevice,
                                c.s));
+        CKS(task_offsets(c));
         c.st.ms_tasks += tm.stop(c.s);
     }
     const uint32_t nt = (uint32_t)c.tasks.size();
@@ -743,21 +770,26 @@ sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
     CK(c.queueHead.ensure(1));
     CK(c.taskHits.ensure(nt ? nt : 1));
     CK(cudaMemsetAsync(c.taskHits.p, 0, sizeof(uint32_t) * (nt ? nt : 1), c.s));
+    CK(c.dTaskEvals.ensure(nt ? nt : 1));
+    CK(c.dTaskRefined.ensure(nt ? nt : 1));
+    CK(cudaMemsetAsync(c.dTaskEvals.p, 0, sizeof(uint32_t) * (nt ? nt : 1), c.s));
+    CK(cudaMemsetAsync(c.dTaskRefined.p, 0, sizeof(uint32_t) * (nt ? nt : 1), c.s));
     CK(c.pinTotal.ensure(64));
     CK(cudaMemsetAsync(c.stat.p, 0, sizeof(unsigned long long) * 8, c.s));
     double predTotal = 0;
     for (double v : c.taskPred) predTotal += v;
     c.st.estimated_pairs = predTotal;
 
-    // greedy batch plan on predicted pairs
+    // greedy batch plan on predicted pairs (and on hit-mask words)
     std::vector<BatchRange> plan;
+    uint64_t maxMaskWords = 1, maxRowWords = 1;
     {
         const double alpha = c.p.alpha;
         uint32_t t0 = 0;
         double acc = 0;
         for (uint32_t t = 0; t < nt; t++) {
             double v = c.taskPred[t] * (1.0 + alpha);
-            if (t > t0 && acc + v > (double)cap) {
+            if (t > t0 && (acc + v > (double)cap || c.hMaskOff[t + 1] - c.hMaskOff[t0] > SJ_MASK_BATCH_WORDS)) {
                 plan.push_back({t0, t});
                 t0 = t;
                 acc = 0;
@@ -765,8 +797,14 @@ sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
             acc += v;
         }
         if (nt > t0) plan.push_back({t0, nt});
+        for (const BatchRange &br : plan) {
+            maxMaskWords = std::max<uint64_t>(maxMaskWords, c.hMaskOff[br.t1] - c.hMaskOff[br.t0]);
+            maxRowWords = std::max<uint64_t>(maxRowWords, c.hRowOff[br.t1] - c.hRowOff[br.t0]);
+        }
     }
     std::reverse(plan.begin(), plan.end());   // used as a stack
+    CK(c.masks.ensure(maxMaskWords));
+    CK(c.rowCnt.ensure(maxRowWords));
 
     sj_join_args a;
     join_args_base(c, a);
@@ -779,6 +817,12 @@ sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
     a.capacity = cap;
     a.stat = c.stat.p;
     a.taskHits = c.taskHits.p;
+    a.taskEvals = c.dTaskEvals.p;
+    a.taskRefined = c.dTaskRefined.p;
+    a.masks = c.masks.p;
+    a.maskOff = c.dMaskOff.p;
+    a.rowCnt = c.rowCnt.p;
+    a.rowOff = c.dRowOff.p;
     {
         const FilterBounds fb = filter_bounds(c);
         a.margin = fb.margin;
@@ -831,12 +875,14 @@ sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
             a.taskEnd = br.t1;
             a.batchPairs = c.batchTot.p + i;
             CK(cudaEventRecord(ev[6 * i + 0], c.s));
-            CKS(run_pass(c, a, false, queue));
+            CKS(run_count(c, a, queue));
             CK(cudaEventRecord(ev[6 * i + 1], c.s));
             CK(sj_exclusive_scan_u32_clear(c.keyCount.p, c.keyCursor.p, n, c.scanTemp.p, c.total.p, c.s));
             CK(cudaEventRecord(ev[6 * i + 2], c.s));
-            CKS(run_pass(c, a, true, queue));
+            CK(sj_expand_keys(c.keyCursor.p, c.total.p, n, a.outKey, a.batchPairs, a.capacity, c.s));
             CK(cudaEventRecord(ev[6 * i + 3], c.s));
+            if (queue) CK(cudaMemsetAsync(c.queueHead.p, 0, sizeof(uint32_t), c.s));
+            CK(sj_launch_emit(a, queue ? 1 : 0, c.numSM, c.s));
             CK(cudaEventRecord(ev[6 * i + 4], c.s));
             CK(sj_hash_pairs_dev(c.outKey.p, c.outVal.p, a.batchPairs, bufCap, bufCap, c.stat.p + 4, c.s));
             CK(cudaEventRecord(ev[6 * i + 5], c.s));
@@ -855,8 +901,8 @@ sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
             cudaEventElapsedTime(&t45, ev[6 * i + 4], ev[6 * i + 5]);
             msCount += t01;
             msScan += t12;
-            msFill += t23;
-            msExpand += t34;
+            msExpand += t23;
+            msFill += t34;
             msDeliver += t45;
         }
         for (size_t i = 0; i < nplan; i++) {
@@ -887,7 +933,7 @@ sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
         a.capacity = c.outKey.n;
         CK(cudaMemsetAsync(slot, 0, sizeof(unsigned long long), c.s));
         tb.start(c.s);
-        CKS(run_pass(c, a, false, queue));
+        CKS(run_count(c, a, queue));
         msCount += tb.stop(c.s);
         tb.start(c.s);
         CK(sj_exclusive_scan_u32_clear(c.keyCount.p, c.keyCursor.p, n, c.scanTemp.p, c.total.p, c.s));
@@ -921,7 +967,11 @@ sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
         a.outVal = c.outVal.p;
         a.capacity = c.outKey.n;
         tb.start(c.s);
-        CKS(run_pass(c, a, true, queue));
+        CK(sj_expand_keys(c.keyCursor.p, c.total.p, n, a.outKey, a.batchPairs, a.capacity, c.s));
+        msExpand += tb.stop(c.s);
+        tb.start(c.s);
+        if (queue) CK(cudaMemsetAsync(c.queueHead.p, 0, sizeof(uint32_t), c.s));
+        CK(sj_launch_emit(a, queue ? 1 : 0, c.numSM, c.s));
         msFill += tb.stop(c.s);
         tb.start(c.s);
         CK(sj_hash_pairs(c.outKey.p, c.outVal.p, cnt, c.stat.p + 4, c.s));
@@ -959,10 +1009,23 @@ sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
         set_error("internal: fill pass exceeded the counted capacity");
         return SJ_ERR_INTERNAL;
     }
+    {
+        std::vector<uint32_t> ev(nt), rf(nt);
+        if (nt) {
+            CK(cudaMemcpyAsync(ev.data(), c.dTaskEvals.p, sizeof(uint32_t) * nt, cudaMemcpyDeviceToHost, c.s));
+            CK(cudaMemcpyAsync(rf.data(), c.dTaskRefined.p, sizeof(uint32_t) * nt, cudaMemcpyDeviceToHost, c.s));
+            CK(cudaStreamSynchronize(c.s));
+        }
+        uint64_t se = 0, sr = 0;
+        for (uint32_t t = 0; t < nt; t++) {
+            se += ev[t];
+            sr += rf[t];
+        }
+        c.st.distance_calcs = se;
+        c.st.refined_pairs = sr;
+    }
     c.st.total_pairs = pairsTotal;
     c.st.pair_hash = hs[4];
-    c.st.distance_calcs = hs[0];
-    c.st.refined_pairs = hs[1];
     c.st.num_batches = batches;
     c.st.overflow_retries = retries;
     c.st.estimator_mean_abs_rel_err = batches ? relErrSum / (double)batches : 0.0;
@@ -1013,9 +1076,18 @@ sj_status run_degrees(Ctx &c, uint32_t *degHost)
         a.margin = fb.margin;
         a.delta = fb.delta;
     }
+    CK(c.dTaskEvals.ensure(nt ? nt : 1));
+    CK(c.dTaskRefined.ensure(nt ? nt : 1));
+    a.taskEvals = c.dTaskEvals.p;
+    a.taskRefined = c.dTaskRefined.p;
     a.taskBegin = 0;
     a.taskEnd = nt;
-    CKS(run_pass(c, a, false, true));
+    CKS(run_count(c, a, true));
+    std::vector<uint32_t> ev(nt), rf(nt);
+    if (nt) {
+        CK(cudaMemcpyAsync(ev.data(), c.dTaskEvals.p, sizeof(uint32_t) * nt, cudaMemcpyDeviceToHost, c.s));
+        CK(cudaMemcpyAsync(rf.data(), c.dTaskRefined.p, sizeof(uint32_t) * nt, cudaMemcpyDeviceToHost, c.s));
+    }
     std::vector<uint32_t> deg(n);
     CK(cudaMemcpyAsync(deg.data(), c.keyCount.p, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost, c.s));
     std::vector<uint32_t> ids(n);
@@ -1035,8 +1107,13 @@ sj_status run_degrees(Ctx &c, uint32_t *degHost)
     uint64_t tot = 0;
     for (uint64_t i = 0; i < n; i++) tot += deg[i];
     c.st.total_pairs = tot;
-    c.st.distance_calcs = hs[0];
-    c.st.refined_pairs = hs[1];
+    uint64_t se = 0, sr = 0;
+    for (uint32_t t = 0; t < nt; t++) {
+        se += ev[t];
+        sr += rf[t];
+    }
+    c.st.distance_calcs = se;
+    c.st.refined_pairs = sr;
     return SJ_OK;
 }
 

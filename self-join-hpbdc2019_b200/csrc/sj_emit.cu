@@ -1,0 +1,312 @@
+// The emission pass: pairs from the count pass's hit masks.
+//
+// The count pass (sj_join.cu) leaves, per task, a hit mask for every query and
+// block of 32 stream positions ([block][query] words, bit i = candidate
+// 32*block+i) and every query's row count; the exclusive scan of the per-key
+// counts gives each key's slot range in the batch buffer.  This pass writes
+// the values (the keys come from sj_expand_keys):
+//
+//   rows    : key = query, values = candidates.  One warp per query: its words
+//             of a chunk of 2048 stream positions spread over the lanes, a warp
+//             scan of their popcounts, set bits expanded into a per-warp shared
+//             buffer, copied out as one contiguous run.  One reservation
+//             (atomicAdd on the key's cursor) per query and task.
+//   columns : key = candidate, values = queries (symmetric tasks only, with the
+//             query itself dropped on the home diagonal).  One warp per block:
+//             the block's words of a group of 32 queries are transposed so that
+//             lane j holds candidate j's query bits; groups are taken four at a
+//             time, one reservation per candidate and group batch.
+//
+// Runs wider than the shared buffer are written directly by the whole warp,
+// one ballot per 32 candidates.  No distance is evaluated here, so the pass is
+// identical for both precisions.
+#include "sj_internal.h"
+#include "sj_device.cuh"
+
+#include <atomic>
+
+namespace {
+using namespace sjdev;
+
+constexpr int EW = 128;                    // threads per emission CTA
+constexpr int ENW = EW / 32;
+constexpr int CHUNK = 2048;                // stream positions whose candidate ids are held at once
+constexpr int EM_CAP = 512;                // staged entries per warp
+constexpr int GB = 4;                      // query groups (of 32) per column batch
+constexpr int MAXQ = SJ_CTA * 4;           // largest query tile (sj_query_slots <= 4)
+constexpr uint32_t NO_SLOT = 0xffffffffu;  // reservation refused (past capacity)
+
+struct EmitSmem {
+    uint32_t segStart[SJ_MAX_SEG];
+    uint32_t segPre[SJ_MAX_SEG + 1];
+    uint32_t candS[CHUNK];
+    uint32_t qIdS[MAXQ];
+    uint32_t rowPos[MAXQ];
+    uint32_t stV[ENW][EM_CAP];
+    uint32_t stP[ENW][EM_CAP];
+    uint32_t scanTmp[ENW];
+    uint32_t curTask;
+};
+
+__device__ __forceinline__ uint32_t warp_excl_scan(uint32_t n, uint32_t lane, uint32_t &total)
+{
+    uint32_t x = n;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= (uint32_t)o) x += y;
+    }
+    total = __shfl_sync(0xffffffffu, x, 31);
+    return x - n;
+}
+
+__global__ void __launch_bounds__(EW) k_emit(sj_join_args a, int queue)
+{
+    __shared__ EmitSmem sm;
+    const uint32_t tid = threadIdx.x;
+    const uint32_t lane = tid & 31u;
+    const uint32_t warp = tid >> 5;
+    const uint32_t ltmask = (1u << lane) - 1u;
+    // a batch whose count exceeded the output buffer is re-planned by the host
+    if (a.batchPairs && *a.batchPairs > a.capacity) {
+        if (tid == 0 && blockIdx.x == 0) atomicMax(&a.stat[5], 1ULL);
+        return;
+    }
+    uint32_t iter = 0;
+    for (;;) {
+        __syncthreads();
+        if (tid == 0)
+            sm.curTask = queue ? (a.taskBegin + atomicAdd(a.queueHead, 1u)) : (a.taskBegin + blockIdx.x + iter);
+        __syncthreads();
+        const uint32_t t = sm.curTask;
+        if (t >= a.taskEnd || (!queue && iter > 0)) break;
+        iter++;
+        const sj_task task = a.tasks[t];
+        const bool sym = (task.flags & SJ_TASK_SYM) != 0;
+        const uint32_t cellA = task.cell;
+        const uint32_t aStart = a.cellStart[cellA], aEnd = a.cellStart[cellA + 1];
+        const uint32_t nbrBase = a.nbrStart[cellA];
+        const uint32_t nSeg = task.segCount;
+        const uint32_t qc = task.qCount;
+
+        // ---- segment table (as the count pass builds it)
+        constexpr int PER = (SJ_MAX_SEG + EW - 1) / EW;
+        uint32_t locLen[PER];
+        uint32_t mySum = 0;
+#pragma unroll
+        for (int r = 0; r < PER; r++) {
+            const uint32_t s = tid * PER + r;
+            uint32_t len = 0;
+            if (s < nSeg) {
+                const uint32_t gs = task.segBase + s;
+                uint32_t st0, en;
+                if (gs == 0) {
+                    st0 = sym ? task.qBegin : aStart;
+                    en = aEnd;
+                } else {
+                    const uint32_t b = a.nbrCell[nbrBase + gs - 1];
+                    st0 = a.cellStart[b];
+                    en = a.cellStart[b + 1];
+                }
+                sm.segStart[s] = st0;
+                len = en - st0;
+            }
+            locLen[r] = len;
+            mySum += len;
+        }
+        {
+            uint32_t dummy;
+            const uint32_t ex = warp_excl_scan(mySum, lane, dummy);
+            if (lane == 31) sm.scanTmp[warp] = ex + mySum;
+            __syncthreads();
+            uint32_t run = ex;
+            for (uint32_t w = 0; w < warp; w++) run += sm.scanTmp[w];
+#pragma unroll
+            for (int r = 0; r < PER; r++) {
+                const uint32_t s = tid * PER + r;
+                if (s <= nSeg) sm.segPre[s] = run;
+                run += locLen[r];
+            }
+            if (tid == EW - 1) sm.segPre[nSeg] = run;
+        }
+        for (uint32_t qi = tid; qi < qc; qi += EW) sm.qIdS[qi] = a.ids[task.qBegin + qi];
+        __syncthreads();
+        const uint32_t homeEnd = (task.segBase == 0 && (task.flags & SJ_TASK_HOME)) ? sm.segPre[1] : 0u;
+        const uint32_t L = min(task.sEnd, sm.segPre[nSeg]) - task.sBegin;
+        const uint32_t *const masks = a.masks + (a.maskOff[t] - a.maskOff[a.taskBegin]);
+        const uint32_t *const rows = a.rowCnt + (a.rowOff[t] - a.rowOff[a.taskBegin]);
+
+        // ---- one row reservation per query and task
+        for (uint32_t qi = tid; qi < qc; qi += EW) {
+            const uint32_t c = rows[qi];
+            uint32_t pos = 0;
+            if (c) {
+                pos = atomicAdd(&a.keyCursor[sm.qIdS[qi]], c);
+                if ((uint64_t)pos + c > a.capacity) {
+                    atomicMax(&a.stat[3], 1ULL);
+                    pos = NO_SLOT;
+                }
+            }
+            sm.rowPos[qi] = pos;
+        }
+
+        const uint32_t nG = (qc + 31) / 32;
+        uint32_t *const stV = sm.stV[warp];
+        uint32_t *const stP = sm.stP[warp];
+        for (uint32_t c0 = 0; c0 < L; c0 += CHUNK) {
+            const uint32_t nC = min((uint32_t)CHUNK, L - c0);
+            __syncthreads();
+            for (uint32_t j = tid; j < nC; j += EW) {
+                const uint32_t s = task.sBegin + c0 + j;
+                uint32_t lo = 0, hi = nSeg;   // largest seg with segPre[seg] <= s
+                while (hi - lo > 1) {
+                    const uint32_t mid = (lo + hi) >> 1;
+                    if (sm.segPre[mid] <= s) lo = mid; else hi = mid;
+                }
+                sm.candS[j] = a.ids[sm.segStart[lo] + (s - sm.segPre[lo])];
+            }
+            __syncthreads();
+            const uint32_t nb = (nC + 31) / 32;
+            const uint64_t b0 = c0 / 32;
+
+            // ---- rows: one query per warp
+            for (uint32_t qi = warp; qi < qc; qi += ENW) {
+                const uint32_t w0 = lane < nb ? masks[(b0 + lane) * qc + qi] : 0u;
+                const uint32_t w1 = lane + 32 < nb ? masks[(b0 + lane + 32) * qc + qi] : 0u;
+                uint32_t T;
+                const uint32_t ex = warp_excl_scan(__popc(w0) + __popc(w1), lane, T);
+                if (T == 0) continue;
+                const uint32_t pos0 = sm.rowPos[qi];
+                __syncwarp();
+                if (lane == 0) sm.rowPos[qi] = (pos0 == NO_SLOT) ? NO_SLOT : pos0 + T;
+                if (pos0 == NO_SLOT) continue;
+                if (T <= (uint32_t)EM_CAP) {
+                    uint32_t k = ex;
+                    uint32_t m = w0;
+                    while (m) {
+                        const int b = __ffs(m) - 1;
+                        m &= m - 1;
+                        stV[k++] = sm.candS[lane * 32 + b];
+                    }
+                    m = w1;
+                    while (m) {
+                        const int b = __ffs(m) - 1;
+                        m &= m - 1;
+                        stV[k++] = sm.candS[(lane + 32) * 32 + b];
+                    }
+                    __syncwarp();
+                    for (uint32_t e = lane; e < T; e += 32) a.outVal[pos0 + e] = (int32_t)stV[e];
+                    __syncwarp();
+                } else {
+                    uint32_t off = 0;
+                    for (uint32_t bb = 0; bb < nb; bb++) {
+                        const uint32_t word = __shfl_sync(0xffffffffu, bb < 32 ? w0 : w1, bb & 31);
+                        const bool h = (word >> lane) & 1u;
+                        const uint32_t bal = __ballot_sync(0xffffffffu, h);
+                        if (h) a.outVal[pos0 + off + __popc(bal & ltmask)] = (int32_t)sm.candS[bb * 32 + lane];
+                        off += __popc(bal);
+                    }
+                }
+            }
+            if (!sym) continue;
+
+            // ---- columns: one block of 32 candidates per warp
+            for (uint32_t bb = warp; bb < nb; bb += ENW) {
+                const uint32_t blk = task.sBegin + c0 + bb * 32;   // absolute stream position
+                const uint32_t hb = home_bits(blk, homeEnd, true);
+                const uint32_t key = sm.candS[bb * 32 + lane];
+                const uint32_t *const wrow = masks + (b0 + bb) * qc;
+                for (uint32_t g0 = 0; g0 < nG; g0 += GB) {
+                    uint32_t rw[GB], cw[GB];
+                    uint32_t n = 0;
+#pragma unroll
+                    for (int gg = 0; gg < GB; gg++) {
+                        rw[gg] = cw[gg] = 0;
+                        if (g0 + gg < nG) {   // warp-uniform
+                            const uint32_t qi = (g0 + gg) * 32 + lane;
+                            const uint32_t w = qi < qc ? (wrow[qi] & mir_keep(qi, blk, hb)) : 0u;
+                            rw[gg] = w;
+                            cw[gg] = transpose32(w, lane);
+                            n += __popc(cw[gg]);
+                        }
+                    }
+                    uint32_t base = 0;
+                    bool bad = false;
+                    if (n) {
+                        base = atomicAdd(&a.keyCursor[key], n);
+                        if ((uint64_t)base + n > a.capacity) {
+                            atomicMax(&a.stat[3], 1ULL);
+                            bad = true;
+                        }
+                    }
+                    if (__any_sync(0xffffffffu, bad)) continue;
+                    uint32_t T;
+                    const uint32_t ex = warp_excl_scan(n, lane, T);
+                    if (T == 0) continue;
+                    if (T <= (uint32_t)EM_CAP) {
+                        uint32_t k = ex;
+#pragma unroll
+                        for (int gg = 0; gg < GB; gg++) {
+                            uint32_t m = cw[gg];
+                            while (m) {
+                                const int b = __ffs(m) - 1;
+                                m &= m - 1;
+                                stV[k] = sm.qIdS[(g0 + gg) * 32 + b];
+                                stP[k] = base + (k - ex);
+                                k++;
+                            }
+                        }
+                        __syncwarp();
+                        for (uint32_t e = lane; e < T; e += 32) a.outVal[stP[e]] = (int32_t)stV[e];
+                        __syncwarp();
+                    } else {
+                        uint32_t off = 0;
+#pragma unroll
+                        for (int gg = 0; gg < GB; gg++) {
+                            uint32_t live = __ballot_sync(0xffffffffu, cw[gg] != 0);
+                            while (live) {
+                                const int Lk = __ffs(live) - 1;
+                                live &= live - 1;
+                                const uint32_t pL = __shfl_sync(0xffffffffu, base + off, Lk);
+                                const bool h = (rw[gg] >> Lk) & 1u;
+                                const uint32_t bal = __ballot_sync(0xffffffffu, h);
+                                if (h) a.outVal[pL + __popc(bal & ltmask)] = (int32_t)sm.qIdS[(g0 + gg) * 32 + lane];
+                            }
+                            off += __popc(cw[gg]);
+                        }
+                    }
+                }
+            }
+        }
+    }
+}
+
+int emit_occupancy()
+{
+    constexpr int MAXDEV = 64;
+    static std::atomic<int> occ[MAXDEV];
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= MAXDEV) dev = 0;
+    int o = occ[dev].load();
+    if (o == 0) {
+        int b = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_emit, EW, 0);
+        o = b > 0 ? b : 1;
+        occ[dev].store(o);
+    }
+    return o;
+}
+
+}  // namespace
+
+cudaError_t sj_launch_emit(const sj_join_args &a, int queue, int numSM, cudaStream_t s)
+{
+    const uint32_t nt = a.taskEnd - a.taskBegin;
+    if (nt == 0) return cudaSuccess;
+    unsigned grid = queue ? (unsigned)(numSM * emit_occupancy()) : nt;
+    if (queue && grid > nt) grid = nt;
+    k_emit<<<grid, EW, 0, s>>>(a, queue);
+    sj_note_launch();
+    return cudaGetLastError();
+}

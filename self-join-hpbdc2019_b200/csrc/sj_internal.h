@@ -70,13 +70,21 @@ struct sj_join_args {
     uint32_t taskBegin, taskEnd;
     uint32_t *queueHead;        // persistent-queue cursor (work-queue modes)
     uint32_t *keyCount;         // count pass: per point-id pair counts
-    uint32_t *keyCursor;        // fill pass: per point-id write cursors (exclusive offsets)
-    int32_t *outKey, *outVal;   // fill pass output
+    uint32_t *keyCursor;        // emission: per point-id write cursors (exclusive offsets)
+    int32_t *outKey, *outVal;   // batch output (keys by sj_expand_keys, values by the emission)
     uint64_t capacity;          // pairs the output buffers hold
-    unsigned long long *stat;   // [0] evals, [1] refined, [2] pairs (count pass), [3] run past capacity,
-                                // [4] set hash, [5] batches skipped for overflow
+    unsigned long long *stat;   // [2] pairs (count pass), [3] run past capacity, [4] set hash,
+                                // [5] batches skipped for overflow
     unsigned long long *batchPairs;  // this batch's pair total (count pass adds, later passes read)
     uint32_t *taskHits;         // optional per-task measured pairs (count pass)
+    // count-pass records consumed by the emission pass (null: not recorded).
+    // Offsets are absolute over all tasks; a batch indexes from its first task's.
+    uint32_t *masks;            // per task: [block][query] hit masks (bit i = candidate 32*block+i)
+    const uint64_t *maskOff;    // per task: first mask word
+    uint32_t *rowCnt;           // per task and query: pairs keyed by the query
+    const uint64_t *rowOff;     // per task: first row count
+    uint32_t *taskEvals;        // per task: candidate evaluations
+    uint32_t *taskRefined;      // per task: FP32 borderline re-evaluations
     double margin;              // FP32 filter: bound M on |FP32 estimate - (FP64 d2 - T)|
     float delta;                // FP32 filter: width of the borderline band (>= 2M plus threshold rounding)
 };
@@ -106,9 +114,9 @@ cudaError_t sj_hash_pairs(const int32_t *key, const int32_t *val, uint64_t m,
 // same, with the pair count read on the device (skipped when it exceeds cap)
 cudaError_t sj_hash_pairs_dev(const int32_t *key, const int32_t *val, const unsigned long long *count, uint64_t cap,
                               uint64_t gridHint, unsigned long long *hashOut, cudaStream_t s);
-// keys of a batch from its row structure: rows are [cursor-count, cursor) after
-// the fill pass; also clears `count` for the next batch
-cudaError_t sj_expand_keys(uint32_t *count, const uint32_t *cursor, uint64_t n, int32_t *outKey,
+// keys of a batch from its row structure: key k owns [excl[k], excl[k+1])
+// (excl[n] = *total); skipped when the batch's count exceeds cap
+cudaError_t sj_expand_keys(const uint32_t *excl, const uint32_t *total, uint64_t n, int32_t *outKey,
                            const unsigned long long *batchPairs, uint64_t cap, cudaStream_t s);
 
 // index build (sj_index.cu)
@@ -129,9 +137,12 @@ cudaError_t sj_launch_neighbours(const uint64_t *cellLid, const uint32_t *cellCo
                                  uint32_t *nbrCountOrCell, uint64_t *candFull, float *feat, int pass,
                                  cudaStream_t s);
 
-// join (sj_join.cu)
-cudaError_t sj_launch_join(const sj_join_args &a, const sj_grid_dev &g, int fill, int fp32, int queue,
-                           int numSM, cudaStream_t s);
+// join (sj_join.cu): the count pass (per-key pair counts, hit masks)
+cudaError_t sj_launch_join(const sj_join_args &a, const sj_grid_dev &g, int fp32, int queue, int numSM,
+                           cudaStream_t s);
+// emission (sj_emit.cu): pair values from the recorded hit masks into the
+// counted row slots
+cudaError_t sj_launch_emit(const sj_join_args &a, int queue, int numSM, cudaStream_t s);
 
 // estimators (sj_estimate.cu)
 cudaError_t sj_launch_sample(const sj_join_args &a, const sj_grid_dev &g, uint32_t sampleStride,

@@ -1,4 +1,4 @@
-// The distance join: count pass and fill pass over cell tasks.
+// The distance join's count pass over cell tasks.
 //
 // One CTA of 128 threads takes a task: up to 128*R query points of one cell
 // (R query "slots" of 128; thread t holds queries t, t+128, ... in registers)
@@ -11,44 +11,30 @@
 // holds candidate L's hits for the mirrored direction (symmetric traversals
 // emit (p,q) and (q,p) from one evaluation).
 //
-// count pass: per-key pair counts (the row lengths of this batch).
-// fill pass : keys are placed at exclusive offsets of those counts, so every
-//             key's values land contiguously and keys come out ascending --
-//             the order thrust::sort_by_key gives the reference (GPU.cu:2336)
-//             without sorting.  Dense blocks write each key's share as one run
-//             by the whole warp (ballot rank -> consecutive addresses); sparse
-//             blocks stage their short runs in shared memory and copy them out.
+// The pass produces per-key pair counts (the row lengths of a batch) and
+// records every hit mask; the emission pass (sj_emit.cu) writes the pairs from
+// those masks at exclusive offsets of the counts, so each key's values land
+// contiguously and keys come out ascending -- the order thrust::sort_by_key
+// gives the reference (GPU.cu:2336) -- without sorting and without evaluating
+// any distance twice.
 //
 // Predicate (kernel.cu:344-349): the squared distance in the reference build's
 // rounding order (ref_dist2), hit iff sqrt(acc) <= eps, evaluated as acc <= T
 // with T the largest double whose rounded sqrt is <= eps (identical by
 // monotonicity of the correctly rounded square root).
-// FP32 filter: acc32 = |b|^2 + sum(-2 a_l b_l) in local coordinates around the
+// FP32 filter: |b|^2 - 2 a.b against T - |a|^2 in local coordinates around the
 // home cell's centre; pairs inside a proven error band of the threshold are
 // re-evaluated with the exact FP64 arithmetic, so the pair set is the FP64 set.
 #include "sj_internal.h"
+#include "sj_device.cuh"
+
+#include <atomic>
 
 namespace {
+using namespace sjdev;
 
 constexpr int NW = SJ_CTA / 32;
-constexpr int EMIT_STAGE = 256;   // staged emissions per warp and direction (sparse blocks)
 
-__device__ __forceinline__ uint32_t transpose32(uint32_t x, uint32_t lane)
-{
-    // Lane i holds row i of a 32x32 bit matrix; afterwards lane j holds column j.
-#pragma unroll
-    for (int s = 16; s > 0; s >>= 1) {
-        const uint32_t lo = (s == 16) ? 0x0000ffffu
-                          : (s == 8)  ? 0x00ff00ffu
-                          : (s == 4)  ? 0x0f0f0f0fu
-                          : (s == 2)  ? 0x33333333u
-                                      : 0x55555555u;
-        uint32_t y = __shfl_xor_sync(0xffffffffu, x, s);
-        if (lane & s) x = (x & ~lo) | ((y & ~lo) >> s);
-        else x = (x & lo) | ((y & lo) << s);
-    }
-    return x;
-}
 
 // Squared distance in the reference build's exact rounding order (pinned by
 // its own outputs): the first addition fuses the FIRST product,
@@ -109,7 +95,7 @@ __device__ __forceinline__ void eval_block_f32(const Stage32<DP> &st, uint32_t p
                                                uint32_t (&near)[R])
 {
     constexpr int CW2 = Stage32<DP>::CW2;
-#pragma unroll
+#pragma unroll 2
     for (int p = 15; p >= 0; p--) {
         const float4 *row = reinterpret_cast<const float4 *>(&st.c[pb + p][0]);
         float2 y[RR];
@@ -156,7 +142,7 @@ template <int DP, int RR, int R>
 __device__ __forceinline__ void eval_block_f64(const Stage64<DP> &st, uint32_t jb, const double (&q)[R][DP],
                                                long long T1, uint32_t (&hit)[R])
 {
-#pragma unroll
+#pragma unroll 2
     for (int jj = 31; jj >= 0; jj--) {
         const double *cb = &st.c[jb + jj][0];
         double acc[RR];
@@ -195,97 +181,49 @@ __device__ __forceinline__ void eval_block_f64(const Stage64<DP> &st, uint32_t j
     }
 }
 
-// Writes one direction of a block's pairs.  Lane x owns `mask` (bits = the
-// partner lanes of its key), a run of n slots reserved at `pos`, and its key;
-// partnerOf(b) is the value partner lane b contributes and myPartnerVal this
-// lane's own contribution.  maskT (lane b: bits = keys it partners) serves the
-// dense path.  Sparse blocks (<= EMIT_STAGE pairs) stage every lane's run in
-// shared memory and copy them out with all lanes; dense blocks take one warp
-// iteration per non-empty run, written coalesced by the partner lanes.
-template <class Partner>
-__device__ __forceinline__ void emit_block(uint32_t mask, uint32_t maskT, uint32_t n, uint32_t pos, uint32_t key,
-                                           uint32_t myPartnerVal, Partner partnerOf, int32_t *__restrict__ outKey,
-                                           int32_t *__restrict__ outVal, uint32_t *sS, uint32_t *sK, uint32_t *sV,
-                                           uint32_t lane, uint32_t ltmask)
-{
-    uint32_t inc = n;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
-        if (lane >= (uint32_t)o) inc += y;
-    }
-    const uint32_t tot = __shfl_sync(0xffffffffu, inc, 31);
-    if (tot == 0) return;
-    if (tot <= EMIT_STAGE) {
-        uint32_t m = n ? mask : 0u, at = inc - n, slot = pos;
-        while (m) {
-            const int b = __ffs(m) - 1;
-            m &= m - 1;
-            sS[at] = slot++;
-            sK[at] = key;
-            sV[at] = partnerOf(b);
-            at++;
-        }
-        __syncwarp();
-        for (uint32_t e = lane; e < tot; e += 32) {
-            outKey[sS[e]] = (int32_t)sK[e];
-            outVal[sS[e]] = (int32_t)sV[e];
-        }
-        __syncwarp();
-    } else {
-        uint32_t live = __ballot_sync(0xffffffffu, n != 0);
-        while (live) {
-            const int L = __ffs(live) - 1;
-            live &= live - 1;
-            const uint32_t base = __shfl_sync(0xffffffffu, pos, L);
-            const uint32_t k = __shfl_sync(0xffffffffu, key, L);
-            const bool h = (maskT >> L) & 1u;
-            const uint32_t b = __ballot_sync(0xffffffffu, h);
-            if (h) {
-                const uint32_t at = base + __popc(b & ltmask);
-                outKey[at] = (int32_t)k;
-                outVal[at] = (int32_t)myPartnerVal;
-            }
-        }
-    }
-}
+// Shared memory of one count-pass CTA.
+template <int DP, bool F32, int R>
+struct __align__(16) JoinSmem {
+    using Stage = typename StageOf<DP, F32>::T;
+    static constexpr int S = Stage::S;
+    Stage st;
+    uint32_t candId[S];
+    uint32_t segStart[SJ_MAX_SEG];
+    uint32_t segPre[SJ_MAX_SEG + 1];
+    uint32_t colCnt[NW][S];
+    double originS[F32 ? DP : 1];
+    uint32_t scanTmp[NW];
+    uint32_t curTask;
+    unsigned long long taskPairs;
+    unsigned long long taskEvals;
+    unsigned long long taskRefined;
+};
 
-template <int DP, bool F32, bool FILL, int R>
+// Count pass over tasks [taskBegin, taskEnd): per-key pair counts (keyCount,
+// both directions of symmetric tasks), the batch total, and -- when a.masks is
+// set -- every query's hit mask per block of 32 stream positions plus its row
+// count, which the emission pass turns into pairs without a second distance
+// evaluation.
+template <int DP, bool F32, int R>
 __global__ void __launch_bounds__(SJ_CTA) k_join(sj_join_args a, sj_grid_dev g, int queue)
 {
-    using Stage = typename StageOf<DP, F32>::T;
-    constexpr int S = Stage::S;
-    __shared__ Stage st;
-    __shared__ uint32_t candId[S];
-    __shared__ uint32_t segStart[SJ_MAX_SEG];
-    __shared__ uint32_t segPre[SJ_MAX_SEG + 1];
-    __shared__ uint32_t colCnt[FILL ? 1 : NW][FILL ? 1 : S];
-    // fill pass, sparse blocks: per-warp staging of (slot, key, value)
-    __shared__ uint32_t stSlot[FILL ? NW : 1][FILL ? EMIT_STAGE : 1];
-    __shared__ uint32_t stKey[FILL ? NW : 1][FILL ? EMIT_STAGE : 1];
-    __shared__ uint32_t stVal[FILL ? NW : 1][FILL ? EMIT_STAGE : 1];
-    __shared__ uint32_t qIdS[FILL ? R : 1][FILL ? SJ_CTA : 1];
-    __shared__ double originS[F32 ? DP : 1];
-    __shared__ uint32_t scanTmp[NW];
-    __shared__ uint32_t curTask;
-    __shared__ unsigned long long taskPairs;
+    using Smem = JoinSmem<DP, F32, R>;
+    constexpr int S = Smem::S;
+    __shared__ Smem sm;
+    auto &st = sm.st;
+    auto &candId = sm.candId;
+    auto &segStart = sm.segStart;
+    auto &segPre = sm.segPre;
+    auto &colCnt = sm.colCnt;
+    auto &originS = sm.originS;
 
     const uint32_t tid = threadIdx.x;
     const uint32_t lane = tid & 31u;
     const uint32_t warp = tid >> 5;
-    const uint32_t ltmask = (1u << lane) - 1u;
     const int D = g.D;
-    // fill pass of a batch whose count exceeded the output buffer: skip it
-    // (the host re-plans it); the count pass always runs
-    if (FILL && a.batchPairs && *a.batchPairs > a.capacity) {
-        if (tid == 0 && blockIdx.x == 0) atomicMax(&a.stat[5], 1ULL);
-        return;
-    }
     const double T = g.thresh;
 
-    if (!FILL) {
-        for (int j = tid; j < NW * S; j += SJ_CTA) (&colCnt[0][0])[j] = 0;
-    }
+    for (int j = tid; j < NW * S; j += SJ_CTA) (&colCnt[0][0])[j] = 0;
 
     uint32_t iter = 0;
     for (;;) {
@@ -293,11 +231,13 @@ __global__ void __launch_bounds__(SJ_CTA) k_join(sj_join_args a, sj_grid_dev g, 
         __syncthreads();
         if (tid == 0) {
             uint32_t t = queue ? (a.taskBegin + atomicAdd(a.queueHead, 1u)) : (a.taskBegin + blockIdx.x + iter);
-            curTask = t;
-            taskPairs = 0ULL;
+            sm.curTask = t;
+            sm.taskPairs = 0ULL;
+            sm.taskEvals = 0ULL;
+            sm.taskRefined = 0ULL;
         }
         __syncthreads();
-        const uint32_t t = curTask;
+        const uint32_t t = sm.curTask;
         if (t >= a.taskEnd || (!queue && iter > 0)) break;
         iter++;
         const sj_task task = a.tasks[t];
@@ -347,10 +287,10 @@ __global__ void __launch_bounds__(SJ_CTA) k_join(sj_join_args a, sj_grid_dev g, 
                 uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
                 if (lane >= (uint32_t)o) x += y;
             }
-            if (lane == 31) scanTmp[warp] = x;
+            if (lane == 31) sm.scanTmp[warp] = x;
             __syncthreads();
             uint32_t wpre = 0;
-            for (uint32_t w = 0; w < warp; w++) wpre += scanTmp[w];
+            for (uint32_t w = 0; w < warp; w++) wpre += sm.scanTmp[w];
             uint32_t run = wpre + x - mySum;
 #pragma unroll
             for (int r = 0; r < (SJ_MAX_SEG + SJ_CTA - 1) / SJ_CTA; r++) {
@@ -378,7 +318,6 @@ __global__ void __launch_bounds__(SJ_CTA) k_join(sj_join_args a, sj_grid_dev g, 
             const bool v = qi < task.qCount;
             const uint32_t qpos = task.qBegin + (v ? qi : 0u);
             qid[r] = a.ids[qpos];
-            if (FILL) qIdS[FILL ? r : 0][tid] = qid[r];
             const double *src = a.xs + (uint64_t)qpos * DP;
             if (F32) {
                 double na = 0.0;
@@ -398,8 +337,9 @@ __global__ void __launch_bounds__(SJ_CTA) k_join(sj_join_args a, sj_grid_dev g, 
         }
         const float2 nd = make_float2(-a.delta, -a.delta);
         const long long T1 = __double_as_longlong(T) + 1;
+        uint32_t *const maskBase = a.masks ? a.masks + (a.maskOff[t] - a.maskOff[a.taskBegin]) : nullptr;
 
-        uint32_t rowCount[R];   // count pass: pairs keyed by each query
+        uint32_t rowCount[R];   // pairs keyed by each query
         uint32_t evals = 0;     // candidate evaluations
         uint32_t refined = 0;   // FP32 borderline re-evaluations
 #pragma unroll
@@ -438,7 +378,9 @@ __global__ void __launch_bounds__(SJ_CTA) k_join(sj_join_args a, sj_grid_dev g, 
                 }
             }
             __syncthreads();
-            // a warp without queries skips the evaluation (but not the barriers below)
+            // ---- hit masks of every block of the stage.  A warp without
+            // queries skips the evaluation (but not the barriers).
+#pragma unroll 1
             for (uint32_t jb = 0; nAct != 0 && jb < nIn; jb += 32) {
                 const uint32_t nb = min(32u, nIn - jb);
                 const uint32_t inRange = (nb == 32) ? 0xffffffffu : ((1u << nb) - 1u);
@@ -449,32 +391,20 @@ __global__ void __launch_bounds__(SJ_CTA) k_join(sj_join_args a, sj_grid_dev g, 
                 // active slot set rounds up; the extra slots are ignored below)
                 if constexpr (F32) {
                     if (nAct == 1) eval_block_f32<DP, 1, R>(st, jb >> 1, qa, nt, nd, hits, near);
-                    else if (R == 2 || nAct == 2) eval_block_f32<DP, (R >= 2 ? 2 : 1), R>(st, jb >> 1, qa, nt, nd, hits, near);
                     else eval_block_f32<DP, R, R>(st, jb >> 1, qa, nt, nd, hits, near);
                 } else {
                     if (nAct == 1) eval_block_f64<DP, 1, R>(st, jb, q64, T1, hits);
-                    else if (R == 2 || nAct == 2) eval_block_f64<DP, (R >= 2 ? 2 : 1), R>(st, jb, q64, T1, hits);
                     else eval_block_f64<DP, R, R>(st, jb, q64, T1, hits);
                 }
                 const uint32_t blk = sBase + jb;
+                const uint32_t hb = home_bits(blk, homeEnd, sym);
+                const uint64_t blockIdxInTask = (blk - task.sBegin) >> 5;
 #pragma unroll
                 for (int r = 0; r < R; r++) {
                     if ((uint32_t)r >= nAct) continue;   // warp-uniform
                     const uint32_t qi = (uint32_t)r * SJ_CTA + tid;
                     const bool qValid = qi < task.qCount;
-                    // validity: the symmetric home segment keeps only cand >= query
-                    uint32_t rowValid = inRange, mirValid = sym ? inRange : 0u;
-                    if (sym && blk < homeEnd) {
-                        const uint32_t hn = homeEnd - blk;
-                        const uint32_t homeBits = hn >= 32 ? 0xffffffffu : ((1u << hn) - 1u);
-                        const int lo = (int)qi - (int)blk;   // home cand index >= query index
-                        const uint32_t ge = lo <= 0 ? 0xffffffffu : (lo >= 32 ? 0u : (0xffffffffu << lo));
-                        const uint32_t gt = (lo + 1) <= 0 ? 0xffffffffu
-                                          : ((lo + 1) >= 32 ? 0u : (0xffffffffu << (lo + 1)));
-                        rowValid &= (~homeBits) | (homeBits & ge);
-                        mirValid &= (~homeBits) | (homeBits & gt);
-                    }
-                    if (!qValid) { rowValid = 0; mirValid = 0; }
+                    const uint32_t rowValid = qValid ? (inRange & row_keep(qi, blk, hb)) : 0u;
                     uint32_t h = hits[r];
                     if (F32) {
                         uint32_t bm = near[r] & ~h & rowValid;
@@ -494,42 +424,12 @@ __global__ void __launch_bounds__(SJ_CTA) k_join(sj_join_args a, sj_grid_dev g, 
                     }
                     evals += __popc(rowValid);
                     const uint32_t rowMask = h & rowValid;   // lane = query, bit = candidate
-                    const uint32_t mirRow = h & mirValid;    // pairs also emitted with the candidate as key
-                    if (FILL) {
-                        // rowT / mirT: lane j holds, for candidate jb+j, the mask of
-                        // this warp's queries it pairs with (one transpose suffices
-                        // outside the home diagonal, where both masks agree)
-                        const bool diag = sym && (blk < homeEnd);
-                        const uint32_t rowT = transpose32(rowMask, lane);
-                        const uint32_t mirT = sym ? (diag ? transpose32(mirRow, lane) : rowT) : 0u;
-                        const uint32_t cidL = candId[jb + lane];
-                        const uint32_t nRow = __popc(rowMask), nCol = __popc(mirT);
-                        uint32_t pRow = 0, pCol = 0;
-                        if (nRow) pRow = atomicAdd(&a.keyCursor[qid[r]], nRow);
-                        if (nCol) pCol = atomicAdd(&a.keyCursor[cidL], nCol);
-                        // positions come from the counted offsets; a run past the
-                        // end would mean the two passes disagree
-                        const bool okRow = (uint64_t)pRow + nRow <= a.capacity;
-                        const bool okCol = (uint64_t)pCol + nCol <= a.capacity;
-                        if (!okRow || !okCol) atomicMax(&a.stat[3], 1ULL);
-                        uint32_t *const sS = stSlot[FILL ? warp : 0];
-                        uint32_t *const sK = stKey[FILL ? warp : 0];
-                        uint32_t *const sV = stVal[FILL ? warp : 0];
-                        // rows: key = this lane's query, values = candidates
-                        emit_block(rowMask, rowT, okRow ? nRow : 0u, pRow, qid[r], cidL,
-                                   [&](int b) { return candId[jb + b]; }, a.outKey, a.outVal, sS, sK, sV, lane,
-                                   ltmask);
-                        // columns: key = this lane's candidate, values = queries
-                        const uint32_t *qrow = &qIdS[FILL ? r : 0][warp * 32];
-                        emit_block(mirT, mirRow, okCol ? nCol : 0u, pCol, cidL, qid[r],
-                                   [&](int b) { return qrow[b]; }, a.outKey, a.outVal, sS, sK, sV, lane, ltmask);
-                    } else {
-                        rowCount[r] += __popc(rowMask);
-                        if (sym) colCnt[warp][jb + lane] += __popc(transpose32(mirRow, lane));
-                    }
+                    if (maskBase && qValid) maskBase[blockIdxInTask * task.qCount + qi] = rowMask;
+                    rowCount[r] += __popc(rowMask);
+                    if (sym) colCnt[warp][jb + lane] += __popc(transpose32(rowMask & mir_keep(qi, blk, hb), lane));
                 }
             }
-            if (!FILL && sym) {
+            if (sym) {
                 __syncthreads();
                 uint32_t local = 0;
                 for (uint32_t j = tid; j < nIn; j += SJ_CTA) {
@@ -538,94 +438,99 @@ __global__ void __launch_bounds__(SJ_CTA) k_join(sj_join_args a, sj_grid_dev g, 
                     for (int w = 0; w < NW; w++) { tot += colCnt[w][j]; colCnt[w][j] = 0; }
                     if (tot) { atomicAdd(&a.keyCount[candId[j]], tot); local += tot; }
                 }
-                if (local) atomicAdd(&taskPairs, (unsigned long long)local);
+                if (local) atomicAdd(&sm.taskPairs, (unsigned long long)local);
             }
         }
-        if (!FILL) {
+        {
             uint32_t mine = 0;
+            uint32_t *const rowBase = a.rowCnt ? a.rowCnt + (a.rowOff[t] - a.rowOff[a.taskBegin]) : nullptr;
 #pragma unroll
-            for (int r = 0; r < R; r++)
+            for (int r = 0; r < R; r++) {
+                const uint32_t qi = (uint32_t)r * SJ_CTA + tid;
+                if (rowBase && qi < task.qCount) rowBase[qi] = rowCount[r];
                 if (rowCount[r]) {
                     atomicAdd(&a.keyCount[qid[r]], rowCount[r]);
                     mine += rowCount[r];
                 }
-            if (mine) atomicAdd(&taskPairs, (unsigned long long)mine);
+            }
+            if (mine) atomicAdd(&sm.taskPairs, (unsigned long long)mine);
         }
-        // ---- statistics
+        // ---- statistics (per task: a re-run of the task overwrites them)
         unsigned long long e = evals, rf = refined;
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
             e += __shfl_xor_sync(0xffffffffu, e, o);
             rf += __shfl_xor_sync(0xffffffffu, rf, o);
         }
-        if (FILL && lane == 0) {   // each task is filled exactly once
-            if (e) atomicAdd(&a.stat[0], e);
-            if (rf) atomicAdd(&a.stat[1], rf);
+        if (lane == 0) {
+            if (e) atomicAdd(&sm.taskEvals, e);
+            if (rf) atomicAdd(&sm.taskRefined, rf);
         }
-        if (!FILL) {
-            __syncthreads();
-            if (tid == 0) {
-                if (taskPairs) {
-                    atomicAdd(&a.stat[2], taskPairs);
-                    if (a.batchPairs) atomicAdd(a.batchPairs, taskPairs);
-                }
-                if (a.taskHits) a.taskHits[t] = (uint32_t)min(taskPairs, 0xffffffffULL);
+        __syncthreads();
+        if (tid == 0) {
+            const unsigned long long tp = sm.taskPairs;
+            if (tp) {
+                atomicAdd(&a.stat[2], tp);
+                if (a.batchPairs) atomicAdd(a.batchPairs, tp);
             }
+            if (a.taskHits) a.taskHits[t] = (uint32_t)min(tp, 0xffffffffULL);
+            if (a.taskEvals) a.taskEvals[t] = (uint32_t)min(sm.taskEvals, 0xffffffffULL);
+            if (a.taskRefined) a.taskRefined[t] = (uint32_t)min(sm.taskRefined, 0xffffffffULL);
         }
     }
 }
 
-template <int DP, bool F32, bool FILL>
+template <int DP, bool F32>
 int occupancy_of()
 {
-    static int occ = 0;
-    if (occ == 0) {
+    constexpr int MAXDEV = 64;
+    static std::atomic<int> occ[MAXDEV];   // per device ordinal, 0 = not measured yet
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= MAXDEV) dev = 0;
+    int o = occ[dev].load();
+    if (o == 0) {
         int b = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_join<DP, F32, FILL, sj_query_slots(DP, F32)>, SJ_CTA,
-                                                      0);
-        occ = b > 0 ? b : 4;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_join<DP, F32, sj_query_slots(DP, F32)>, SJ_CTA, 0);
+        o = b > 0 ? b : 1;
+        occ[dev].store(o);
     }
-    return occ;
+    return o;
 }
 
-template <int DP, bool F32, bool FILL>
+template <int DP, bool F32>
 cudaError_t launch_one(const sj_join_args &a, const sj_grid_dev &g, int queue, int numSM, cudaStream_t s)
 {
     const uint32_t nt = a.taskEnd - a.taskBegin;
     if (nt == 0) return cudaSuccess;
     // persistent queue: one full wave of resident CTAs
-    unsigned grid = queue ? (unsigned)(numSM * occupancy_of<DP, F32, FILL>()) : nt;
+    unsigned grid = queue ? (unsigned)(numSM * occupancy_of<DP, F32>()) : nt;
     if (queue && grid > nt) grid = nt;
-    k_join<DP, F32, FILL, sj_query_slots(DP, F32)><<<grid, SJ_CTA, 0, s>>>(a, g, queue);
+    k_join<DP, F32, sj_query_slots(DP, F32)><<<grid, SJ_CTA, 0, s>>>(a, g, queue);
     sj_note_launch();
     return cudaGetLastError();
 }
 
 template <int DP>
-cudaError_t launch_dp(const sj_join_args &a, const sj_grid_dev &g, int fill, int fp32, int queue, int numSM,
-                      cudaStream_t s)
+cudaError_t launch_dp(const sj_join_args &a, const sj_grid_dev &g, int fp32, int queue, int numSM, cudaStream_t s)
 {
-    if (fp32)
-        return fill ? launch_one<DP, true, true>(a, g, queue, numSM, s)
-                    : launch_one<DP, true, false>(a, g, queue, numSM, s);
-    return fill ? launch_one<DP, false, true>(a, g, queue, numSM, s)
-                : launch_one<DP, false, false>(a, g, queue, numSM, s);
+    return fp32 ? launch_one<DP, true>(a, g, queue, numSM, s) : launch_one<DP, false>(a, g, queue, numSM, s);
 }
 
 }  // namespace
 
-cudaError_t sj_launch_join(const sj_join_args &a, const sj_grid_dev &g, int fill, int fp32, int queue, int numSM,
+cudaError_t sj_launch_join(const sj_join_args &a, const sj_grid_dev &g, int fp32, int queue, int numSM,
                            cudaStream_t s)
 {
     switch (g.Dp) {
-    case 1: return launch_dp<1>(a, g, fill, fp32, queue, numSM, s);
-    case 2: return launch_dp<2>(a, g, fill, fp32, queue, numSM, s);
-    case 3: return launch_dp<3>(a, g, fill, fp32, queue, numSM, s);
-    case 4: return launch_dp<4>(a, g, fill, fp32, queue, numSM, s);
-    case 6: return launch_dp<6>(a, g, fill, fp32, queue, numSM, s);
-    case 8: return launch_dp<8>(a, g, fill, fp32, queue, numSM, s);
-    case 12: return launch_dp<12>(a, g, fill, fp32, queue, numSM, s);
-    case 16: return launch_dp<16>(a, g, fill, fp32, queue, numSM, s);
+    case 1: return launch_dp<1>(a, g, fp32, queue, numSM, s);
+    case 2: return launch_dp<2>(a, g, fp32, queue, numSM, s);
+    case 3: return launch_dp<3>(a, g, fp32, queue, numSM, s);
+    case 4: return launch_dp<4>(a, g, fp32, queue, numSM, s);
+    case 6: return launch_dp<6>(a, g, fp32, queue, numSM, s);
+    case 8: return launch_dp<8>(a, g, fp32, queue, numSM, s);
+    case 12: return launch_dp<12>(a, g, fp32, queue, numSM, s);
+    case 16: return launch_dp<16>(a, g, fp32, queue, numSM, s);
     }
     return cudaErrorInvalidValue;
 }

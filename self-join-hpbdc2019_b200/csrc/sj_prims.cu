@@ -290,34 +290,31 @@ __global__ void __launch_bounds__(256) k_hash_pairs_dev(const int32_t *__restric
 // Block per 256 keys: the keys' rows are consecutive in the batch (their
 // offsets came from one exclusive scan over ascending ids), so the block
 // writes the key of every position in its span, coalesced.
-__global__ void __launch_bounds__(256) k_expand_keys(uint32_t *__restrict__ count, const uint32_t *__restrict__ cursor,
-                                                     uint64_t n, int32_t *__restrict__ outKey,
+__global__ void __launch_bounds__(256) k_expand_keys(const uint32_t *__restrict__ excl,
+                                                     const uint32_t *__restrict__ total, uint64_t n,
+                                                     int32_t *__restrict__ outKey,
                                                      const unsigned long long *__restrict__ batchPairs, uint64_t cap)
 {
-    __shared__ uint32_t sStart[256];
-    __shared__ uint32_t sEnd[256];
-    const uint64_t k = (uint64_t)blockIdx.x * 256 + threadIdx.x;
-    uint32_t c = 0, e = 0;
-    if (k < n) {
-        c = count[k];
-        e = cursor[k];
-        count[k] = 0;
+    // keys k0..k0+255 own the slot ranges [excl[k], excl[k+1]) (excl[n] = *total);
+    // the block writes every slot of its keys, coalesced
+    __shared__ uint32_t sStart[257];
+    if (*batchPairs > cap) return;
+    const uint64_t k0 = (uint64_t)blockIdx.x * 256;
+    const int nk = (n - k0) < 256 ? (int)(n - k0) : 256;
+    for (int i = threadIdx.x; i <= nk; i += 256) {
+        const uint64_t k = k0 + i;
+        sStart[i] = k < n ? excl[k] : *total;
     }
-    const bool write = *batchPairs <= cap;
-    sStart[threadIdx.x] = e - c;
-    sEnd[threadIdx.x] = e;
     __syncthreads();
-    if (!write) return;
-    const uint64_t left = n - (uint64_t)blockIdx.x * 256;
-    const int nk = left < 256 ? (int)left : 256;
-    const uint32_t lo = sStart[0], hi = sEnd[nk - 1];
+    const uint32_t lo = sStart[0], hi = sStart[nk];
+    int a = 0;   // positions only grow, so each thread's key index only grows
     for (uint32_t pos = lo + threadIdx.x; pos < hi; pos += 256) {
-        int a = 0, b = nk - 1;        // last key whose row starts at or before pos
+        int b = nk - 1;   // last key whose range starts at or before pos
         while (a < b) {
-            int mid = (a + b + 1) >> 1;
+            const int mid = (a + b + 1) >> 1;
             if (sStart[mid] <= pos) a = mid; else b = mid - 1;
         }
-        outKey[pos] = (int32_t)((uint64_t)blockIdx.x * 256 + a);
+        outKey[pos] = (int32_t)(k0 + a);
     }
 }
 
@@ -334,11 +331,11 @@ cudaError_t sj_hash_pairs_dev(const int32_t *key, const int32_t *val, const unsi
     return cudaGetLastError();
 }
 
-cudaError_t sj_expand_keys(uint32_t *count, const uint32_t *cursor, uint64_t n, int32_t *outKey,
+cudaError_t sj_expand_keys(const uint32_t *excl, const uint32_t *total, uint64_t n, int32_t *outKey,
                            const unsigned long long *batchPairs, uint64_t cap, cudaStream_t s)
 {
     if (n == 0) return cudaSuccess;
-    k_expand_keys<<<(unsigned)ceil_div(n, 256), 256, 0, s>>>(count, cursor, n, outKey, batchPairs, cap);
+    k_expand_keys<<<(unsigned)ceil_div(n, 256), 256, 0, s>>>(excl, total, n, outKey, batchPairs, cap);
     sj_note_launch();
     return cudaGetLastError();
 }
