@@ -197,9 +197,9 @@ struct Ctx {
     DevBuf<uint32_t> dTaskEvals, dTaskRefined;   // per task, written by the count pass
     // count-pass records for the emission pass: per task, [block][query] hit
     // masks and per-query row counts (offsets: prefix sums over all tasks)
-    std::vector<uint64_t> hMaskOff, hRowOff;
-    DevBuf<uint64_t> dMaskOff, dRowOff;
-    DevBuf<uint32_t> masks, rowCnt;
+    std::vector<uint64_t> hMaskOff, hColOff, hRowOff;
+    DevBuf<uint64_t> dMaskOff, dColOff, dRowOff;
+    DevBuf<uint32_t> masks, colMasks, rowCnt;
     DevBuf<unsigned long long> batchTot;
     std::vector<cudaEvent_t> events;   // per-batch stage boundaries of the asynchronous phase
     PinBuf pinTotal, pinKey[2], pinVal[2];
@@ -686,28 +686,34 @@ sj_status run_count(Ctx &c, sj_join_args &a, bool queue)
     return SJ_OK;
 }
 
-// Per-task record offsets of the count pass: ceil(stream length / 32) mask
-// words per query, and one row count per query.
+// Per-task record offsets of the count pass: per block of 32 stream
+// positions one row-mask word per query and (symmetric tasks) one column-mask
+// word per candidate and group of 32 queries; one row count per query.
 sj_status task_offsets(Ctx &c)
 {
     const size_t nt = c.tasks.size();
     c.hMaskOff.assign(nt + 1, 0);
+    c.hColOff.assign(nt + 1, 0);
     c.hRowOff.assign(nt + 1, 0);
     for (size_t i = 0; i < nt; i++) {
         const sj_task &t = c.tasks[i];
         const uint64_t blocks = ((uint64_t)(t.sEnd - t.sBegin) + 31) / 32;
+        const uint64_t groups = ((uint64_t)t.qCount + 31) / 32;
         c.hMaskOff[i + 1] = c.hMaskOff[i] + blocks * t.qCount;
+        c.hColOff[i + 1] = c.hColOff[i] + ((t.flags & SJ_TASK_SYM) ? blocks * groups * 32 : 0);
         c.hRowOff[i + 1] = c.hRowOff[i] + t.qCount;
     }
     CK(c.dMaskOff.ensure(nt + 1));
+    CK(c.dColOff.ensure(nt + 1));
     CK(c.dRowOff.ensure(nt + 1));
     CK(cudaMemcpyAsync(c.dMaskOff.p, c.hMaskOff.data(), sizeof(uint64_t) * (nt + 1), cudaMemcpyHostToDevice, c.s));
+    CK(cudaMemcpyAsync(c.dColOff.p, c.hColOff.data(), sizeof(uint64_t) * (nt + 1), cudaMemcpyHostToDevice, c.s));
     CK(cudaMemcpyAsync(c.dRowOff.p, c.hRowOff.data(), sizeof(uint64_t) * (nt + 1), cudaMemcpyHostToDevice, c.s));
     return SJ_OK;
 }
 
-// Hit-mask words one batch may record (4 bytes each); a batch is also cut
-// when its masks would exceed this.
+// Hit-mask words (row or column) one batch may record (4 bytes each); a batch
+// is also cut when its masks would exceed this.
 constexpr uint64_t SJ_MASK_BATCH_WORDS = 1ULL << 29;
 
 sj_status prepare_join(Ctx &c, int &pattern, bool &queue)
@@ -782,14 +788,15 @@ sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
 
     // greedy batch plan on predicted pairs (and on hit-mask words)
     std::vector<BatchRange> plan;
-    uint64_t maxMaskWords = 1, maxRowWords = 1;
+    uint64_t maxMaskWords = 1, maxColWords = 1, maxRowWords = 1;
     {
         const double alpha = c.p.alpha;
         uint32_t t0 = 0;
         double acc = 0;
         for (uint32_t t = 0; t < nt; t++) {
             double v = c.taskPred[t] * (1.0 + alpha);
-            if (t > t0 && (acc + v > (double)cap || c.hMaskOff[t + 1] - c.hMaskOff[t0] > SJ_MASK_BATCH_WORDS)) {
+            if (t > t0 && (acc + v > (double)cap || c.hMaskOff[t + 1] - c.hMaskOff[t0] > SJ_MASK_BATCH_WORDS ||
+                           c.hColOff[t + 1] - c.hColOff[t0] > SJ_MASK_BATCH_WORDS)) {
                 plan.push_back({t0, t});
                 t0 = t;
                 acc = 0;
@@ -799,11 +806,13 @@ sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
         if (nt > t0) plan.push_back({t0, nt});
         for (const BatchRange &br : plan) {
             maxMaskWords = std::max<uint64_t>(maxMaskWords, c.hMaskOff[br.t1] - c.hMaskOff[br.t0]);
+            maxColWords = std::max<uint64_t>(maxColWords, c.hColOff[br.t1] - c.hColOff[br.t0]);
             maxRowWords = std::max<uint64_t>(maxRowWords, c.hRowOff[br.t1] - c.hRowOff[br.t0]);
         }
     }
     std::reverse(plan.begin(), plan.end());   // used as a stack
     CK(c.masks.ensure(maxMaskWords));
+    CK(c.colMasks.ensure(maxColWords));
     CK(c.rowCnt.ensure(maxRowWords));
 
     sj_join_args a;
@@ -821,6 +830,8 @@ sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
     a.taskRefined = c.dTaskRefined.p;
     a.masks = c.masks.p;
     a.maskOff = c.dMaskOff.p;
+    a.colMasks = c.colMasks.p;
+    a.colOff = c.dColOff.p;
     a.rowCnt = c.rowCnt.p;
     a.rowOff = c.dRowOff.p;
     {

@@ -1,38 +1,39 @@
 // The emission pass: pairs from the count pass's hit masks.
 //
-// The count pass (sj_join.cu) leaves, per task, a hit mask for every query and
-// block of 32 stream positions ([block][query] words, bit i = candidate
-// 32*block+i) and every query's row count; the exclusive scan of the per-key
-// counts gives each key's slot range in the batch buffer.  This pass writes
-// the values (the keys come from sj_expand_keys):
+// The count pass (sj_join.cu) leaves, per task, every query's hit mask per
+// block of 32 stream positions (row masks), the transposed masks of symmetric
+// tasks (column masks: per block and group of 32 queries, candidate j's query
+// bits) and every query's row count; the exclusive scan of the per-key counts
+// gives each key's slot range in the batch buffer.  This pass writes the
+// values (the keys come from sj_expand_keys):
 //
-//   rows    : key = query, values = candidates.  One warp per query: its words
-//             of a chunk of 2048 stream positions spread over the lanes, a warp
-//             scan of their popcounts, set bits expanded into a per-warp shared
-//             buffer, copied out as one contiguous run.  One reservation
+//   rows    : key = query, values = candidates.  One warp per query and chunk
+//             of 64 blocks (2048 stream positions): the query's 64 words (two
+//             per lane, contiguous), a warp scan of their popcounts, the set
+//             bits decoded into chunk positions in shared memory, then the
+//             candidate ids copied out as one contiguous run.  One reservation
 //             (atomicAdd on the key's cursor) per query and task.
-//   columns : key = candidate, values = queries (symmetric tasks only, with the
-//             query itself dropped on the home diagonal).  One warp per block:
-//             the block's words of a group of 32 queries are transposed so that
-//             lane j holds candidate j's query bits; groups are taken four at a
-//             time, one reservation per candidate and group batch.
+//   columns : key = candidate, values = queries (symmetric tasks).  One warp
+//             per block: lane j reads candidate j's words of eight query
+//             groups, one reservation per candidate and group batch, decode,
+//             copy-out through shared memory.
 //
-// Runs wider than the shared buffer are written directly by the whole warp,
-// one ballot per 32 candidates.  No distance is evaluated here, so the pass is
-// identical for both precisions.
+// Decoding (a per-lane loop over set bits, whose trip count is the busiest
+// lane's) only writes small indices; the loads and global stores run in the
+// balanced copy-out.  Runs wider than the shared buffer are written directly
+// by the whole warp.  No distance is evaluated here, so the pass is identical
+// for both precisions.
 #include "sj_internal.h"
-#include "sj_device.cuh"
 
 #include <atomic>
 
 namespace {
-using namespace sjdev;
 
 constexpr int EW = 128;                    // threads per emission CTA
 constexpr int ENW = EW / 32;
-constexpr int CHUNK = 2048;                // stream positions whose candidate ids are held at once
-constexpr int EM_CAP = 512;                // staged entries per warp
-constexpr int GB = 4;                      // query groups (of 32) per column batch
+constexpr int CHUNK = 2048;                // stream positions (64 blocks) whose candidate ids are held at once
+constexpr int EM_CAP = 1024;               // staged entries per warp
+constexpr int GB = 8;                      // query groups (of 32) per column batch
 constexpr int MAXQ = SJ_CTA * 4;           // largest query tile (sj_query_slots <= 4)
 constexpr uint32_t NO_SLOT = 0xffffffffu;  // reservation refused (past capacity)
 
@@ -42,11 +43,22 @@ struct EmitSmem {
     uint32_t candS[CHUNK];
     uint32_t qIdS[MAXQ];
     uint32_t rowPos[MAXQ];
-    uint32_t stV[ENW][EM_CAP];
-    uint32_t stP[ENW][EM_CAP];
+    uint32_t colRun[ENW][2][32]; // column batch: per lane, run start and first staged entry
+    uint16_t stQ[ENW][EM_CAP];   // row entries: chunk position; column entries: lane << 9 | query index
     uint32_t scanTmp[ENW];
     uint32_t curTask;
 };
+
+// Appends base + (index of each set bit of m) to buf[k...]; returns the new k.
+__device__ __forceinline__ uint32_t decode_bits(uint32_t m, uint32_t base, uint16_t *buf, uint32_t k)
+{
+    while (m) {
+        const uint32_t b = 31u - __clz(m);
+        m ^= 1u << b;
+        buf[k++] = (uint16_t)(base + b);
+    }
+    return k;
+}
 
 __device__ __forceinline__ uint32_t warp_excl_scan(uint32_t n, uint32_t lane, uint32_t &total)
 {
@@ -131,9 +143,10 @@ __global__ void __launch_bounds__(EW) k_emit(sj_join_args a, int queue)
         }
         for (uint32_t qi = tid; qi < qc; qi += EW) sm.qIdS[qi] = a.ids[task.qBegin + qi];
         __syncthreads();
-        const uint32_t homeEnd = (task.segBase == 0 && (task.flags & SJ_TASK_HOME)) ? sm.segPre[1] : 0u;
         const uint32_t L = min(task.sEnd, sm.segPre[nSeg]) - task.sBegin;
+        const uint32_t nBlk = (L + 31) / 32;
         const uint32_t *const masks = a.masks + (a.maskOff[t] - a.maskOff[a.taskBegin]);
+        const uint32_t *const colMasks = a.colMasks + (a.colOff[t] - a.colOff[a.taskBegin]);
         const uint32_t *const rows = a.rowCnt + (a.rowOff[t] - a.rowOff[a.taskBegin]);
 
         // ---- one row reservation per query and task
@@ -151,8 +164,7 @@ __global__ void __launch_bounds__(EW) k_emit(sj_join_args a, int queue)
         }
 
         const uint32_t nG = (qc + 31) / 32;
-        uint32_t *const stV = sm.stV[warp];
-        uint32_t *const stP = sm.stP[warp];
+        uint16_t *const stQ = sm.stQ[warp];
         for (uint32_t c0 = 0; c0 < L; c0 += CHUNK) {
             const uint32_t nC = min((uint32_t)CHUNK, L - c0);
             __syncthreads();
@@ -167,12 +179,14 @@ __global__ void __launch_bounds__(EW) k_emit(sj_join_args a, int queue)
             }
             __syncthreads();
             const uint32_t nb = (nC + 31) / 32;
-            const uint64_t b0 = c0 / 32;
+            const uint32_t b0 = c0 / 32;   // first block of the chunk (a multiple of 64)
 
-            // ---- rows: one query per warp
+            // ---- rows: one query per warp, its words of the chunk contiguous
+            const uint64_t chunkBase = sj_row_mask_index(b0, 0, qc, nBlk);
             for (uint32_t qi = warp; qi < qc; qi += ENW) {
-                const uint32_t w0 = lane < nb ? masks[(b0 + lane) * qc + qi] : 0u;
-                const uint32_t w1 = lane + 32 < nb ? masks[(b0 + lane + 32) * qc + qi] : 0u;
+                const uint32_t *wq = masks + chunkBase + (uint64_t)qi * nb;
+                const uint32_t w0 = lane < nb ? wq[lane] : 0u;
+                const uint32_t w1 = lane + 32 < nb ? wq[lane + 32] : 0u;
                 uint32_t T;
                 const uint32_t ex = warp_excl_scan(__popc(w0) + __popc(w1), lane, T);
                 if (T == 0) continue;
@@ -181,21 +195,10 @@ __global__ void __launch_bounds__(EW) k_emit(sj_join_args a, int queue)
                 if (lane == 0) sm.rowPos[qi] = (pos0 == NO_SLOT) ? NO_SLOT : pos0 + T;
                 if (pos0 == NO_SLOT) continue;
                 if (T <= (uint32_t)EM_CAP) {
-                    uint32_t k = ex;
-                    uint32_t m = w0;
-                    while (m) {
-                        const int b = __ffs(m) - 1;
-                        m &= m - 1;
-                        stV[k++] = sm.candS[lane * 32 + b];
-                    }
-                    m = w1;
-                    while (m) {
-                        const int b = __ffs(m) - 1;
-                        m &= m - 1;
-                        stV[k++] = sm.candS[(lane + 32) * 32 + b];
-                    }
+                    uint32_t k = decode_bits(w0, lane * 32, stQ, ex);
+                    decode_bits(w1, (lane + 32) * 32, stQ, k);
                     __syncwarp();
-                    for (uint32_t e = lane; e < T; e += 32) a.outVal[pos0 + e] = (int32_t)stV[e];
+                    for (uint32_t e = lane; e < T; e += 32) a.outVal[pos0 + e] = (int32_t)sm.candS[stQ[e]];
                     __syncwarp();
                 } else {
                     uint32_t off = 0;
@@ -210,25 +213,18 @@ __global__ void __launch_bounds__(EW) k_emit(sj_join_args a, int queue)
             }
             if (!sym) continue;
 
-            // ---- columns: one block of 32 candidates per warp
+            // ---- columns: one block of 32 candidates per warp, lane j = candidate j
             for (uint32_t bb = warp; bb < nb; bb += ENW) {
-                const uint32_t blk = task.sBegin + c0 + bb * 32;   // absolute stream position
-                const uint32_t hb = home_bits(blk, homeEnd, true);
                 const uint32_t key = sm.candS[bb * 32 + lane];
-                const uint32_t *const wrow = masks + (b0 + bb) * qc;
+                const uint32_t *const wb = colMasks + (uint64_t)(b0 + bb) * nG * 32 + lane;
                 for (uint32_t g0 = 0; g0 < nG; g0 += GB) {
-                    uint32_t rw[GB], cw[GB];
+                    const uint32_t gn = min((uint32_t)GB, nG - g0);
+                    uint32_t cw[GB];
                     uint32_t n = 0;
 #pragma unroll
                     for (int gg = 0; gg < GB; gg++) {
-                        rw[gg] = cw[gg] = 0;
-                        if (g0 + gg < nG) {   // warp-uniform
-                            const uint32_t qi = (g0 + gg) * 32 + lane;
-                            const uint32_t w = qi < qc ? (wrow[qi] & mir_keep(qi, blk, hb)) : 0u;
-                            rw[gg] = w;
-                            cw[gg] = transpose32(w, lane);
-                            n += __popc(cw[gg]);
-                        }
+                        cw[gg] = (uint32_t)gg < gn ? wb[(g0 + gg) * 32] : 0u;
+                        n += __popc(cw[gg]);
                     }
                     uint32_t base = 0;
                     bool bad = false;
@@ -246,18 +242,17 @@ __global__ void __launch_bounds__(EW) k_emit(sj_join_args a, int queue)
                     if (T <= (uint32_t)EM_CAP) {
                         uint32_t k = ex;
 #pragma unroll
-                        for (int gg = 0; gg < GB; gg++) {
-                            uint32_t m = cw[gg];
-                            while (m) {
-                                const int b = __ffs(m) - 1;
-                                m &= m - 1;
-                                stV[k] = sm.qIdS[(g0 + gg) * 32 + b];
-                                stP[k] = base + (k - ex);
-                                k++;
-                            }
-                        }
+                        for (int gg = 0; gg < GB; gg++) k = decode_bits(cw[gg], (lane << 9) | ((g0 + gg) * 32), stQ, k);
+                        // staged entries [ex, ex + n) of lane L go to its run [base, base + n)
+                        sm.colRun[warp][0][lane] = base;
+                        sm.colRun[warp][1][lane] = ex;
                         __syncwarp();
-                        for (uint32_t e = lane; e < T; e += 32) a.outVal[stP[e]] = (int32_t)stV[e];
+                        for (uint32_t e = lane; e < T; e += 32) {
+                            const uint32_t ent = stQ[e];
+                            const uint32_t owner = ent >> 9;
+                            a.outVal[sm.colRun[warp][0][owner] + (e - sm.colRun[warp][1][owner])] =
+                                (int32_t)sm.qIdS[ent & 511u];
+                        }
                         __syncwarp();
                     } else {
                         uint32_t off = 0;
@@ -267,8 +262,9 @@ __global__ void __launch_bounds__(EW) k_emit(sj_join_args a, int queue)
                             while (live) {
                                 const int Lk = __ffs(live) - 1;
                                 live &= live - 1;
+                                const uint32_t word = __shfl_sync(0xffffffffu, cw[gg], Lk);
                                 const uint32_t pL = __shfl_sync(0xffffffffu, base + off, Lk);
-                                const bool h = (rw[gg] >> Lk) & 1u;
+                                const bool h = (word >> lane) & 1u;
                                 const uint32_t bal = __ballot_sync(0xffffffffu, h);
                                 if (h) a.outVal[pL + __popc(bal & ltmask)] = (int32_t)sm.qIdS[(g0 + gg) * 32 + lane];
                             }

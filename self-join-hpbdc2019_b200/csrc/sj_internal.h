@@ -79,8 +79,12 @@ struct sj_join_args {
     uint32_t *taskHits;         // optional per-task measured pairs (count pass)
     // count-pass records consumed by the emission pass (null: not recorded).
     // Offsets are absolute over all tasks; a batch indexes from its first task's.
-    uint32_t *masks;            // per task: [block][query] hit masks (bit i = candidate 32*block+i)
-    const uint64_t *maskOff;    // per task: first mask word
+    uint32_t *masks;            // per task: row hit masks, bit i = candidate 32*block+i, laid out
+                                // [chunk of 64 blocks][query][block in chunk] (sj_row_mask_index)
+    const uint64_t *maskOff;    // per task: first row-mask word
+    uint32_t *colMasks;         // per symmetric task: column hit masks [block][query group][candidate],
+                                // bit i = query 32*group+i (the query itself dropped on the home diagonal)
+    const uint64_t *colOff;     // per task: first column-mask word
     uint32_t *rowCnt;           // per task and query: pairs keyed by the query
     const uint64_t *rowOff;     // per task: first row count
     uint32_t *taskEvals;        // per task: candidate evaluations
@@ -88,6 +92,16 @@ struct sj_join_args {
     double margin;              // FP32 filter: bound M on |FP32 estimate - (FP64 d2 - T)|
     float delta;                // FP32 filter: width of the borderline band (>= 2M plus threshold rounding)
 };
+
+// Row-mask word of query qi and block b of a task with qc queries and nBlk
+// blocks: chunks of 64 blocks, each [query][block in chunk], so one query's
+// words of a chunk are contiguous.
+__host__ __device__ inline uint64_t sj_row_mask_index(uint32_t b, uint32_t qi, uint32_t qc, uint32_t nBlk)
+{
+    const uint32_t c = b >> 6;
+    const uint32_t cb = (nBlk - 64 * c) < 64 ? (nBlk - 64 * c) : 64;
+    return (uint64_t)64 * c * qc + (uint64_t)qi * cb + (b & 63);
+}
 
 // Kernel launches made by this library since load (every launcher calls
 // sj_note_launch() after each <<<...>>>; bench and tests read the total).

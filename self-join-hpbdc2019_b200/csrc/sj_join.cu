@@ -338,6 +338,7 @@ __global__ void __launch_bounds__(SJ_CTA) k_join(sj_join_args a, sj_grid_dev g, 
         const float2 nd = make_float2(-a.delta, -a.delta);
         const long long T1 = __double_as_longlong(T) + 1;
         uint32_t *const maskBase = a.masks ? a.masks + (a.maskOff[t] - a.maskOff[a.taskBegin]) : nullptr;
+        uint32_t *const colBase = (a.colMasks && sym) ? a.colMasks + (a.colOff[t] - a.colOff[a.taskBegin]) : nullptr;
 
         uint32_t rowCount[R];   // pairs keyed by each query
         uint32_t evals = 0;     // candidate evaluations
@@ -347,6 +348,8 @@ __global__ void __launch_bounds__(SJ_CTA) k_join(sj_join_args a, sj_grid_dev g, 
 
         // the stream can never extend past the segments actually present
         const uint32_t sEnd = min(task.sEnd, segPre[nSeg]);
+        const uint32_t nBlk = (sEnd - task.sBegin + 31) / 32;
+        const uint32_t nG = (task.qCount + 31) / 32;
         for (uint32_t sBase = task.sBegin; sBase < sEnd; sBase += S) {
             const uint32_t nIn = min((uint32_t)S, sEnd - sBase);
             __syncthreads();
@@ -398,7 +401,7 @@ __global__ void __launch_bounds__(SJ_CTA) k_join(sj_join_args a, sj_grid_dev g, 
                 }
                 const uint32_t blk = sBase + jb;
                 const uint32_t hb = home_bits(blk, homeEnd, sym);
-                const uint64_t blockIdxInTask = (blk - task.sBegin) >> 5;
+                const uint32_t bInTask = (blk - task.sBegin) >> 5;
 #pragma unroll
                 for (int r = 0; r < R; r++) {
                     if ((uint32_t)r >= nAct) continue;   // warp-uniform
@@ -424,9 +427,13 @@ __global__ void __launch_bounds__(SJ_CTA) k_join(sj_join_args a, sj_grid_dev g, 
                     }
                     evals += __popc(rowValid);
                     const uint32_t rowMask = h & rowValid;   // lane = query, bit = candidate
-                    if (maskBase && qValid) maskBase[blockIdxInTask * task.qCount + qi] = rowMask;
+                    if (maskBase && qValid) maskBase[sj_row_mask_index(bInTask, qi, task.qCount, nBlk)] = rowMask;
                     rowCount[r] += __popc(rowMask);
-                    if (sym) colCnt[warp][jb + lane] += __popc(transpose32(rowMask & mir_keep(qi, blk, hb), lane));
+                    if (sym) {
+                        const uint32_t colW = transpose32(rowMask & mir_keep(qi, blk, hb), lane);
+                        colCnt[warp][jb + lane] += __popc(colW);
+                        if (colBase) colBase[((uint64_t)bInTask * nG + (uint32_t)r * NW + warp) * 32 + lane] = colW;
+                    }
                 }
             }
             if (sym) {

@@ -287,34 +287,30 @@ __global__ void __launch_bounds__(256) k_hash_pairs_dev(const int32_t *__restric
     }
 }
 
-// Block per 256 keys: the keys' rows are consecutive in the batch (their
-// offsets came from one exclusive scan over ascending ids), so the block
-// writes the key of every position in its span, coalesced.
+// Keys of a batch: key k owns slots [excl[k], excl[k+1]) (excl[n] = *total).
+// A warp takes 32 consecutive keys and writes each key's run with all lanes,
+// 128 contiguous bytes per store.
 __global__ void __launch_bounds__(256) k_expand_keys(const uint32_t *__restrict__ excl,
                                                      const uint32_t *__restrict__ total, uint64_t n,
                                                      int32_t *__restrict__ outKey,
                                                      const unsigned long long *__restrict__ batchPairs, uint64_t cap)
 {
-    // keys k0..k0+255 own the slot ranges [excl[k], excl[k+1]) (excl[n] = *total);
-    // the block writes every slot of its keys, coalesced
-    __shared__ uint32_t sStart[257];
     if (*batchPairs > cap) return;
-    const uint64_t k0 = (uint64_t)blockIdx.x * 256;
-    const int nk = (n - k0) < 256 ? (int)(n - k0) : 256;
-    for (int i = threadIdx.x; i <= nk; i += 256) {
-        const uint64_t k = k0 + i;
-        sStart[i] = k < n ? excl[k] : *total;
-    }
-    __syncthreads();
-    const uint32_t lo = sStart[0], hi = sStart[nk];
-    int a = 0;   // positions only grow, so each thread's key index only grows
-    for (uint32_t pos = lo + threadIdx.x; pos < hi; pos += 256) {
-        int b = nk - 1;   // last key whose range starts at or before pos
-        while (a < b) {
-            const int mid = (a + b + 1) >> 1;
-            if (sStart[mid] <= pos) a = mid; else b = mid - 1;
-        }
-        outKey[pos] = (int32_t)(k0 + a);
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint64_t k0 = ((uint64_t)blockIdx.x * 256 + (threadIdx.x & ~31u));
+    if (k0 >= n) return;
+    const uint64_t k = k0 + lane;
+    const uint32_t tot = *total;
+    const uint32_t st = k < n ? excl[k] : tot;
+    const uint32_t en = k + 1 < n ? excl[k + 1] : tot;
+    uint32_t live = __ballot_sync(0xffffffffu, en > st);
+    while (live) {
+        const int i = __ffs(live) - 1;
+        live &= live - 1;
+        const uint32_t s0 = __shfl_sync(0xffffffffu, st, i);
+        const uint32_t e0 = __shfl_sync(0xffffffffu, en, i);
+        const int32_t key = (int32_t)(k0 + i);
+        for (uint32_t pos = s0 + lane; pos < e0; pos += 32) outKey[pos] = key;
     }
 }
 
