@@ -5,8 +5,9 @@ Workload (default c2): 2-D, n = 2,000,000 points with i.i.d. exponential(40)
 coordinates clipped to [0, 1] (seeded synthetic), eps = 0.0015, B-Unicomp
 traversal with workload-sorted tasks on a persistent work queue, FP64, result
 batches of at most 5e7 pairs.  One step = grid-index build + estimate + batched
-join (count, scan, fill per batch) + an on-device fold of every batch into the
-pair count and set hash, with the points already resident in HBM.
+join (per batch: count pass recording hit masks, scan of the per-key counts,
+key expansion, pair emission from the masks) + an on-device fold of every batch
+into the pair count and set hash, with the points already resident in HBM.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                   [--workload c1..c5] [--n N]
@@ -38,9 +39,12 @@ sys.path.insert(0, os.path.join(REPO, "self-join-hpbdc2019_b200"))
 
 import numpy as np  # noqa: E402
 
-# dram__bytes_read.sum + dram__bytes_write.sum per output pair of the fill
-# kernel, from the ncu capture summarised in profiles/ (None until captured)
-FILL_TRAFFIC_BYTES_PER_PAIR = None
+# dram__bytes_read.sum + dram__bytes_write.sum per output pair of the emission
+# kernel (k_emit), from the ncu capture summarised in profiles/ (None: not captured)
+EMIT_TRAFFIC_BYTES_PER_PAIR = None
+
+# CUDA-core lanes per SM (B200): FP64 FMA and FP32 FMA per clock
+FP64_LANES, FP32_LANES, NUM_SM = 64, 128, 148
 
 L2_BYTES = 126 * 1024 * 1024
 
@@ -180,6 +184,7 @@ def run_ours(args):
     prec = spec["precision"] if args.precision is None else args.precision
     flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device="cuda")
     sj = sjoin.SelfJoin(spec["D"], eps, indexed_dims=k, mode=spec["mode"], precision=prec,
+                        scheduler=sjoin.SCHED_LEARNED if args.learned else sjoin.SCHED_SAMPLING,
                         capacity=spec["capacity"], device=local)
     if args.learned:
         sj.load_estimator(args.learned)
@@ -263,15 +268,22 @@ def run_ours(args):
     nb = max(1, s["num_batches"])
     # per-stage device time (CUDA events around every launch) and algorithmic bytes
     stages = {
-        "fill": (s["ms_fill_kernel"], 4 * pairs, "k_join fill pass: pair values to their row slots"),
-        "expand": (s["ms_expand"], 4 * pairs + 12 * spec["n"] * nb, "k_expand_keys: key array from row offsets"),
+        "emit": (s["ms_fill_kernel"], 4 * pairs, "k_emit: pair values from the hit masks into their row slots"),
+        "expand": (s["ms_expand"], 4 * pairs + 4 * spec["n"] * nb, "k_expand_keys: key array from row offsets"),
         "hash": (s["ms_deliver"], 8 * pairs, "k_hash_pairs_dev: consumer fold of every batch"),
-        "count": (s["ms_count"], 0, "k_join count pass"),
+        "count": (s["ms_count"], None, "k_join count pass (distance loop)"),
     }
-    top = max(("fill", "expand", "hash"), key=lambda k2: stages[k2][0])
+    top = max(("emit", "expand", "hash"), key=lambda k2: stages[k2][0])
     t_ms, algo_bytes, kdesc = stages[top]
     achieved = algo_bytes / (t_ms / 1e3) / 1e9 if t_ms > 0 else None
-    traffic = (FILL_TRAFFIC_BYTES_PER_PAIR * pairs / nb) if (FILL_TRAFFIC_BYTES_PER_PAIR and top == "fill") else None
+    traffic = (EMIT_TRAFFIC_BYTES_PER_PAIR * pairs / nb) if (EMIT_TRAFFIC_BYTES_PER_PAIR and top == "emit") else None
+    # distance loop against the CUDA-core pipe it runs on: 3*D flops (subtract,
+    # multiply, add per dimension) per evaluated candidate, nominal lanes x the
+    # SM clock sampled during the timed steps
+    mhz = clocks.get("sm_mhz") or 1965.0
+    lanes = FP64_LANES if prec == 0 else FP32_LANES
+    pipe_tflops = NUM_SM * lanes * 2 * mhz * 1e6 / 1e12
+    dist_tflops = (3 * spec["D"] * s["distance_calcs"]) / (s["ms_count"] / 1e3) / 1e12 if s["ms_count"] > 0 else None
     cpu = None
     if not args.no_cpu:
         rate, cores, sample, _ = cpu_oracle_rate(pts, eps, k, target_s=args.cpu_seconds)
@@ -286,6 +298,11 @@ def run_ours(args):
                      "frac": (achieved / peak) if achieved else None, "peak_kind": peak_kind,
                      "algorithmic_bytes_per_launch": algo_bytes / nb, "launches": nb, "traffic": traffic,
                      "stage_ms": {k2: round(v[0], 3) for k2, v in stages.items()}},
+        "roofline_distance_loop": {"bound": "fp64 pipe" if prec == 0 else "fp32 pipe",
+                                   "kernel": stages["count"][2], "achieved": dist_tflops, "peak": pipe_tflops,
+                                   "unit": "TFLOP/s", "frac": (dist_tflops / pipe_tflops) if dist_tflops else None,
+                                   "peak_kind": "nominal lanes x sampled SM clock",
+                                   "flops_per_candidate": 3 * spec["D"]},
         "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clocks,
         "phases_ms": {k2: round(s[k2], 3) for k2 in ("ms_index", "ms_tasks", "ms_estimate", "ms_count", "ms_scan",
                                                      "ms_fill", "ms_expand", "ms_deliver", "ms_total")},
@@ -307,7 +324,8 @@ def main():
     ap.add_argument("--workload", default="c2")
     ap.add_argument("--n", type=int, default=None)
     ap.add_argument("--precision", type=int, default=None)
-    ap.add_argument("--learned", default=None)
+    ap.add_argument("--learned", default=None,
+                    help="estimator weights file: learned scheduler instead of the sampling estimate")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-cpu", action="store_true")

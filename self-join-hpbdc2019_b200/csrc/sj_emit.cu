@@ -34,7 +34,8 @@ constexpr int ENW = EW / 32;
 constexpr int CHUNK = 2048;                // stream positions (64 blocks) whose candidate ids are held at once
 constexpr int EM_CAP = 1024;               // staged entries per warp
 constexpr int GB = 8;                      // query groups (of 32) per column batch
-constexpr int MAXQ = SJ_CTA * 4;           // largest query tile (sj_query_slots <= 4)
+constexpr int MAXQ = SJ_CTA * 4;           // largest query tile
+static_assert(SJ_SLOTS_F32 <= 4 && SJ_SLOTS_F64 <= 4, "query tiles are at most 4 * SJ_CTA points");
 constexpr uint32_t NO_SLOT = 0xffffffffu;  // reservation refused (past capacity)
 
 struct EmitSmem {
@@ -182,11 +183,21 @@ __global__ void __launch_bounds__(EW) k_emit(sj_join_args a, int queue)
             const uint32_t b0 = c0 / 32;   // first block of the chunk (a multiple of 64)
 
             // ---- rows: one query per warp, its words of the chunk contiguous
+            // (the next query's words are loaded while this one is written)
             const uint64_t chunkBase = sj_row_mask_index(b0, 0, qc, nBlk);
+            uint32_t n0 = 0, n1 = 0;
+            if (warp < qc) {
+                const uint32_t *wq = masks + chunkBase + (uint64_t)warp * nb;
+                n0 = lane < nb ? wq[lane] : 0u;
+                n1 = lane + 32 < nb ? wq[lane + 32] : 0u;
+            }
             for (uint32_t qi = warp; qi < qc; qi += ENW) {
-                const uint32_t *wq = masks + chunkBase + (uint64_t)qi * nb;
-                const uint32_t w0 = lane < nb ? wq[lane] : 0u;
-                const uint32_t w1 = lane + 32 < nb ? wq[lane + 32] : 0u;
+                const uint32_t w0 = n0, w1 = n1;
+                if (qi + ENW < qc) {
+                    const uint32_t *wq = masks + chunkBase + (uint64_t)(qi + ENW) * nb;
+                    n0 = lane < nb ? wq[lane] : 0u;
+                    n1 = lane + 32 < nb ? wq[lane + 32] : 0u;
+                }
                 uint32_t T;
                 const uint32_t ex = warp_excl_scan(__popc(w0) + __popc(w1), lane, T);
                 if (T == 0) continue;
@@ -213,37 +224,47 @@ __global__ void __launch_bounds__(EW) k_emit(sj_join_args a, int queue)
             }
             if (!sym) continue;
 
-            // ---- columns: one block of 32 candidates per warp, lane j = candidate j
+            // ---- columns: one block of 32 candidates per warp, lane j = candidate j;
+            // one reservation per candidate and task over all query groups, the
+            // groups then written GB at a time
             for (uint32_t bb = warp; bb < nb; bb += ENW) {
                 const uint32_t key = sm.candS[bb * 32 + lane];
                 const uint32_t *const wb = colMasks + (uint64_t)(b0 + bb) * nG * 32 + lane;
+                uint32_t n = 0;
+                for (uint32_t g = 0; g < nG; g++) n += __popc(wb[g * 32]);
+                // the reservation's result is first needed by the copy-out below,
+                // so its latency overlaps the first batch's loads and decode
+                const uint32_t base0 = n ? atomicAdd(&a.keyCursor[key], n) : 0u;
+                uint32_t base = base0;
+                bool checked = false;
                 for (uint32_t g0 = 0; g0 < nG; g0 += GB) {
                     const uint32_t gn = min((uint32_t)GB, nG - g0);
                     uint32_t cw[GB];
-                    uint32_t n = 0;
+                    uint32_t m = 0;
 #pragma unroll
                     for (int gg = 0; gg < GB; gg++) {
                         cw[gg] = (uint32_t)gg < gn ? wb[(g0 + gg) * 32] : 0u;
-                        n += __popc(cw[gg]);
+                        m += __popc(cw[gg]);
                     }
-                    uint32_t base = 0;
-                    bool bad = false;
-                    if (n) {
-                        base = atomicAdd(&a.keyCursor[key], n);
-                        if ((uint64_t)base + n > a.capacity) {
-                            atomicMax(&a.stat[3], 1ULL);
-                            bad = true;
-                        }
-                    }
-                    if (__any_sync(0xffffffffu, bad)) continue;
                     uint32_t T;
-                    const uint32_t ex = warp_excl_scan(n, lane, T);
+                    const uint32_t ex = warp_excl_scan(m, lane, T);
                     if (T == 0) continue;
-                    if (T <= (uint32_t)EM_CAP) {
+                    const bool staged = T <= (uint32_t)EM_CAP;
+                    if (staged) {
                         uint32_t k = ex;
 #pragma unroll
                         for (int gg = 0; gg < GB; gg++) k = decode_bits(cw[gg], (lane << 9) | ((g0 + gg) * 32), stQ, k);
-                        // staged entries [ex, ex + n) of lane L go to its run [base, base + n)
+                    }
+                    if (!checked) {   // first use of the reservation
+                        checked = true;
+                        const bool bad = n && (uint64_t)base0 + n > a.capacity;
+                        if (__any_sync(0xffffffffu, bad)) {
+                            if (bad) atomicMax(&a.stat[3], 1ULL);
+                            break;
+                        }
+                    }
+                    if (staged) {
+                        // staged entries [ex, ex + m) of lane L go to its run from base
                         sm.colRun[warp][0][lane] = base;
                         sm.colRun[warp][1][lane] = ex;
                         __syncwarp();
@@ -271,6 +292,7 @@ __global__ void __launch_bounds__(EW) k_emit(sj_join_args a, int queue)
                             off += __popc(cw[gg]);
                         }
                     }
+                    base += m;
                 }
             }
         }

@@ -18,10 +18,15 @@
 // Query slots per join thread: a join task covers up to SJ_CTA * slots query
 // points of one cell (each thread evaluates every staged candidate against
 // `slots` queries held in registers).
+#ifndef SJ_SLOTS_F32
+#define SJ_SLOTS_F32 4       // query slots of the FP32 filter for Dp <= 8 (2 above)
+#endif
+#ifndef SJ_SLOTS_F64
+#define SJ_SLOTS_F64 4       // query slots of the FP64 predicate for Dp <= 8 (2 above)
+#endif
 constexpr int sj_query_slots(int Dp, bool fp32)
 {
-    (void)fp32;
-    return Dp <= 8 ? 4 : 2;
+    return Dp <= 8 ? (fp32 ? SJ_SLOTS_F32 : SJ_SLOTS_F64) : 2;
 }
 
 // Traversal (neighbour ownership) patterns, mapped from the reference's search modes.

@@ -30,8 +30,16 @@
 
 #include <atomic>
 
+#ifndef SJ_PUSH_SIGN
+#define SJ_PUSH_SIGN 1      // sign-bit packing: 1 inline funnel shift, 2 shift+or, 0 intrinsic
+#endif
+#ifndef SJ_EVAL_UNROLL
+#define SJ_EVAL_UNROLL 2    // unrolling of the per-block candidate loop
+#endif
+
 namespace {
 using namespace sjdev;
+constexpr int kEvalUnroll = SJ_EVAL_UNROLL;
 
 constexpr int NW = SJ_CTA / 32;
 
@@ -83,6 +91,21 @@ struct StageOf { using T = Stage64<DP>; };
 template <int DP>
 struct StageOf<DP, true> { using T = Stage32<DP>; };
 
+// mask << 1 | sign bit of v: one funnel shift (the value's bits are not
+// inspected as a float, so no comparison is generated)
+__device__ __forceinline__ uint32_t push_sign(uint32_t mask, float v)
+{
+#if SJ_PUSH_SIGN == 1
+    uint32_t r;
+    asm("shf.l.wrap.b32 %0, %1, %2, 1;" : "=r"(r) : "r"(__float_as_uint(v)), "r"(mask));
+    return r;
+#elif SJ_PUSH_SIGN == 2
+    return (mask << 1) | (__float_as_uint(v) >> 31);
+#else
+    return __funnelshift_l(__float_as_uint(v), mask, 1);
+#endif
+}
+
 // FP32 filter over one block of 32 staged candidates for slots 0..RR-1.
 //   y = (|b|^2 - tLo) + sum_l (-2 a_l) b_l      (packed f32x2: two candidates per op)
 //   z = y - delta
@@ -95,7 +118,7 @@ __device__ __forceinline__ void eval_block_f32(const Stage32<DP> &st, uint32_t p
                                                uint32_t (&near)[R])
 {
     constexpr int CW2 = Stage32<DP>::CW2;
-#pragma unroll 2
+#pragma unroll kEvalUnroll
     for (int p = 15; p >= 0; p--) {
         const float4 *row = reinterpret_cast<const float4 *>(&st.c[pb + p][0]);
         float2 y[RR];
@@ -127,10 +150,10 @@ __device__ __forceinline__ void eval_block_f32(const Stage32<DP> &st, uint32_t p
 #pragma unroll
         for (int r = 0; r < RR; r++) {
             const float2 z = __fadd2_rn(y[r], nd);
-            hit[r] = __funnelshift_l(__float_as_uint(y[r].y), hit[r], 1);
-            hit[r] = __funnelshift_l(__float_as_uint(y[r].x), hit[r], 1);
-            near[r] = __funnelshift_l(__float_as_uint(z.y), near[r], 1);
-            near[r] = __funnelshift_l(__float_as_uint(z.x), near[r], 1);
+            hit[r] = push_sign(hit[r], y[r].y);
+            hit[r] = push_sign(hit[r], y[r].x);
+            near[r] = push_sign(near[r], z.y);
+            near[r] = push_sign(near[r], z.x);
         }
     }
 }
@@ -142,7 +165,7 @@ template <int DP, int RR, int R>
 __device__ __forceinline__ void eval_block_f64(const Stage64<DP> &st, uint32_t jb, const double (&q)[R][DP],
                                                long long T1, uint32_t (&hit)[R])
 {
-#pragma unroll 2
+#pragma unroll kEvalUnroll
     for (int jj = 31; jj >= 0; jj--) {
         const double *cb = &st.c[jb + jj][0];
         double acc[RR];
@@ -176,7 +199,7 @@ __device__ __forceinline__ void eval_block_f64(const Stage64<DP> &st, uint32_t j
 #pragma unroll
         for (int r = 0; r < RR; r++) {
             const long long diff = __double_as_longlong(acc[r]) - T1;
-            hit[r] = __funnelshift_l((uint32_t)((unsigned long long)diff >> 32), hit[r], 1);
+            hit[r] = push_sign(hit[r], __int_as_float((int)((unsigned long long)diff >> 32)));
         }
     }
 }
@@ -204,8 +227,17 @@ struct __align__(16) JoinSmem {
 // set -- every query's hit mask per block of 32 stream positions plus its row
 // count, which the emission pass turns into pairs without a second distance
 // evaluation.
+// Resident CTAs per SM the register allocation must allow: the FP32 filter
+// gains from a fifth CTA, the FP64 predicate from keeping its registers.
+#ifndef SJ_JOIN_MIN_BLOCKS_F32
+#define SJ_JOIN_MIN_BLOCKS_F32 5
+#endif
+#ifndef SJ_JOIN_MIN_BLOCKS_F64
+#define SJ_JOIN_MIN_BLOCKS_F64 1
+#endif
+
 template <int DP, bool F32, int R>
-__global__ void __launch_bounds__(SJ_CTA) k_join(sj_join_args a, sj_grid_dev g, int queue)
+__global__ void __launch_bounds__(SJ_CTA, F32 ? SJ_JOIN_MIN_BLOCKS_F32 : SJ_JOIN_MIN_BLOCKS_F64) k_join(sj_join_args a, sj_grid_dev g, int queue)
 {
     using Smem = JoinSmem<DP, F32, R>;
     constexpr int S = Smem::S;
@@ -402,12 +434,17 @@ __global__ void __launch_bounds__(SJ_CTA) k_join(sj_join_args a, sj_grid_dev g, 
                 const uint32_t blk = sBase + jb;
                 const uint32_t hb = home_bits(blk, homeEnd, sym);
                 const uint32_t bInTask = (blk - task.sBegin) >> 5;
+                // record addresses of this block: row masks [chunk][query][block in
+                // chunk], column masks [block][query group][candidate]
+                uint32_t *const rowRec = maskBase ? maskBase + sj_row_mask_index(bInTask, 0, task.qCount, nBlk) : nullptr;
+                const uint32_t rowStride = min(64u, nBlk - (bInTask & ~63u));
+                uint32_t *const colRec = colBase ? colBase + ((uint64_t)bInTask * nG + warp) * 32 + lane : nullptr;
 #pragma unroll
                 for (int r = 0; r < R; r++) {
                     if ((uint32_t)r >= nAct) continue;   // warp-uniform
                     const uint32_t qi = (uint32_t)r * SJ_CTA + tid;
                     const bool qValid = qi < task.qCount;
-                    const uint32_t rowValid = qValid ? (inRange & row_keep(qi, blk, hb)) : 0u;
+                    const uint32_t rowValid = qValid ? (hb ? (inRange & row_keep(qi, blk, hb)) : inRange) : 0u;
                     uint32_t h = hits[r];
                     if (F32) {
                         uint32_t bm = near[r] & ~h & rowValid;
@@ -427,12 +464,12 @@ __global__ void __launch_bounds__(SJ_CTA) k_join(sj_join_args a, sj_grid_dev g, 
                     }
                     evals += __popc(rowValid);
                     const uint32_t rowMask = h & rowValid;   // lane = query, bit = candidate
-                    if (maskBase && qValid) maskBase[sj_row_mask_index(bInTask, qi, task.qCount, nBlk)] = rowMask;
+                    if (rowRec && qValid) rowRec[(uint64_t)qi * rowStride] = rowMask;
                     rowCount[r] += __popc(rowMask);
                     if (sym) {
-                        const uint32_t colW = transpose32(rowMask & mir_keep(qi, blk, hb), lane);
+                        const uint32_t colW = transpose32(hb ? (rowMask & mir_keep(qi, blk, hb)) : rowMask, lane);
                         colCnt[warp][jb + lane] += __popc(colW);
-                        if (colBase) colBase[((uint64_t)bInTask * nG + (uint32_t)r * NW + warp) * 32 + lane] = colW;
+                        if (colRec) colRec[(uint32_t)r * NW * 32] = colW;
                     }
                 }
             }

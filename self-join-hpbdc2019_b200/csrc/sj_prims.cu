@@ -310,7 +310,13 @@ __global__ void __launch_bounds__(256) k_expand_keys(const uint32_t *__restrict_
         const uint32_t s0 = __shfl_sync(0xffffffffu, st, i);
         const uint32_t e0 = __shfl_sync(0xffffffffu, en, i);
         const int32_t key = (int32_t)(k0 + i);
-        for (uint32_t pos = s0 + lane; pos < e0; pos += 32) outKey[pos] = key;
+        // up to 3 single slots to a 16-byte boundary, 16-byte stores, the rest
+        const uint32_t a = min((s0 + 3u) & ~3u, e0);
+        const uint32_t b = a + ((e0 - a) & ~3u);
+        if (lane < a - s0) outKey[s0 + lane] = key;
+        const int4 kv = make_int4(key, key, key, key);
+        for (uint32_t pos = a + 4 * lane; pos < b; pos += 128) *reinterpret_cast<int4 *>(outKey + pos) = kv;
+        if (lane < e0 - b) outKey[b + lane] = key;
     }
 }
 
