@@ -187,7 +187,7 @@ struct Ctx {
     std::vector<double> taskPred, taskEvals;
     DevBuf<sj_task> dTasks;
     // batch state
-    DevBuf<uint32_t> keyCount, keyCursor;
+    DevBuf<uint32_t> keyCount, keyStart;
     DevBuf<int32_t> outKey, outVal;
     DevBuf<uint8_t> scanTemp;
     DevBuf<uint32_t> total;
@@ -195,11 +195,12 @@ struct Ctx {
     DevBuf<uint32_t> queueHead;
     DevBuf<uint32_t> taskHits;
     DevBuf<uint32_t> dTaskEvals, dTaskRefined;   // per task, written by the count pass
-    // count-pass records for the emission pass: per task, [block][query] hit
-    // masks and per-query row counts (offsets: prefix sums over all tasks)
-    std::vector<uint64_t> hMaskOff, hColOff, hRowOff;
-    DevBuf<uint64_t> dMaskOff, dColOff, dRowOff;
-    DevBuf<uint32_t> masks, colMasks, rowCnt;
+    // count-pass records for the emission pass: per task, row and column hit
+    // masks, per-query row-run offsets and per-position candidate records;
+    // offsets are prefix sums over all tasks, as are the emission units
+    std::vector<uint64_t> hMaskOff, hColOff, hRowOff, hCandOff, hUnitOff;
+    DevBuf<uint64_t> dMaskOff, dColOff, dRowOff, dCandOff, dUnitOff;
+    DevBuf<uint32_t> masks, colMasks, rowRel, candId, candRel;
     DevBuf<unsigned long long> batchTot;
     std::vector<cudaEvent_t> events;   // per-batch stage boundaries of the asynchronous phase
     PinBuf pinTotal, pinKey[2], pinVal[2];
@@ -688,27 +689,38 @@ sj_status run_count(Ctx &c, sj_join_args &a, bool queue)
 
 // Per-task record offsets of the count pass: per block of 32 stream
 // positions one row-mask word per query and (symmetric tasks) one column-mask
-// word per candidate and group of 32 queries; one row count per query.
+// word per candidate and group of 32 queries; one row-run offset per query;
+// one candidate record per stream position.  Also the emission units.
 sj_status task_offsets(Ctx &c)
 {
     const size_t nt = c.tasks.size();
     c.hMaskOff.assign(nt + 1, 0);
     c.hColOff.assign(nt + 1, 0);
     c.hRowOff.assign(nt + 1, 0);
+    c.hCandOff.assign(nt + 1, 0);
+    c.hUnitOff.assign(nt + 1, 0);
     for (size_t i = 0; i < nt; i++) {
         const sj_task &t = c.tasks[i];
-        const uint64_t blocks = ((uint64_t)(t.sEnd - t.sBegin) + 31) / 32;
+        const uint32_t len = t.sEnd - t.sBegin;
+        const bool sym = (t.flags & SJ_TASK_SYM) != 0;
+        const uint64_t blocks = ((uint64_t)len + 31) / 32;
         const uint64_t groups = ((uint64_t)t.qCount + 31) / 32;
         c.hMaskOff[i + 1] = c.hMaskOff[i] + blocks * t.qCount;
-        c.hColOff[i + 1] = c.hColOff[i] + ((t.flags & SJ_TASK_SYM) ? blocks * groups * 32 : 0);
+        c.hColOff[i + 1] = c.hColOff[i] + (sym ? blocks * groups * 32 : 0);
         c.hRowOff[i + 1] = c.hRowOff[i] + t.qCount;
+        c.hCandOff[i + 1] = c.hCandOff[i] + len;
+        c.hUnitOff[i + 1] = c.hUnitOff[i] + sj_task_units(t.qCount, len, sym);
     }
     CK(c.dMaskOff.ensure(nt + 1));
     CK(c.dColOff.ensure(nt + 1));
     CK(c.dRowOff.ensure(nt + 1));
+    CK(c.dCandOff.ensure(nt + 1));
+    CK(c.dUnitOff.ensure(nt + 1));
     CK(cudaMemcpyAsync(c.dMaskOff.p, c.hMaskOff.data(), sizeof(uint64_t) * (nt + 1), cudaMemcpyHostToDevice, c.s));
     CK(cudaMemcpyAsync(c.dColOff.p, c.hColOff.data(), sizeof(uint64_t) * (nt + 1), cudaMemcpyHostToDevice, c.s));
     CK(cudaMemcpyAsync(c.dRowOff.p, c.hRowOff.data(), sizeof(uint64_t) * (nt + 1), cudaMemcpyHostToDevice, c.s));
+    CK(cudaMemcpyAsync(c.dCandOff.p, c.hCandOff.data(), sizeof(uint64_t) * (nt + 1), cudaMemcpyHostToDevice, c.s));
+    CK(cudaMemcpyAsync(c.dUnitOff.p, c.hUnitOff.data(), sizeof(uint64_t) * (nt + 1), cudaMemcpyHostToDevice, c.s));
     return SJ_OK;
 }
 
@@ -769,7 +781,7 @@ sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
     const uint32_t nt = (uint32_t)c.tasks.size();
     c.st.num_tasks = nt;
     CK(c.keyCount.ensure(n));
-    CK(c.keyCursor.ensure(n));
+    CK(c.keyStart.ensure(n));
     CK(c.scanTemp.ensure(sj_scan_temp_bytes(n)));
     CK(c.total.ensure(1));
     CK(c.stat.ensure(8));
@@ -788,7 +800,7 @@ sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
 
     // greedy batch plan on predicted pairs (and on hit-mask words)
     std::vector<BatchRange> plan;
-    uint64_t maxMaskWords = 1, maxColWords = 1, maxRowWords = 1;
+    uint64_t maxMaskWords = 1, maxColWords = 1, maxRowWords = 1, maxCandRecs = 1;
     {
         const double alpha = c.p.alpha;
         uint32_t t0 = 0;
@@ -796,7 +808,8 @@ sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
         for (uint32_t t = 0; t < nt; t++) {
             double v = c.taskPred[t] * (1.0 + alpha);
             if (t > t0 && (acc + v > (double)cap || c.hMaskOff[t + 1] - c.hMaskOff[t0] > SJ_MASK_BATCH_WORDS ||
-                           c.hColOff[t + 1] - c.hColOff[t0] > SJ_MASK_BATCH_WORDS)) {
+                           c.hColOff[t + 1] - c.hColOff[t0] > SJ_MASK_BATCH_WORDS ||
+                           c.hUnitOff[t + 1] - c.hUnitOff[t0] > 0xffffffffULL)) {
                 plan.push_back({t0, t});
                 t0 = t;
                 acc = 0;
@@ -808,19 +821,22 @@ sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
             maxMaskWords = std::max<uint64_t>(maxMaskWords, c.hMaskOff[br.t1] - c.hMaskOff[br.t0]);
             maxColWords = std::max<uint64_t>(maxColWords, c.hColOff[br.t1] - c.hColOff[br.t0]);
             maxRowWords = std::max<uint64_t>(maxRowWords, c.hRowOff[br.t1] - c.hRowOff[br.t0]);
+            maxCandRecs = std::max<uint64_t>(maxCandRecs, c.hCandOff[br.t1] - c.hCandOff[br.t0]);
         }
     }
     std::reverse(plan.begin(), plan.end());   // used as a stack
     CK(c.masks.ensure(maxMaskWords));
     CK(c.colMasks.ensure(maxColWords));
-    CK(c.rowCnt.ensure(maxRowWords));
+    CK(c.rowRel.ensure(maxRowWords));
+    CK(c.candId.ensure(maxCandRecs));
+    CK(c.candRel.ensure(maxCandRecs));
 
     sj_join_args a;
     join_args_base(c, a);
     a.tasks = c.dTasks.p;
     a.queueHead = c.queueHead.p;
     a.keyCount = c.keyCount.p;
-    a.keyCursor = c.keyCursor.p;
+    a.keyStart = c.keyStart.p;
     a.outKey = c.outKey.p;
     a.outVal = c.outVal.p;
     a.capacity = cap;
@@ -832,8 +848,12 @@ sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
     a.maskOff = c.dMaskOff.p;
     a.colMasks = c.colMasks.p;
     a.colOff = c.dColOff.p;
-    a.rowCnt = c.rowCnt.p;
+    a.rowRel = c.rowRel.p;
     a.rowOff = c.dRowOff.p;
+    a.candId = c.candId.p;
+    a.candRel = c.candRel.p;
+    a.candOff = c.dCandOff.p;
+    a.unitOff = c.dUnitOff.p;
     {
         const FilterBounds fb = filter_bounds(c);
         a.margin = fb.margin;
@@ -843,7 +863,7 @@ sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
     std::vector<uint32_t> hTaskHits(nt);
     uint64_t pairsTotal = 0, batches = 0, retries = 0;
     double relErrSum = 0;
-    float msCount = 0, msScan = 0, msFill = 0, msDeliver = 0, msExpand = 0;
+    float msCount = 0, msScan = 0, msFill = 0, msDeliver = 0;
     int pinSel = 0;
     sj_status result = SJ_OK;
     CK(c.batchTot.ensure(plan.size() + 1));
@@ -856,9 +876,9 @@ sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
     };
 
     // ---- asynchronous phase: batches folded on the device (no host delivery).
-    // Every batch runs count -> scan -> fill -> key expansion -> hash without
-    // a host round trip; a batch whose count exceeds the output buffer skips
-    // its fill and is re-run below, split.
+    // Every batch runs count -> scan -> emission -> hash without a host round
+    // trip; a batch whose count exceeds the output buffer skips its emission
+    // and is re-run below, split.
     std::vector<BatchRange> stack;
     if (delivery == SJ_DELIVER_NONE && !plan.empty()) {
         double maxPred = 0;
@@ -874,7 +894,7 @@ sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
         a.outVal = c.outVal.p;
         a.capacity = bufCap;
         const size_t nplan = plan.size();
-        while (c.events.size() < 6 * nplan) {
+        while (c.events.size() < 5 * nplan) {
             cudaEvent_t e;
             CK(cudaEventCreate(&e));
             c.events.push_back(e);
@@ -885,18 +905,16 @@ sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
             a.taskBegin = br.t0;
             a.taskEnd = br.t1;
             a.batchPairs = c.batchTot.p + i;
-            CK(cudaEventRecord(ev[6 * i + 0], c.s));
+            CK(cudaEventRecord(ev[5 * i + 0], c.s));
             CKS(run_count(c, a, queue));
-            CK(cudaEventRecord(ev[6 * i + 1], c.s));
-            CK(sj_exclusive_scan_u32_clear(c.keyCount.p, c.keyCursor.p, n, c.scanTemp.p, c.total.p, c.s));
-            CK(cudaEventRecord(ev[6 * i + 2], c.s));
-            CK(sj_expand_keys(c.keyCursor.p, c.total.p, n, a.outKey, a.batchPairs, a.capacity, c.s));
-            CK(cudaEventRecord(ev[6 * i + 3], c.s));
-            if (queue) CK(cudaMemsetAsync(c.queueHead.p, 0, sizeof(uint32_t), c.s));
-            CK(sj_launch_emit(a, queue ? 1 : 0, c.numSM, c.s));
-            CK(cudaEventRecord(ev[6 * i + 4], c.s));
+            CK(cudaEventRecord(ev[5 * i + 1], c.s));
+            CK(sj_exclusive_scan_u32_clear(c.keyCount.p, c.keyStart.p, n, c.scanTemp.p, c.total.p, c.s));
+            CK(cudaEventRecord(ev[5 * i + 2], c.s));
+            CK(cudaMemsetAsync(c.queueHead.p, 0, sizeof(uint32_t), c.s));
+            CK(sj_launch_emit(a, c.numSM, c.s));
+            CK(cudaEventRecord(ev[5 * i + 3], c.s));
             CK(sj_hash_pairs_dev(c.outKey.p, c.outVal.p, a.batchPairs, bufCap, bufCap, c.stat.p + 4, c.s));
-            CK(cudaEventRecord(ev[6 * i + 5], c.s));
+            CK(cudaEventRecord(ev[5 * i + 4], c.s));
         }
         std::vector<unsigned long long> tot(nplan);
         CK(cudaMemcpyAsync(tot.data(), c.batchTot.p, sizeof(unsigned long long) * nplan, cudaMemcpyDeviceToHost,
@@ -904,17 +922,15 @@ sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
         CK(cudaMemcpyAsync(hTaskHits.data(), c.taskHits.p, sizeof(uint32_t) * nt, cudaMemcpyDeviceToHost, c.s));
         CK(cudaStreamSynchronize(c.s));
         for (size_t i = 0; i < nplan; i++) {
-            float t01, t12, t23, t34, t45;
-            cudaEventElapsedTime(&t01, ev[6 * i + 0], ev[6 * i + 1]);
-            cudaEventElapsedTime(&t12, ev[6 * i + 1], ev[6 * i + 2]);
-            cudaEventElapsedTime(&t23, ev[6 * i + 2], ev[6 * i + 3]);
-            cudaEventElapsedTime(&t34, ev[6 * i + 3], ev[6 * i + 4]);
-            cudaEventElapsedTime(&t45, ev[6 * i + 4], ev[6 * i + 5]);
+            float t01, t12, t23, t34;
+            cudaEventElapsedTime(&t01, ev[5 * i + 0], ev[5 * i + 1]);
+            cudaEventElapsedTime(&t12, ev[5 * i + 1], ev[5 * i + 2]);
+            cudaEventElapsedTime(&t23, ev[5 * i + 2], ev[5 * i + 3]);
+            cudaEventElapsedTime(&t34, ev[5 * i + 3], ev[5 * i + 4]);
             msCount += t01;
             msScan += t12;
-            msExpand += t23;
-            msFill += t34;
-            msDeliver += t45;
+            msFill += t23;
+            msDeliver += t34;
         }
         for (size_t i = 0; i < nplan; i++) {
             const BatchRange &br = plan[nplan - 1 - i];
@@ -947,7 +963,7 @@ sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
         CKS(run_count(c, a, queue));
         msCount += tb.stop(c.s);
         tb.start(c.s);
-        CK(sj_exclusive_scan_u32_clear(c.keyCount.p, c.keyCursor.p, n, c.scanTemp.p, c.total.p, c.s));
+        CK(sj_exclusive_scan_u32_clear(c.keyCount.p, c.keyStart.p, n, c.scanTemp.p, c.total.p, c.s));
         unsigned long long cnt = 0;
         CK(cudaMemcpyAsync(c.pinTotal.p, slot, sizeof(unsigned long long), cudaMemcpyDeviceToHost, c.s));
         CK(cudaMemcpyAsync(hTaskHits.data() + br.t0, c.taskHits.p + br.t0, sizeof(uint32_t) * (br.t1 - br.t0),
@@ -978,11 +994,8 @@ sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
         a.outVal = c.outVal.p;
         a.capacity = c.outKey.n;
         tb.start(c.s);
-        CK(sj_expand_keys(c.keyCursor.p, c.total.p, n, a.outKey, a.batchPairs, a.capacity, c.s));
-        msExpand += tb.stop(c.s);
-        tb.start(c.s);
-        if (queue) CK(cudaMemsetAsync(c.queueHead.p, 0, sizeof(uint32_t), c.s));
-        CK(sj_launch_emit(a, queue ? 1 : 0, c.numSM, c.s));
+        CK(cudaMemsetAsync(c.queueHead.p, 0, sizeof(uint32_t), c.s));
+        CK(sj_launch_emit(a, c.numSM, c.s));
         msFill += tb.stop(c.s);
         tb.start(c.s);
         CK(sj_hash_pairs(c.outKey.p, c.outVal.p, cnt, c.stat.p + 4, c.s));
@@ -1016,8 +1029,9 @@ sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
     unsigned long long hs[8];
     CK(cudaMemcpyAsync(hs, c.stat.p, sizeof(hs), cudaMemcpyDeviceToHost, c.s));
     CK(cudaStreamSynchronize(c.s));
-    if (hs[3]) {
-        set_error("internal: fill pass exceeded the counted capacity");
+    if (hs[3] || hs[6]) {
+        set_error(hs[3] ? "internal: the emission exceeded the counted capacity"
+                        : "internal: the emission met a count-pass record out of range");
         return SJ_ERR_INTERNAL;
     }
     {
@@ -1054,7 +1068,7 @@ sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
     c.st.ms_deliver = msDeliver;
     c.st.ms_join_kernels = msCount + msFill;
     c.st.ms_fill_kernel = msFill;
-    c.st.ms_expand = msExpand;
+    c.st.ms_expand = 0.0f;   // keys are written by the emission pass
     c.st.ms_total = total.stop(c.s);
     c.st.kernel_launches = sj_launch_total() - launches0;
     return result;

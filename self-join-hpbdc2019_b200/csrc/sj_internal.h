@@ -75,11 +75,11 @@ struct sj_join_args {
     uint32_t taskBegin, taskEnd;
     uint32_t *queueHead;        // persistent-queue cursor (work-queue modes)
     uint32_t *keyCount;         // count pass: per point-id pair counts
-    uint32_t *keyCursor;        // emission: per point-id write cursors (exclusive offsets)
-    int32_t *outKey, *outVal;   // batch output (keys by sj_expand_keys, values by the emission)
+    const uint32_t *keyStart;   // emission: first slot of each point id's key run (exclusive scan)
+    int32_t *outKey, *outVal;   // batch output, written by the emission
     uint64_t capacity;          // pairs the output buffers hold
     unsigned long long *stat;   // [2] pairs (count pass), [3] run past capacity, [4] set hash,
-                                // [5] batches skipped for overflow
+                                // [5] batches skipped for overflow, [6] emission record out of range
     unsigned long long *batchPairs;  // this batch's pair total (count pass adds, later passes read)
     uint32_t *taskHits;         // optional per-task measured pairs (count pass)
     // count-pass records consumed by the emission pass (null: not recorded).
@@ -90,8 +90,14 @@ struct sj_join_args {
     uint32_t *colMasks;         // per symmetric task: column hit masks [block][query group][candidate],
                                 // bit i = query 32*group+i (the query itself dropped on the home diagonal)
     const uint64_t *colOff;     // per task: first column-mask word
-    uint32_t *rowCnt;           // per task and query: pairs keyed by the query
-    const uint64_t *rowOff;     // per task: first row count
+    uint32_t *rowRel;           // per task and query: offset of the task's row run inside the
+                                // query's key run (the key's count before the task added to it)
+    const uint64_t *rowOff;     // per task: first row offset
+    uint32_t *candId;           // per task and stream position: the candidate's point id
+    uint32_t *candRel;          // per symmetric task and stream position: offset of the position's
+                                // column run inside the candidate's key run
+    const uint64_t *candOff;    // per task: first candidate record (prefix of stream lengths)
+    const uint64_t *unitOff;    // per task: first emission unit (query groups, then column blocks)
     uint32_t *taskEvals;        // per task: candidate evaluations
     uint32_t *taskRefined;      // per task: FP32 borderline re-evaluations
     double margin;              // FP32 filter: bound M on |FP32 estimate - (FP64 d2 - T)|
@@ -133,10 +139,6 @@ cudaError_t sj_hash_pairs(const int32_t *key, const int32_t *val, uint64_t m,
 // same, with the pair count read on the device (skipped when it exceeds cap)
 cudaError_t sj_hash_pairs_dev(const int32_t *key, const int32_t *val, const unsigned long long *count, uint64_t cap,
                               uint64_t gridHint, unsigned long long *hashOut, cudaStream_t s);
-// keys of a batch from its row structure: key k owns [excl[k], excl[k+1])
-// (excl[n] = *total); skipped when the batch's count exceeds cap
-cudaError_t sj_expand_keys(const uint32_t *excl, const uint32_t *total, uint64_t n, int32_t *outKey,
-                           const unsigned long long *batchPairs, uint64_t cap, cudaStream_t s);
 
 // index build (sj_index.cu)
 cudaError_t sj_launch_minmax(const double *pts, uint64_t n, int D, double *minmax_dev, cudaStream_t s);
@@ -159,9 +161,16 @@ cudaError_t sj_launch_neighbours(const uint64_t *cellLid, const uint32_t *cellCo
 // join (sj_join.cu): the count pass (per-key pair counts, hit masks)
 cudaError_t sj_launch_join(const sj_join_args &a, const sj_grid_dev &g, int fp32, int queue, int numSM,
                            cudaStream_t s);
-// emission (sj_emit.cu): pair values from the recorded hit masks into the
-// counted row slots
-cudaError_t sj_launch_emit(const sj_join_args &a, int queue, int numSM, cudaStream_t s);
+// emission (sj_emit.cu): (key, value) pairs from the recorded hit masks into
+// their key runs; a.queueHead must be zero at launch
+cudaError_t sj_launch_emit(const sj_join_args &a, int numSM, cudaStream_t s);
+
+// emission units of a task: one per group of 32 queries, plus one per block of
+// 32 stream positions for a symmetric task
+__host__ __device__ inline uint32_t sj_task_units(uint32_t qCount, uint32_t streamLen, bool sym)
+{
+    return (qCount + 31) / 32 + (sym ? (streamLen + 31) / 32 : 0u);
+}
 
 // estimators (sj_estimate.cu)
 cudaError_t sj_launch_sample(const sj_join_args &a, const sj_grid_dev &g, uint32_t sampleStride,

@@ -12,11 +12,12 @@
 // emit (p,q) and (q,p) from one evaluation).
 //
 // The pass produces per-key pair counts (the row lengths of a batch) and
-// records every hit mask; the emission pass (sj_emit.cu) writes the pairs from
-// those masks at exclusive offsets of the counts, so each key's values land
-// contiguously and keys come out ascending -- the order thrust::sort_by_key
-// gives the reference (GPU.cu:2336) -- without sorting and without evaluating
-// any distance twice.
+// records every hit mask, each run's offset inside its key's run (the value an
+// atomicAdd on the key's count returns) and the candidates' point ids; the
+// emission pass (sj_emit.cu) writes the pairs from those records at the
+// exclusive offsets of the counts, so each key's values land contiguously and
+// keys come out ascending -- the order thrust::sort_by_key gives the reference
+// (GPU.cu:2336) -- without sorting and without evaluating any distance twice.
 //
 // Predicate (kernel.cu:344-349): the squared distance in the reference build's
 // rounding order (ref_dist2), hit iff sqrt(acc) <= eps, evaluated as acc <= T
@@ -371,6 +372,9 @@ __global__ void __launch_bounds__(SJ_CTA, F32 ? SJ_JOIN_MIN_BLOCKS_F32 : SJ_JOIN
         const long long T1 = __double_as_longlong(T) + 1;
         uint32_t *const maskBase = a.masks ? a.masks + (a.maskOff[t] - a.maskOff[a.taskBegin]) : nullptr;
         uint32_t *const colBase = (a.colMasks && sym) ? a.colMasks + (a.colOff[t] - a.colOff[a.taskBegin]) : nullptr;
+        const uint64_t candRecOff = a.candOff ? a.candOff[t] - a.candOff[a.taskBegin] : 0;
+        uint32_t *const candIdRec = a.candId ? a.candId + candRecOff : nullptr;
+        uint32_t *const candRelRec = (a.candRel && sym) ? a.candRel + candRecOff : nullptr;
 
         uint32_t rowCount[R];   // pairs keyed by each query
         uint32_t evals = 0;     // candidate evaluations
@@ -394,7 +398,9 @@ __global__ void __launch_bounds__(SJ_CTA, F32 ? SJ_JOIN_MIN_BLOCKS_F32 : SJ_JOIN
                     if (segPre[mid] <= s) lo = mid; else hi = mid;
                 }
                 uint32_t pos = segStart[lo] + (s - segPre[lo]);
-                candId[j] = a.ids[pos];
+                const uint32_t cid = a.ids[pos];
+                candId[j] = cid;
+                if (candIdRec) candIdRec[s - task.sBegin] = cid;   // the emission's candidate record
                 const double *src = a.xs + (uint64_t)pos * DP;
                 if constexpr (F32) {
                     float *dst = reinterpret_cast<float *>(&st.c[j >> 1][0]) + (j & 1);
@@ -480,22 +486,26 @@ __global__ void __launch_bounds__(SJ_CTA, F32 ? SJ_JOIN_MIN_BLOCKS_F32 : SJ_JOIN
                     uint32_t tot = 0;
 #pragma unroll
                     for (int w = 0; w < NW; w++) { tot += colCnt[w][j]; colCnt[w][j] = 0; }
-                    if (tot) { atomicAdd(&a.keyCount[candId[j]], tot); local += tot; }
+                    // the count before this stage's addition is the offset of
+                    // these column pairs inside the candidate's key run
+                    const uint32_t rel = tot ? atomicAdd(&a.keyCount[candId[j]], tot) : 0u;
+                    if (candRelRec) candRelRec[sBase + j - task.sBegin] = rel;
+                    local += tot;
                 }
                 if (local) atomicAdd(&sm.taskPairs, (unsigned long long)local);
             }
         }
         {
             uint32_t mine = 0;
-            uint32_t *const rowBase = a.rowCnt ? a.rowCnt + (a.rowOff[t] - a.rowOff[a.taskBegin]) : nullptr;
+            uint32_t *const rowBase = a.rowRel ? a.rowRel + (a.rowOff[t] - a.rowOff[a.taskBegin]) : nullptr;
 #pragma unroll
             for (int r = 0; r < R; r++) {
                 const uint32_t qi = (uint32_t)r * SJ_CTA + tid;
-                if (rowBase && qi < task.qCount) rowBase[qi] = rowCount[r];
-                if (rowCount[r]) {
-                    atomicAdd(&a.keyCount[qid[r]], rowCount[r]);
-                    mine += rowCount[r];
-                }
+                // the key's count before this addition: where this task's row
+                // run starts inside the query's key run
+                const uint32_t rel = rowCount[r] ? atomicAdd(&a.keyCount[qid[r]], rowCount[r]) : 0u;
+                if (rowBase && qi < task.qCount) rowBase[qi] = rel;
+                mine += rowCount[r];
             }
             if (mine) atomicAdd(&sm.taskPairs, (unsigned long long)mine);
         }

@@ -287,39 +287,6 @@ __global__ void __launch_bounds__(256) k_hash_pairs_dev(const int32_t *__restric
     }
 }
 
-// Keys of a batch: key k owns slots [excl[k], excl[k+1]) (excl[n] = *total).
-// A warp takes 32 consecutive keys and writes each key's run with all lanes,
-// 128 contiguous bytes per store.
-__global__ void __launch_bounds__(256) k_expand_keys(const uint32_t *__restrict__ excl,
-                                                     const uint32_t *__restrict__ total, uint64_t n,
-                                                     int32_t *__restrict__ outKey,
-                                                     const unsigned long long *__restrict__ batchPairs, uint64_t cap)
-{
-    if (*batchPairs > cap) return;
-    const uint32_t lane = threadIdx.x & 31u;
-    const uint64_t k0 = ((uint64_t)blockIdx.x * 256 + (threadIdx.x & ~31u));
-    if (k0 >= n) return;
-    const uint64_t k = k0 + lane;
-    const uint32_t tot = *total;
-    const uint32_t st = k < n ? excl[k] : tot;
-    const uint32_t en = k + 1 < n ? excl[k + 1] : tot;
-    uint32_t live = __ballot_sync(0xffffffffu, en > st);
-    while (live) {
-        const int i = __ffs(live) - 1;
-        live &= live - 1;
-        const uint32_t s0 = __shfl_sync(0xffffffffu, st, i);
-        const uint32_t e0 = __shfl_sync(0xffffffffu, en, i);
-        const int32_t key = (int32_t)(k0 + i);
-        // up to 3 single slots to a 16-byte boundary, 16-byte stores, the rest
-        const uint32_t a = min((s0 + 3u) & ~3u, e0);
-        const uint32_t b = a + ((e0 - a) & ~3u);
-        if (lane < a - s0) outKey[s0 + lane] = key;
-        const int4 kv = make_int4(key, key, key, key);
-        for (uint32_t pos = a + 4 * lane; pos < b; pos += 128) *reinterpret_cast<int4 *>(outKey + pos) = kv;
-        if (lane < e0 - b) outKey[b + lane] = key;
-    }
-}
-
 }  // namespace
 
 cudaError_t sj_hash_pairs_dev(const int32_t *key, const int32_t *val, const unsigned long long *count, uint64_t cap,
@@ -329,15 +296,6 @@ cudaError_t sj_hash_pairs_dev(const int32_t *key, const int32_t *val, const unsi
     if (blocks > 148 * 8) blocks = 148 * 8;
     if (blocks == 0) blocks = 1;
     k_hash_pairs_dev<<<(unsigned)blocks, 256, 0, s>>>(key, val, count, cap, hashOut);
-    sj_note_launch();
-    return cudaGetLastError();
-}
-
-cudaError_t sj_expand_keys(const uint32_t *excl, const uint32_t *total, uint64_t n, int32_t *outKey,
-                           const unsigned long long *batchPairs, uint64_t cap, cudaStream_t s)
-{
-    if (n == 0) return cudaSuccess;
-    k_expand_keys<<<(unsigned)ceil_div(n, 256), 256, 0, s>>>(excl, total, n, outKey, batchPairs, cap);
     sj_note_launch();
     return cudaGetLastError();
 }

@@ -59,13 +59,14 @@ def test_engine_matches_reference_pairs(path, prec):
         assert st.pair_hash == int(f["mode3_hash"])
 
 
-@pytest.mark.parametrize("path", FIXTURES[:4], ids=[os.path.basename(p)[:-4] for p in FIXTURES[:4]])
-def test_engine_matches_reference_in_small_batches(path):
-    # a batch capacity of ~1/5 of the set forces several batches (and overflow retries)
-    f = _load(path)
+@pytest.mark.parametrize("mode", [3, 6, 10])
+@pytest.mark.parametrize("prec", [sjoin.PREC_FP64, sjoin.PREC_FP32_REFINE])
+def test_engine_matches_reference_in_several_batches(mode, prec):
+    # the smallest batch capacity the engine accepts (65536 pairs) splits the
+    # largest fixture (72,448 pairs) into at least two batches
+    f = _load(os.path.join(HERE, "golden", "exp4d.npz"))
     pts, eps, k = f["pts"], float(f["eps"]), int(f["k"])
     ref_key = np.repeat(np.arange(len(pts), dtype=np.int32), f["deg"])
-    cap = max(int(f["deg"].max()) * 4, len(ref_key) // 5)
-    key, val, st = _join(pts, eps, k, 10, sjoin.PREC_FP32_REFINE, capacity=cap)
+    key, val, st = _join(pts, eps, k, mode, prec, capacity=65536)
     assert st.num_batches >= 2
     assert np.array_equal(key, ref_key) and np.array_equal(val, f["val"])
