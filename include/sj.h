@@ -106,8 +106,7 @@ typedef struct {
     float ms_join_kernels;      /* count + fill kernel time */
     float ms_fill_kernel;       /* fill kernel time alone */
     uint64_t kernel_launches;   /* this library's kernel launches during the last join */
-    float ms_expand;            /* 0: keys are written together with the values by the emission pass
-                                   (the field keeps the struct's layout) */
+    float ms_expand;            /* key-array expansion from the batch's key runs */
 } sj_stats;
 
 /* Fill `p` with params.h defaults: D=k=2, BLOCKSIZE 256, THREADPERPOINT 1,

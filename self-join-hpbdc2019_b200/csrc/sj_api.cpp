@@ -203,7 +203,11 @@ struct Ctx {
     DevBuf<uint32_t> masks, colMasks, rowRel, candId, candRel;
     DevBuf<unsigned long long> batchTot;
     std::vector<cudaEvent_t> events;   // per-batch stage boundaries of the asynchronous phase
-    PinBuf pinTotal, pinKey[2], pinVal[2];
+    PinBuf pinTotal, pinKey[2], pinVal[2], pinStart[2];
+    // host delivery: copy stream and its events (per pinned buffer set: run
+    // offsets copied, values copied)
+    cudaStream_t cs = nullptr;
+    cudaEvent_t evStart[2] = {nullptr, nullptr}, evVals[2] = {nullptr, nullptr}, evEmit = nullptr;
     // estimator
     std::vector<float> mlpW;
     DevBuf<float> dMlpW;
@@ -754,6 +758,19 @@ uint64_t auto_capacity(Ctx &c)
     return std::max<uint64_t>(1 << 20, std::min<uint64_t>(byMem, 2000000000ULL));
 }
 
+// Keys of a delivered batch from its run offsets: key k owns slots
+// [start[k], start[k+1]) (start[n] = cnt).  Parallel over keys on the host.
+void expand_keys_host(const uint32_t *start, uint64_t n, uint64_t cnt, int32_t *key)
+{
+    if (cnt == 0) return;
+#pragma omp parallel for schedule(static)
+    for (int64_t k = 0; k < (int64_t)n; k++) {
+        const uint64_t b = start[k];
+        const uint64_t e = (k + 1 < (int64_t)n) ? start[k + 1] : cnt;
+        for (uint64_t i = b; i < e; i++) key[i] = (int32_t)k;
+    }
+}
+
 sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
 {
     const unsigned long long launches0 = sj_launch_total();
@@ -863,7 +880,7 @@ sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
     std::vector<uint32_t> hTaskHits(nt);
     uint64_t pairsTotal = 0, batches = 0, retries = 0;
     double relErrSum = 0;
-    float msCount = 0, msScan = 0, msFill = 0, msDeliver = 0;
+    float msCount = 0, msScan = 0, msFill = 0, msDeliver = 0, msExpand = 0;
     int pinSel = 0;
     sj_status result = SJ_OK;
     CK(c.batchTot.ensure(plan.size() + 1));
@@ -876,9 +893,9 @@ sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
     };
 
     // ---- asynchronous phase: batches folded on the device (no host delivery).
-    // Every batch runs count -> scan -> emission -> hash without a host round
-    // trip; a batch whose count exceeds the output buffer skips its emission
-    // and is re-run below, split.
+    // Every batch runs count -> scan -> key expansion -> emission -> hash
+    // without a host round trip; a batch whose count exceeds the output buffer
+    // skips its expansion and emission and is re-run below, split.
     std::vector<BatchRange> stack;
     if (delivery == SJ_DELIVER_NONE && !plan.empty()) {
         double maxPred = 0;
@@ -894,7 +911,7 @@ sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
         a.outVal = c.outVal.p;
         a.capacity = bufCap;
         const size_t nplan = plan.size();
-        while (c.events.size() < 5 * nplan) {
+        while (c.events.size() < 6 * nplan) {
             cudaEvent_t e;
             CK(cudaEventCreate(&e));
             c.events.push_back(e);
@@ -905,16 +922,18 @@ sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
             a.taskBegin = br.t0;
             a.taskEnd = br.t1;
             a.batchPairs = c.batchTot.p + i;
-            CK(cudaEventRecord(ev[5 * i + 0], c.s));
+            CK(cudaEventRecord(ev[6 * i + 0], c.s));
             CKS(run_count(c, a, queue));
-            CK(cudaEventRecord(ev[5 * i + 1], c.s));
+            CK(cudaEventRecord(ev[6 * i + 1], c.s));
             CK(sj_exclusive_scan_u32_clear(c.keyCount.p, c.keyStart.p, n, c.scanTemp.p, c.total.p, c.s));
-            CK(cudaEventRecord(ev[5 * i + 2], c.s));
+            CK(cudaEventRecord(ev[6 * i + 2], c.s));
+            CK(sj_expand_keys(c.keyStart.p, c.total.p, n, a.outKey, a.batchPairs, a.capacity, c.s));
+            CK(cudaEventRecord(ev[6 * i + 3], c.s));
             CK(cudaMemsetAsync(c.queueHead.p, 0, sizeof(uint32_t), c.s));
             CK(sj_launch_emit(a, c.numSM, c.s));
-            CK(cudaEventRecord(ev[5 * i + 3], c.s));
+            CK(cudaEventRecord(ev[6 * i + 4], c.s));
             CK(sj_hash_pairs_dev(c.outKey.p, c.outVal.p, a.batchPairs, bufCap, bufCap, c.stat.p + 4, c.s));
-            CK(cudaEventRecord(ev[5 * i + 4], c.s));
+            CK(cudaEventRecord(ev[6 * i + 5], c.s));
         }
         std::vector<unsigned long long> tot(nplan);
         CK(cudaMemcpyAsync(tot.data(), c.batchTot.p, sizeof(unsigned long long) * nplan, cudaMemcpyDeviceToHost,
@@ -922,15 +941,17 @@ sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
         CK(cudaMemcpyAsync(hTaskHits.data(), c.taskHits.p, sizeof(uint32_t) * nt, cudaMemcpyDeviceToHost, c.s));
         CK(cudaStreamSynchronize(c.s));
         for (size_t i = 0; i < nplan; i++) {
-            float t01, t12, t23, t34;
-            cudaEventElapsedTime(&t01, ev[5 * i + 0], ev[5 * i + 1]);
-            cudaEventElapsedTime(&t12, ev[5 * i + 1], ev[5 * i + 2]);
-            cudaEventElapsedTime(&t23, ev[5 * i + 2], ev[5 * i + 3]);
-            cudaEventElapsedTime(&t34, ev[5 * i + 3], ev[5 * i + 4]);
+            float t01, t12, t23, t34, t45;
+            cudaEventElapsedTime(&t01, ev[6 * i + 0], ev[6 * i + 1]);
+            cudaEventElapsedTime(&t12, ev[6 * i + 1], ev[6 * i + 2]);
+            cudaEventElapsedTime(&t23, ev[6 * i + 2], ev[6 * i + 3]);
+            cudaEventElapsedTime(&t34, ev[6 * i + 3], ev[6 * i + 4]);
+            cudaEventElapsedTime(&t45, ev[6 * i + 4], ev[6 * i + 5]);
             msCount += t01;
             msScan += t12;
-            msFill += t23;
-            msDeliver += t34;
+            msExpand += t23;
+            msFill += t34;
+            msDeliver += t45;
         }
         for (size_t i = 0; i < nplan; i++) {
             const BatchRange &br = plan[nplan - 1 - i];
@@ -948,9 +969,32 @@ sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
         stack = plan;
     }
 
-    // ---- synchronous phase: host / device delivery, and batches to re-plan
+    // ---- synchronous phase: host / device delivery, and batches to re-plan.
+    // Host delivery does not copy the key array over PCIe: the keys of a
+    // batch are ascending runs, so the copy stream brings back the values and
+    // the per-key run offsets (keyStart), and the host cores expand the keys
+    // into pinned memory.  A batch is handed to the callback after the next
+    // batch's GPU work and copies have been queued, so the expansion and the
+    // callback overlap them (double-buffered pinned sets).
     Timer tb;
     unsigned long long *slot = c.batchTot.p + plan.size();
+    struct Pending {
+        bool live = false;
+        uint64_t cnt = 0, index = 0;
+        int sel = 0;
+    } pend;
+    auto finishPending = [&]() -> sj_status {
+        if (!pend.live) return SJ_OK;
+        pend.live = false;
+        CK(cudaEventSynchronize(c.evVals[pend.sel]));
+        int32_t *hk = (int32_t *)c.pinKey[pend.sel].p, *hv = (int32_t *)c.pinVal[pend.sel].p;
+        expand_keys_host((const uint32_t *)c.pinStart[pend.sel].p, n, pend.cnt, hk);
+        if (cb) {
+            sj_batch b{pend.index, pend.cnt, hk, hv, 0};
+            if (cb(&b, user)) return SJ_ERR_ABORTED;
+        }
+        return SJ_OK;
+    };
     while (!stack.empty() && result == SJ_OK) {
         BatchRange br = stack.back();
         stack.pop_back();
@@ -963,6 +1007,8 @@ sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
         CKS(run_count(c, a, queue));
         msCount += tb.stop(c.s);
         tb.start(c.s);
+        // the previous batch's run offsets must be copied before the scan rewrites them
+        if (pend.live) CK(cudaStreamWaitEvent(c.s, c.evStart[pend.sel], 0));
         CK(sj_exclusive_scan_u32_clear(c.keyCount.p, c.keyStart.p, n, c.scanTemp.p, c.total.p, c.s));
         unsigned long long cnt = 0;
         CK(cudaMemcpyAsync(c.pinTotal.p, slot, sizeof(unsigned long long), cudaMemcpyDeviceToHost, c.s));
@@ -986,6 +1032,7 @@ sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
         if (cnt > 0) relErrSum += std::fabs(predOf(br) - (double)cnt) / (double)cnt;
         // output buffers follow the exact batch size (grow-only, 25% headroom, <= capacity)
         if (cnt > c.outKey.n) {
+            CKS(finishPending());   // its copy may still read the old buffers
             uint64_t want = std::min<uint64_t>(cap, std::max<uint64_t>(cnt, (uint64_t)(1.25 * (double)c.outKey.n)));
             CK(c.outKey.ensure(want));
             CK(c.outVal.ensure(want));
@@ -993,6 +1040,11 @@ sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
         a.outKey = c.outKey.p;
         a.outVal = c.outVal.p;
         a.capacity = c.outKey.n;
+        tb.start(c.s);
+        // the previous batch's values must be copied before the emission rewrites them
+        if (pend.live) CK(cudaStreamWaitEvent(c.s, c.evVals[pend.sel], 0));
+        CK(sj_expand_keys(c.keyStart.p, c.total.p, n, a.outKey, a.batchPairs, a.capacity, c.s));
+        msExpand += tb.stop(c.s);
         tb.start(c.s);
         CK(cudaMemsetAsync(c.queueHead.p, 0, sizeof(uint32_t), c.s));
         CK(sj_launch_emit(a, c.numSM, c.s));
@@ -1004,28 +1056,46 @@ sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
             sj_batch b{batches, cnt, c.outKey.p, c.outVal.p, 1};
             if (cb(&b, user)) result = SJ_ERR_ABORTED;
         } else if (delivery == SJ_DELIVER_HOST) {
-            if (cnt * sizeof(int32_t) > c.pinKey[pinSel].bytes) {
-                size_t want = std::max<size_t>(cnt * sizeof(int32_t), (size_t)(1.25 * (double)c.pinKey[pinSel].bytes));
-                want = std::min<size_t>(want, cap * sizeof(int32_t));
-                CK(c.pinKey[pinSel].ensure(want));
-                CK(c.pinVal[pinSel].ensure(want));
+            const int sel = pinSel;
+            const size_t vb = std::max<size_t>(cnt, 1) * sizeof(int32_t);
+            if (vb > c.pinVal[sel].bytes) {
+                size_t want = std::max<size_t>(vb, (size_t)(1.25 * (double)c.pinVal[sel].bytes));
+                want = std::min<size_t>(std::max<size_t>(want, vb), cap * sizeof(int32_t));
+                CK(c.pinKey[sel].ensure(want));
+                CK(c.pinVal[sel].ensure(want));
             }
-            int32_t *hk = (int32_t *)c.pinKey[pinSel].p, *hv = (int32_t *)c.pinVal[pinSel].p;
-            if (cnt) {
-                CK(cudaMemcpyAsync(hk, c.outKey.p, cnt * sizeof(int32_t), cudaMemcpyDeviceToHost, c.s));
-                CK(cudaMemcpyAsync(hv, c.outVal.p, cnt * sizeof(int32_t), cudaMemcpyDeviceToHost, c.s));
+            CK(c.pinStart[sel].ensure(n * sizeof(uint32_t)));
+            CK(cudaEventRecord(c.evEmit, c.s));
+            CK(cudaStreamWaitEvent(c.cs, c.evEmit, 0));
+            CK(cudaMemcpyAsync(c.pinStart[sel].p, c.keyStart.p, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, c.cs));
+            CK(cudaEventRecord(c.evStart[sel], c.cs));
+            if (cnt)
+                CK(cudaMemcpyAsync(c.pinVal[sel].p, c.outVal.p, cnt * sizeof(int32_t), cudaMemcpyDeviceToHost, c.cs));
+            CK(cudaEventRecord(c.evVals[sel], c.cs));
+            // the previous batch goes to the consumer while this one is copied
+            sj_status ps = finishPending();
+            if (ps != SJ_OK) {
+                result = ps;
+                if (ps != SJ_ERR_ABORTED) return ps;
             }
-            CK(cudaStreamSynchronize(c.s));
-            if (cb) {
-                sj_batch b{batches, cnt, hk, hv, 0};
-                if (cb(&b, user)) result = SJ_ERR_ABORTED;
-            }
+            pend.live = true;
+            pend.cnt = cnt;
+            pend.index = batches;
+            pend.sel = sel;
             pinSel ^= 1;
         }
         msDeliver += tb.stop(c.s);
         pairsTotal += cnt;
         batches++;
     }
+    if (result == SJ_OK) {
+        sj_status ps = finishPending();
+        if (ps != SJ_OK) {
+            result = ps;
+            if (ps != SJ_ERR_ABORTED) return ps;
+        }
+    }
+    CK(cudaStreamSynchronize(c.cs));
     unsigned long long hs[8];
     CK(cudaMemcpyAsync(hs, c.stat.p, sizeof(hs), cudaMemcpyDeviceToHost, c.s));
     CK(cudaStreamSynchronize(c.s));
@@ -1068,7 +1138,7 @@ sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
     c.st.ms_deliver = msDeliver;
     c.st.ms_join_kernels = msCount + msFill;
     c.st.ms_fill_kernel = msFill;
-    c.st.ms_expand = 0.0f;   // keys are written by the emission pass
+    c.st.ms_expand = msExpand;
     c.st.ms_total = total.stop(c.s);
     c.st.kernel_launches = sj_launch_total() - launches0;
     return result;
@@ -1227,6 +1297,12 @@ sj_status sj_create(const sj_params *p, void **out)
     e = cudaSetDevice(c->dev);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&c->numSM, cudaDevAttrMultiProcessorCount, c->dev);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->s, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->cs, cudaStreamNonBlocking);
+    for (int i = 0; i < 2 && e == cudaSuccess; i++) {
+        e = cudaEventCreateWithFlags(&c->evStart[i], cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->evVals[i], cudaEventDisableTiming);
+    }
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->evEmit, cudaEventDisableTiming);
     if (e != cudaSuccess) {
         set_error("device setup: %s", cudaGetErrorString(e));
         delete c;
@@ -1242,10 +1318,17 @@ sj_status sj_destroy(void *ctx)
     Ctx *c = as_ctx(ctx);
     cudaSetDevice(c->dev);
     cudaStreamSynchronize(c->s);
-    cudaStream_t s = c->s;
+    if (c->cs) cudaStreamSynchronize(c->cs);
+    cudaStream_t s = c->s, cs = c->cs;
     for (cudaEvent_t e : c->events) cudaEventDestroy(e);
+    for (int i = 0; i < 2; i++) {
+        if (c->evStart[i]) cudaEventDestroy(c->evStart[i]);
+        if (c->evVals[i]) cudaEventDestroy(c->evVals[i]);
+    }
+    if (c->evEmit) cudaEventDestroy(c->evEmit);
     delete c;
     if (s) cudaStreamDestroy(s);
+    if (cs) cudaStreamDestroy(cs);
     return SJ_OK;
 }
 

@@ -20,14 +20,18 @@
 //               contiguous; a window of 32 words (lane = word; one window
 //               spans several queries when the task has few blocks) is
 //               popcounted and scanned, its set bits are decoded into shared
-//               memory as (word, bit) entries in slot order, and the warp
+//               memory as (query, stream position) entries in slot order, and the warp
 //               copies the entries out: consecutive entries of one query go to
 //               consecutive slots, so the stores are coalesced.
 //   column unit (symmetric task, block of 32 stream positions): lane j is
 //               candidate j; per query group its word is decoded lane-major
 //               and copied out the same way, each lane's run continuing across
 //               groups.
-// Both keys and values are written here.  Every record index is checked
+// Only the values are written here: the keys of a batch are its key runs in
+// key order, which sj_expand_keys writes sequentially (the emission's writes
+// land at scattered run positions, which HBM absorbs at a fraction of its
+// sequential rate, so writing the keys there too would cost more than the
+// separate sequential pass).  Every record index is checked
 // against its task's sizes; an index out of range (which a consistent count
 // pass never produces) skips the write and raises an error flag that the host
 // reports.  No distance is evaluated, so the pass is the same for both
@@ -42,12 +46,17 @@ constexpr int EW = 256;             // threads per emission CTA (independent war
 constexpr int ENW = EW / 32;
 constexpr int EM_CAP = 1024;        // staged entries per warp: one window of 32 words x 32 bits
 constexpr uint32_t FULL = 0xffffffffu;
+constexpr uint32_t NO_SLOT = 0xffffffffu;
+#ifndef SJ_EMIT_UNROLL
+#define SJ_EMIT_UNROLL 4
+#endif
+constexpr int CO = SJ_EMIT_UNROLL;  // copy-out entries per lane whose loads are in flight together
 
 struct WarpSmem {
-    uint16_t ent[EM_CAP];   // staged entries: (lane << 5) | bit, in slot order
+    uint32_t ent[EM_CAP];   // staged entries in slot order: rows (query << 16) | chunk position,
+                            // columns (lane << 5) | query bit
     uint32_t base[32];      // slot of entry 0 of the window for each query (rows) / lane (columns)
     uint32_t start[32];     // rows: slot of each query's first pair of the chunk
-    int32_t key[32];        // key of each query (rows) / candidate (columns)
 };
 
 __device__ __forceinline__ uint32_t warp_incl_scan(uint32_t x, uint32_t lane)
@@ -61,19 +70,19 @@ __device__ __forceinline__ uint32_t warp_incl_scan(uint32_t x, uint32_t lane)
 }
 
 // Appends tag | (index of each set bit of m), lowest bit first, to buf[k...].
-__device__ __forceinline__ void decode_bits(uint32_t m, uint32_t tag, uint16_t *buf, uint32_t k)
+__device__ __forceinline__ void decode_bits(uint32_t m, uint32_t tag, uint32_t *buf, uint32_t k)
 {
+    uint32_t *p = buf + k;
     while (m) {
         const uint32_t b = __ffs(m) - 1;
         m &= m - 1;
-        buf[k++] = (uint16_t)(tag | b);
+        *p++ = tag | b;
     }
 }
 
-__device__ __forceinline__ void put(const sj_join_args &a, uint32_t slot, int32_t key, int32_t val)
+__device__ __forceinline__ void put(const sj_join_args &a, uint32_t slot, int32_t val)
 {
     if (slot < a.capacity) {
-        a.outKey[slot] = key;
         a.outVal[slot] = val;
     } else {
         atomicMax(&a.stat[3], 1ULL);
@@ -85,7 +94,7 @@ struct UnitTask {
     uint32_t t, qBegin, qc, L;
 };
 
-// Row unit: queries 32g .. 32g+nq-1 of task u.t, key = query, value = candidate.
+// Row unit: queries 32g .. 32g+nq-1 of task u.t (key = query, value = candidate).
 __device__ __forceinline__ void emit_rows(const sj_join_args &a, const UnitTask &u, uint32_t g, WarpSmem &w,
                                           uint32_t lane)
 {
@@ -100,7 +109,6 @@ __device__ __forceinline__ void emit_rows(const sj_join_args &a, const UnitTask 
     __syncwarp();        // the previous unit is done with the warp's shared memory
     if (lane < nq) {
         const uint32_t qid = a.ids[u.qBegin + q0 + lane];
-        w.key[lane] = (int32_t)qid;
         next = a.keyStart[qid] + rel[q0 + lane];
     }
     for (uint32_t c0 = 0; c0 < nBlk; c0 += 64) {
@@ -112,9 +120,12 @@ __device__ __forceinline__ void emit_rows(const sj_join_args &a, const UnitTask 
         __syncwarp();
         w.start[lane] = next;
         uint32_t carry = 0;   // entries of earlier windows of this chunk
+        uint32_t nextWord = lane < nw ? __ldg(wq + lane) : 0u;
         for (uint32_t ws = 0; ws < nw; ws += 32) {
             const uint32_t f = ws + lane;
-            const uint32_t word = f < nw ? wq[f] : 0u;
+            const uint32_t word = nextWord;
+            // the next window's word is in flight while this one is written
+            nextWord = f + 32 < nw ? __ldg(wq + f + 32) : 0u;
             const uint32_t cnt = __popc(word);
             const uint32_t incl = warp_incl_scan(cnt, lane);
             const uint32_t T = __shfl_sync(FULL, incl, 31);
@@ -123,15 +134,28 @@ __device__ __forceinline__ void emit_rows(const sj_join_args &a, const UnitTask 
             __syncwarp();   // the previous window's copy-out is done with ent / base
             // a query's first word: base = its chunk start slot minus its flat prefix
             if (f < nw && f == q * cb) w.base[q] = w.start[q] - (carry + ex);
-            decode_bits(word, lane << 5, w.ent, ex);
+            decode_bits(word, (q << 16) | ((f - q * cb) << 5), w.ent, ex);
             __syncwarp();
-            for (uint32_t e = lane; e < T; e += 32) {
-                const uint32_t ent = w.ent[e];
-                const uint32_t fe = ws + (ent >> 5);
-                const uint32_t qe = (uint32_t)(((uint64_t)fe * magic) >> 32);
-                const uint32_t pos = (c0 + (fe - qe * cb)) * 32 + (ent & 31u);
-                if (qe < nq && pos < u.L) put(a, w.base[qe] + carry + e, w.key[qe], (int32_t)cid[pos]);
-                else atomicMax(&a.stat[6], 1ULL);
+            // copy-out, CO entries per lane at a time: their candidate-id loads
+            // are all issued before any store
+            for (uint32_t e0 = 0; e0 < T; e0 += 32 * CO) {
+                uint32_t slot[CO], pos[CO], val[CO];
+#pragma unroll
+                for (int i = 0; i < CO; i++) {
+                    const uint32_t e = e0 + 32 * i + lane;
+                    const uint32_t ent = w.ent[e < T ? e : 0];
+                    const uint32_t qe = ent >> 16;
+                    pos[i] = c0 * 32 + (ent & 0xffffu);
+                    const bool ok = e < T && qe < nq && pos[i] < u.L;
+                    if (e < T && !ok) atomicMax(&a.stat[6], 1ULL);
+                    slot[i] = ok ? w.base[qe] + carry + e : NO_SLOT;
+                    if (!ok) pos[i] = 0;
+                }
+#pragma unroll
+                for (int i = 0; i < CO; i++) val[i] = __ldg(cid + pos[i]);
+#pragma unroll
+                for (int i = 0; i < CO; i++)
+                    if (slot[i] != NO_SLOT) put(a, slot[i], (int32_t)val[i]);
             }
             carry += T;
         }
@@ -142,8 +166,8 @@ __device__ __forceinline__ void emit_rows(const sj_join_args &a, const UnitTask 
     }
 }
 
-// Column unit: stream positions 32b .. 32b+31 of symmetric task u.t, key =
-// candidate, value = query.
+// Column unit: stream positions 32b .. 32b+31 of symmetric task u.t (key =
+// candidate, value = query).
 __device__ __forceinline__ void emit_cols(const sj_join_args &a, const UnitTask &u, uint32_t b, WarpSmem &w,
                                           uint32_t lane)
 {
@@ -156,14 +180,12 @@ __device__ __forceinline__ void emit_cols(const sj_join_args &a, const UnitTask 
     uint32_t slot = 0;
     __syncwarp();        // the previous unit is done with the warp's shared memory
     if (s < u.L) {
-        const uint32_t key = a.candId[rec + s];
-        w.key[lane] = (int32_t)key;
-        slot = a.keyStart[key] + a.candRel[rec + s];
+        slot = a.keyStart[a.candId[rec + s]] + a.candRel[rec + s];
     }
-    uint32_t word = cw[0];
+    uint32_t word = __ldg(cw);
     for (uint32_t g = 0; g < nG; g++) {
         const uint32_t cur = word;
-        if (g + 1 < nG) word = cw[(g + 1) * 32];
+        if (g + 1 < nG) word = __ldg(cw + (g + 1) * 32);
         const uint32_t cnt = __popc(cur);
         const uint32_t incl = warp_incl_scan(cnt, lane);
         const uint32_t T = __shfl_sync(FULL, incl, 31);
@@ -173,18 +195,30 @@ __device__ __forceinline__ void emit_cols(const sj_join_args &a, const UnitTask 
         w.base[lane] = slot - ex;   // lane L's entries [ex_L, ex_L + cnt_L) go to slot_L onwards
         decode_bits(cur, lane << 5, w.ent, ex);
         __syncwarp();
-        for (uint32_t e = lane; e < T; e += 32) {
-            const uint32_t ent = w.ent[e];
-            const uint32_t owner = ent >> 5;
-            const uint32_t qi = g * 32 + (ent & 31u);
-            if (b * 32 + owner < u.L && qi < u.qc) put(a, w.base[owner] + e, w.key[owner], (int32_t)qids[qi]);
-            else atomicMax(&a.stat[6], 1ULL);
+        for (uint32_t e0 = 0; e0 < T; e0 += 32 * CO) {
+            uint32_t slot[CO], qi[CO], val[CO];
+#pragma unroll
+            for (int i = 0; i < CO; i++) {
+                const uint32_t e = e0 + 32 * i + lane;
+                const uint32_t ent = w.ent[e < T ? e : 0];
+                const uint32_t owner = ent >> 5;
+                qi[i] = g * 32 + (ent & 31u);
+                const bool ok = e < T && b * 32 + owner < u.L && qi[i] < u.qc;
+                if (e < T && !ok) atomicMax(&a.stat[6], 1ULL);
+                slot[i] = ok ? w.base[owner] + e : NO_SLOT;
+                if (!ok) qi[i] = 0;
+            }
+#pragma unroll
+            for (int i = 0; i < CO; i++) val[i] = __ldg(qids + qi[i]);
+#pragma unroll
+            for (int i = 0; i < CO; i++)
+                if (slot[i] != NO_SLOT) put(a, slot[i], (int32_t)val[i]);
         }
         slot += cnt;
     }
 }
 
-__global__ void __launch_bounds__(EW, 4) k_emit(sj_join_args a)
+__global__ void __launch_bounds__(EW, 5) k_emit(sj_join_args a)
 {
     __shared__ WarpSmem smem[ENW];
     const uint32_t lane = threadIdx.x & 31u;

@@ -76,7 +76,7 @@ struct sj_join_args {
     uint32_t *queueHead;        // persistent-queue cursor (work-queue modes)
     uint32_t *keyCount;         // count pass: per point-id pair counts
     const uint32_t *keyStart;   // emission: first slot of each point id's key run (exclusive scan)
-    int32_t *outKey, *outVal;   // batch output, written by the emission
+    int32_t *outKey, *outVal;   // batch output: keys by sj_expand_keys, values by the emission
     uint64_t capacity;          // pairs the output buffers hold
     unsigned long long *stat;   // [2] pairs (count pass), [3] run past capacity, [4] set hash,
                                 // [5] batches skipped for overflow, [6] emission record out of range
@@ -140,6 +140,11 @@ cudaError_t sj_hash_pairs(const int32_t *key, const int32_t *val, uint64_t m,
 cudaError_t sj_hash_pairs_dev(const int32_t *key, const int32_t *val, const unsigned long long *count, uint64_t cap,
                               uint64_t gridHint, unsigned long long *hashOut, cudaStream_t s);
 
+// keys of a batch from its row structure: key k owns [excl[k], excl[k+1])
+// (excl[n] = *total); skipped when the batch's count exceeds cap
+cudaError_t sj_expand_keys(const uint32_t *excl, const uint32_t *total, uint64_t n, int32_t *outKey,
+                           const unsigned long long *batchPairs, uint64_t cap, cudaStream_t s);
+
 // index build (sj_index.cu)
 cudaError_t sj_launch_minmax(const double *pts, uint64_t n, int D, double *minmax_dev, cudaStream_t s);
 cudaError_t sj_launch_cell_keys(const double *pts, uint64_t n, sj_grid_dev g, uint64_t *keys, uint32_t *vals,
@@ -161,8 +166,8 @@ cudaError_t sj_launch_neighbours(const uint64_t *cellLid, const uint32_t *cellCo
 // join (sj_join.cu): the count pass (per-key pair counts, hit masks)
 cudaError_t sj_launch_join(const sj_join_args &a, const sj_grid_dev &g, int fp32, int queue, int numSM,
                            cudaStream_t s);
-// emission (sj_emit.cu): (key, value) pairs from the recorded hit masks into
-// their key runs; a.queueHead must be zero at launch
+// emission (sj_emit.cu): the values of the pairs from the recorded hit masks
+// into their key runs; a.queueHead must be zero at launch
 cudaError_t sj_launch_emit(const sj_join_args &a, int numSM, cudaStream_t s);
 
 // emission units of a task: one per group of 32 queries, plus one per block of

@@ -88,6 +88,44 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan_tile(const uint32_t *in, 
     if (!blockOffsets && total_dev && threadIdx.x == 0) *total_dev = tot;
 }
 
+// Second pass of the two-launch scan: each block finds its offset by summing
+// the tile sums of all blocks before it (read from L2; used while the tile
+// count is small), then scans its tile; the last block writes the total.
+constexpr uint64_t SCAN_LOOKUP_MAX_TILES = 4096;
+
+__global__ void __launch_bounds__(SCAN_THREADS) k_scan_tile_lookup(const uint32_t *in, uint32_t *out, uint64_t n,
+                                                                   const uint32_t *__restrict__ sums,
+                                                                   uint32_t *total_dev, uint32_t *zeroIn)
+{
+    uint32_t part = 0;
+    for (uint32_t b = threadIdx.x; b < blockIdx.x; b += SCAN_THREADS) part += sums[b];
+    uint32_t blockOff;   // sum of all earlier tiles (the block total of the parts)
+    block_exclusive_scan(part, &blockOff);
+    const uint64_t base = (uint64_t)blockIdx.x * SCAN_TILE + (uint64_t)threadIdx.x * SCAN_ITEMS;
+    uint32_t v[SCAN_ITEMS];
+    uint32_t sum = 0;
+#pragma unroll
+    for (int i = 0; i < SCAN_ITEMS; i++) {
+        const uint64_t idx = base + i;
+        v[i] = (idx < n) ? in[idx] : 0u;
+        sum += v[i];
+    }
+    if (zeroIn) {
+#pragma unroll
+        for (int i = 0; i < SCAN_ITEMS; i++)
+            if (base + i < n) zeroIn[base + i] = 0u;
+    }
+    uint32_t tot;
+    uint32_t off = blockOff + block_exclusive_scan(sum, &tot);
+#pragma unroll
+    for (int i = 0; i < SCAN_ITEMS; i++) {
+        const uint64_t idx = base + i;
+        if (idx < n) out[idx] = off;
+        off += v[i];
+    }
+    if (total_dev && blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) *total_dev = blockOff + tot;
+}
+
 __global__ void k_scan_total(const uint32_t *scannedSums, const uint32_t *sums, uint64_t nb, uint32_t *total_dev)
 {
     if (threadIdx.x == 0 && blockIdx.x == 0 && total_dev) *total_dev = scannedSums[nb - 1] + sums[nb - 1];
@@ -120,6 +158,11 @@ cudaError_t scan_rec(const uint32_t *in, uint32_t *out, uint64_t n, uint32_t *te
     uint64_t nb = ceil_div(n, SCAN_TILE);
     uint32_t *sums = temp, *scanned = temp + nb;
     k_scan_reduce<<<(unsigned)nb, SCAN_THREADS, 0, s>>>(in, n, sums); sj_note_launch();
+    if (nb <= SCAN_LOOKUP_MAX_TILES) {
+        k_scan_tile_lookup<<<(unsigned)nb, SCAN_THREADS, 0, s>>>(in, out, n, sums, total_dev, zeroIn);
+        sj_note_launch();
+        return cudaGetLastError();
+    }
     cudaError_t e = scan_rec(sums, scanned, nb, temp + 2 * nb, nullptr, s);
     if (e != cudaSuccess) return e;
     if (total_dev) {
@@ -287,6 +330,39 @@ __global__ void __launch_bounds__(256) k_hash_pairs_dev(const int32_t *__restric
     }
 }
 
+// Keys of a batch: key k owns slots [excl[k], excl[k+1]) (excl[n] = *total).
+// A warp takes 32 consecutive keys and writes each key's run with all lanes,
+// 128 contiguous bytes per store.
+__global__ void __launch_bounds__(256) k_expand_keys(const uint32_t *__restrict__ excl,
+                                                     const uint32_t *__restrict__ total, uint64_t n,
+                                                     int32_t *__restrict__ outKey,
+                                                     const unsigned long long *__restrict__ batchPairs, uint64_t cap)
+{
+    if (*batchPairs > cap) return;
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint64_t k0 = ((uint64_t)blockIdx.x * 256 + (threadIdx.x & ~31u));
+    if (k0 >= n) return;
+    const uint64_t k = k0 + lane;
+    const uint32_t tot = *total;
+    const uint32_t st = k < n ? excl[k] : tot;
+    const uint32_t en = k + 1 < n ? excl[k + 1] : tot;
+    uint32_t live = __ballot_sync(0xffffffffu, en > st);
+    while (live) {
+        const int i = __ffs(live) - 1;
+        live &= live - 1;
+        const uint32_t s0 = __shfl_sync(0xffffffffu, st, i);
+        const uint32_t e0 = __shfl_sync(0xffffffffu, en, i);
+        const int32_t key = (int32_t)(k0 + i);
+        // up to 3 single slots to a 16-byte boundary, 16-byte stores, the rest
+        const uint32_t a = min((s0 + 3u) & ~3u, e0);
+        const uint32_t b = a + ((e0 - a) & ~3u);
+        if (lane < a - s0) outKey[s0 + lane] = key;
+        const int4 kv = make_int4(key, key, key, key);
+        for (uint32_t pos = a + 4 * lane; pos < b; pos += 128) *reinterpret_cast<int4 *>(outKey + pos) = kv;
+        if (lane < e0 - b) outKey[b + lane] = key;
+    }
+}
+
 }  // namespace
 
 cudaError_t sj_hash_pairs_dev(const int32_t *key, const int32_t *val, const unsigned long long *count, uint64_t cap,
@@ -296,6 +372,15 @@ cudaError_t sj_hash_pairs_dev(const int32_t *key, const int32_t *val, const unsi
     if (blocks > 148 * 8) blocks = 148 * 8;
     if (blocks == 0) blocks = 1;
     k_hash_pairs_dev<<<(unsigned)blocks, 256, 0, s>>>(key, val, count, cap, hashOut);
+    sj_note_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t sj_expand_keys(const uint32_t *excl, const uint32_t *total, uint64_t n, int32_t *outKey,
+                           const unsigned long long *batchPairs, uint64_t cap, cudaStream_t s)
+{
+    if (n == 0) return cudaSuccess;
+    k_expand_keys<<<(unsigned)ceil_div(n, 256), 256, 0, s>>>(excl, total, n, outKey, batchPairs, cap);
     sj_note_launch();
     return cudaGetLastError();
 }
