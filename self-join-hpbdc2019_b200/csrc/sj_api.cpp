@@ -201,6 +201,8 @@ struct Ctx {
     std::vector<uint64_t> hMaskOff, hColOff, hRowOff, hCandOff, hUnitOff;
     DevBuf<uint64_t> dMaskOff, dColOff, dRowOff, dCandOff, dUnitOff;
     DevBuf<uint32_t> masks, colMasks, rowRel, candId, candRel;
+    DevBuf<uint4> longRuns;            // key expansion: runs too long for one warp
+    DevBuf<uint32_t> longCount;
     DevBuf<unsigned long long> batchTot;
     std::vector<cudaEvent_t> events;   // per-batch stage boundaries of the asynchronous phase
     PinBuf pinTotal, pinKey[2], pinVal[2], pinStart[2];
@@ -771,6 +773,45 @@ void expand_keys_host(const uint32_t *start, uint64_t n, uint64_t cnt, int32_t *
     }
 }
 
+// Splits batch br into consecutive task ranges whose measured pair counts
+// (taskHits, exact after a count pass over br) fit cap; appends them to `out`
+// in ascending task order.
+sj_status replan_exact(const BatchRange &br, const std::vector<uint32_t> &taskHits, uint64_t cap,
+                       std::vector<BatchRange> &out)
+{
+    std::vector<BatchRange> parts;
+    uint32_t t0 = br.t0;
+    uint64_t acc = 0;
+    for (uint32_t t = br.t0; t < br.t1; t++) {
+        const uint64_t h = taskHits[t];
+        if (h > cap) {
+            set_error("a single task produces %llu pairs, more than the batch capacity %llu",
+                      (unsigned long long)h, (unsigned long long)cap);
+            return SJ_ERR_INTERNAL;
+        }
+        if (t > t0 && acc + h > cap) {
+            parts.push_back({t0, t});
+            t0 = t;
+            acc = 0;
+        }
+        acc += h;
+    }
+    parts.push_back({t0, br.t1});
+    out.insert(out.end(), parts.begin(), parts.end());
+    return SJ_OK;
+}
+
+// Key array of the current batch (a.outKey, a.capacity) from keyStart.
+sj_status expand_keys(Ctx &c, const sj_join_args &a)
+{
+    const size_t slots = sj_expand_long_slots(a.capacity);
+    CK(c.longRuns.ensure(slots));
+    CK(c.longCount.ensure(1));
+    CK(sj_expand_keys(c.keyStart.p, c.total.p, c.n, a.outKey, a.batchPairs, a.capacity, c.longRuns.p,
+                      (uint32_t)std::min<size_t>(c.longRuns.n, 0xffffffffu), c.longCount.p, c.numSM, c.s));
+    return SJ_OK;
+}
+
 sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
 {
     const unsigned long long launches0 = sj_launch_total();
@@ -927,7 +968,7 @@ sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
             CK(cudaEventRecord(ev[6 * i + 1], c.s));
             CK(sj_exclusive_scan_u32_clear(c.keyCount.p, c.keyStart.p, n, c.scanTemp.p, c.total.p, c.s));
             CK(cudaEventRecord(ev[6 * i + 2], c.s));
-            CK(sj_expand_keys(c.keyStart.p, c.total.p, n, a.outKey, a.batchPairs, a.capacity, c.s));
+            CKS(expand_keys(c, a));
             CK(cudaEventRecord(ev[6 * i + 3], c.s));
             CK(cudaMemsetAsync(c.queueHead.p, 0, sizeof(uint32_t), c.s));
             CK(sj_launch_emit(a, c.numSM, c.s));
@@ -953,10 +994,13 @@ sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
             msFill += t34;
             msDeliver += t45;
         }
+        std::vector<BatchRange> redo;
         for (size_t i = 0; i < nplan; i++) {
             const BatchRange &br = plan[nplan - 1 - i];
             if (tot[i] > bufCap) {
-                stack.push_back(br);
+                // the count pass measured every task's pairs: re-plan this
+                // batch's tasks exactly, so the re-runs cannot overflow again
+                CKS(replan_exact(br, hTaskHits, bufCap, redo));
                 retries++;
                 continue;
             }
@@ -964,7 +1008,7 @@ sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
             pairsTotal += tot[i];
             batches++;
         }
-        std::reverse(stack.begin(), stack.end());
+        stack.assign(redo.rbegin(), redo.rend());   // popped in ascending task order
     } else {
         stack = plan;
     }
@@ -1017,15 +1061,11 @@ sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
         msScan += tb.stop(c.s);
         memcpy(&cnt, c.pinTotal.p, sizeof(cnt));
         if (cnt > cap) {
-            // estimate too low: split the batch (the scan already cleared the counts)
-            if (br.t1 - br.t0 <= 1) {
-                set_error("a single task produces %llu pairs, more than the batch capacity %llu",
-                          (unsigned long long)cnt, (unsigned long long)cap);
-                return SJ_ERR_INTERNAL;
-            }
-            uint32_t mid = br.t0 + (br.t1 - br.t0) / 2;
-            stack.push_back({mid, br.t1});
-            stack.push_back({br.t0, mid});
+            // estimate too low: re-plan the batch from the measured per-task
+            // pairs (the scan already cleared the counts)
+            std::vector<BatchRange> parts;
+            CKS(replan_exact(br, hTaskHits, cap, parts));
+            for (size_t i = parts.size(); i-- > 0;) stack.push_back(parts[i]);
             retries++;
             continue;
         }
@@ -1043,7 +1083,7 @@ sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
         tb.start(c.s);
         // the previous batch's values must be copied before the emission rewrites them
         if (pend.live) CK(cudaStreamWaitEvent(c.s, c.evVals[pend.sel], 0));
-        CK(sj_expand_keys(c.keyStart.p, c.total.p, n, a.outKey, a.batchPairs, a.capacity, c.s));
+        CKS(expand_keys(c, a));
         msExpand += tb.stop(c.s);
         tb.start(c.s);
         CK(cudaMemsetAsync(c.queueHead.p, 0, sizeof(uint32_t), c.s));

@@ -141,9 +141,13 @@ cudaError_t sj_hash_pairs_dev(const int32_t *key, const int32_t *val, const unsi
                               uint64_t gridHint, unsigned long long *hashOut, cudaStream_t s);
 
 // keys of a batch from its row structure: key k owns [excl[k], excl[k+1])
-// (excl[n] = *total); skipped when the batch's count exceeds cap
+// (excl[n] = *total); skipped when the batch's count exceeds cap.  longRuns
+// (16-byte records, sj_expand_long_slots(cap) of them) and longCount are
+// scratch for the runs too long for one warp.
 cudaError_t sj_expand_keys(const uint32_t *excl, const uint32_t *total, uint64_t n, int32_t *outKey,
-                           const unsigned long long *batchPairs, uint64_t cap, cudaStream_t s);
+                           const unsigned long long *batchPairs, uint64_t cap, void *longRuns, uint32_t longCap,
+                           uint32_t *longCount, int numSM, cudaStream_t s);
+size_t sj_expand_long_slots(uint64_t cap);
 
 // index build (sj_index.cu)
 cudaError_t sj_launch_minmax(const double *pts, uint64_t n, int D, double *minmax_dev, cudaStream_t s);

@@ -332,11 +332,29 @@ __global__ void __launch_bounds__(256) k_hash_pairs_dev(const int32_t *__restric
 
 // Keys of a batch: key k owns slots [excl[k], excl[k+1]) (excl[n] = *total).
 // A warp takes 32 consecutive keys and writes each key's run with all lanes,
-// 128 contiguous bytes per store.
+// 128 contiguous bytes per store.  Runs longer than EXP_LONG slots (a dense
+// key can own a million slots of one batch) are queued instead and written by
+// whole CTAs in k_expand_long, so one warp never holds up the launch.
+constexpr uint32_t EXP_LONG = 16384;
+
+__device__ __forceinline__ void write_run(int32_t *__restrict__ outKey, uint32_t s0, uint32_t e0, int32_t key,
+                                          uint32_t t, uint32_t nt)
+{
+    // up to 3 single slots to a 16-byte boundary, 16-byte stores, the rest
+    const uint32_t a = min((s0 + 3u) & ~3u, e0);
+    const uint32_t b = a + ((e0 - a) & ~3u);
+    if (t < a - s0) outKey[s0 + t] = key;
+    const int4 kv = make_int4(key, key, key, key);
+    for (uint32_t pos = a + 4 * t; pos < b; pos += 4 * nt) *reinterpret_cast<int4 *>(outKey + pos) = kv;
+    if (t < e0 - b) outKey[b + t] = key;
+}
+
 __global__ void __launch_bounds__(256) k_expand_keys(const uint32_t *__restrict__ excl,
                                                      const uint32_t *__restrict__ total, uint64_t n,
                                                      int32_t *__restrict__ outKey,
-                                                     const unsigned long long *__restrict__ batchPairs, uint64_t cap)
+                                                     const unsigned long long *__restrict__ batchPairs, uint64_t cap,
+                                                     uint4 *__restrict__ longRuns, uint32_t longCap,
+                                                     uint32_t *__restrict__ longCount)
 {
     if (*batchPairs > cap) return;
     const uint32_t lane = threadIdx.x & 31u;
@@ -353,13 +371,30 @@ __global__ void __launch_bounds__(256) k_expand_keys(const uint32_t *__restrict_
         const uint32_t s0 = __shfl_sync(0xffffffffu, st, i);
         const uint32_t e0 = __shfl_sync(0xffffffffu, en, i);
         const int32_t key = (int32_t)(k0 + i);
-        // up to 3 single slots to a 16-byte boundary, 16-byte stores, the rest
-        const uint32_t a = min((s0 + 3u) & ~3u, e0);
-        const uint32_t b = a + ((e0 - a) & ~3u);
-        if (lane < a - s0) outKey[s0 + lane] = key;
-        const int4 kv = make_int4(key, key, key, key);
-        for (uint32_t pos = a + 4 * lane; pos < b; pos += 128) *reinterpret_cast<int4 *>(outKey + pos) = kv;
-        if (lane < e0 - b) outKey[b + lane] = key;
+        if (e0 - s0 > EXP_LONG) {
+            uint32_t j = 0;
+            if (lane == 0) j = atomicAdd(longCount, 1u);
+            j = __shfl_sync(0xffffffffu, j, 0);
+            if (j < longCap) {
+                if (lane == 0) longRuns[j] = make_uint4((uint32_t)key, s0, e0, 0u);
+                continue;
+            }
+        }
+        write_run(outKey, s0, e0, key, lane, 32);
+    }
+}
+
+// The queued long runs, one CTA per run at a time.
+__global__ void __launch_bounds__(256) k_expand_long(int32_t *__restrict__ outKey,
+                                                     const unsigned long long *__restrict__ batchPairs, uint64_t cap,
+                                                     const uint4 *__restrict__ longRuns, uint32_t longCap,
+                                                     const uint32_t *__restrict__ longCount)
+{
+    if (*batchPairs > cap) return;
+    const uint32_t cnt = min(*longCount, longCap);
+    for (uint32_t j = blockIdx.x; j < cnt; j += gridDim.x) {
+        const uint4 r = longRuns[j];
+        write_run(outKey, r.y, r.z, (int32_t)r.x, threadIdx.x, blockDim.x);
     }
 }
 
@@ -377,13 +412,22 @@ cudaError_t sj_hash_pairs_dev(const int32_t *key, const int32_t *val, const unsi
 }
 
 cudaError_t sj_expand_keys(const uint32_t *excl, const uint32_t *total, uint64_t n, int32_t *outKey,
-                           const unsigned long long *batchPairs, uint64_t cap, cudaStream_t s)
+                           const unsigned long long *batchPairs, uint64_t cap, void *longRuns, uint32_t longCap,
+                           uint32_t *longCount, int numSM, cudaStream_t s)
 {
     if (n == 0) return cudaSuccess;
-    k_expand_keys<<<(unsigned)ceil_div(n, 256), 256, 0, s>>>(excl, total, n, outKey, batchPairs, cap);
+    cudaError_t e = cudaMemsetAsync(longCount, 0, sizeof(uint32_t), s);
+    if (e != cudaSuccess) return e;
+    k_expand_keys<<<(unsigned)ceil_div(n, 256), 256, 0, s>>>(excl, total, n, outKey, batchPairs, cap,
+                                                            (uint4 *)longRuns, longCap, longCount);
+    sj_note_launch();
+    k_expand_long<<<(unsigned)(numSM * 8), 256, 0, s>>>(outKey, batchPairs, cap, (const uint4 *)longRuns, longCap,
+                                                       longCount);
     sj_note_launch();
     return cudaGetLastError();
 }
+
+size_t sj_expand_long_slots(uint64_t cap) { return (size_t)(cap / EXP_LONG) + 1; }
 
 static std::atomic<unsigned long long> g_launches{0};
 void sj_note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
