@@ -181,6 +181,8 @@ def run_ours(args):
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     pts, eps, k, spec = sjoin.datasets.make(args.workload, n=args.n,
                                             seed=sjoin.datasets.SEEDS[args.workload] + 1000 * rank)
+    if args.capacity is not None:
+        spec["capacity"] = args.capacity
     prec = spec["precision"] if args.precision is None else args.precision
     flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device="cuda")
     sj = sjoin.SelfJoin(spec["D"], eps, indexed_dims=k, mode=spec["mode"], precision=prec,
@@ -326,6 +328,7 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", default="c2")
     ap.add_argument("--n", type=int, default=None)
+    ap.add_argument("--capacity", type=int, default=None, help="batch capacity in pairs (default: the workload's)")
     ap.add_argument("--precision", type=int, default=None)
     ap.add_argument("--learned", default=None,
                     help="estimator weights file: learned scheduler instead of the sampling estimate")
