@@ -163,6 +163,17 @@ sj_status sj_degrees(void *ctx, uint32_t *deg);
 sj_status sj_neighbor_table(void *ctx, sj_neighbor_table_lookup *table, int **values, uint64_t *total);
 void sj_free(void *p);
 
+/* On-device CSR neighbour table (replaces the host table of
+ * constructNeighborTableKeyValueWithPtrs, GPU.cu:2595-2637, without leaving
+ * the GPU): rowPtr (n+1 uint64, DEVICE memory, required) receives the row
+ * offsets, cols (DEVICE memory, cols_capacity int32) point i's neighbour ids in
+ * cols[rowPtr[i] .. rowPtr[i+1]), complete across batches.  With cols = NULL
+ * only the degrees run: rowPtr and *total are filled so the caller can size
+ * cols.  Fails with SJ_ERR_BAD_INPUT when cols_capacity < total.  Values inside
+ * a row are in no particular order (the reference's rows are not sorted
+ * either). */
+sj_status sj_neighbor_csr(void *ctx, uint64_t *rowPtr, int32_t *cols, uint64_t cols_capacity, uint64_t *total);
+
 sj_status sj_get_stats(void *ctx, sj_stats *st);
 
 /* The CUDA stream (cudaStream_t) all of this context's work is ordered on, so

@@ -201,6 +201,12 @@ struct Ctx {
     std::vector<uint64_t> hMaskOff, hColOff, hRowOff, hCandOff, hUnitOff;
     DevBuf<uint64_t> dMaskOff, dColOff, dRowOff, dCandOff, dUnitOff;
     DevBuf<uint32_t> masks, colMasks, rowRel, candId, candRel;
+    // device CSR neighbour table under construction (sj_neighbor_csr): the
+    // caller's arrays and the rows' fill cursors
+    uint64_t *csrRowPtr = nullptr;
+    int32_t *csrCols = nullptr;
+    uint64_t csrCap = 0;
+    DevBuf<uint32_t> csrFill;
     DevBuf<uint4> longRuns;            // key expansion: runs too long for one warp
     DevBuf<uint32_t> longCount;
     DevBuf<unsigned long long> batchTot;
@@ -812,6 +818,10 @@ sj_status expand_keys(Ctx &c, const sj_join_args &a)
     return SJ_OK;
 }
 
+// Internal delivery mode of run_join: every batch is appended to the device
+// CSR table set up by sj_neighbor_csr.
+constexpr int SJ_DELIVER_CSR = 100;
+
 sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
 {
     const unsigned long long launches0 = sj_launch_total();
@@ -1091,7 +1101,10 @@ sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
         msFill += tb.stop(c.s);
         tb.start(c.s);
         CK(sj_hash_pairs(c.outKey.p, c.outVal.p, cnt, c.stat.p + 4, c.s));
-        if (delivery == SJ_DELIVER_DEVICE && cb) {
+        if (delivery == SJ_DELIVER_CSR) {
+            CK(sj_csr_append(c.keyStart.p, c.total.p, n, c.outVal.p, c.csrRowPtr, c.csrFill.p, c.csrCols, c.csrCap,
+                             c.stat.p + 7, c.s));
+        } else if (delivery == SJ_DELIVER_DEVICE && cb) {
             CK(cudaStreamSynchronize(c.s));
             sj_batch b{batches, cnt, c.outKey.p, c.outVal.p, 1};
             if (cb(&b, user)) result = SJ_ERR_ABORTED;
@@ -1139,9 +1152,10 @@ sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
     unsigned long long hs[8];
     CK(cudaMemcpyAsync(hs, c.stat.p, sizeof(hs), cudaMemcpyDeviceToHost, c.s));
     CK(cudaStreamSynchronize(c.s));
-    if (hs[3] || hs[6]) {
-        set_error(hs[3] ? "internal: the emission exceeded the counted capacity"
-                        : "internal: the emission met a count-pass record out of range");
+    if (hs[3] || hs[6] || hs[7]) {
+        set_error(hs[3]   ? "internal: the emission exceeded the counted capacity"
+                  : hs[6] ? "internal: the emission met a count-pass record out of range"
+                          : "internal: a neighbour-table row received more values than its degree");
         return SJ_ERR_INTERNAL;
     }
     {
@@ -1578,6 +1592,52 @@ sj_status sj_neighbor_table(void *ctx, sj_neighbor_table_lookup *table, int **va
     }
     *values = vals;
     if (total) *total = tot;
+    return SJ_OK;
+}
+
+sj_status sj_neighbor_csr(void *ctx, uint64_t *rowPtr, int32_t *cols, uint64_t cols_capacity, uint64_t *total)
+{
+    if (!ctx || !rowPtr) {
+        set_error("null argument");
+        return SJ_ERR_BAD_INPUT;
+    }
+    Ctx &c = *as_ctx(ctx);
+    CKS(bind(c));
+    const uint64_t n = c.n;
+    std::vector<uint32_t> deg(n);
+    CKS(run_degrees(c, deg.data()));
+    std::vector<uint64_t> hp(n + 1);
+    hp[0] = 0;
+    for (uint64_t i = 0; i < n; i++) hp[i + 1] = hp[i] + deg[i];
+    if (total) *total = hp[n];
+    CK(cudaMemcpyAsync(rowPtr, hp.data(), sizeof(uint64_t) * (n + 1), cudaMemcpyHostToDevice, c.s));
+    CK(cudaStreamSynchronize(c.s));
+    if (!cols) return SJ_OK;
+    if (cols_capacity < hp[n]) {
+        set_error("cols holds %llu values, the table needs %llu", (unsigned long long)cols_capacity,
+                  (unsigned long long)hp[n]);
+        return SJ_ERR_BAD_INPUT;
+    }
+    CK(c.csrFill.ensure(n ? n : 1));
+    CK(cudaMemsetAsync(c.csrFill.p, 0, sizeof(uint32_t) * (n ? n : 1), c.s));
+    c.csrRowPtr = rowPtr;
+    c.csrCols = cols;
+    c.csrCap = cols_capacity;
+    const sj_status s = run_join(c, SJ_DELIVER_CSR, nullptr, nullptr);
+    c.csrRowPtr = nullptr;
+    c.csrCols = nullptr;
+    c.csrCap = 0;
+    if (s != SJ_OK) return s;
+    // every row must be exactly full
+    std::vector<uint32_t> fill(n);
+    if (n) CK(cudaMemcpyAsync(fill.data(), c.csrFill.p, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost, c.s));
+    CK(cudaStreamSynchronize(c.s));
+    for (uint64_t i = 0; i < n; i++)
+        if (fill[i] != deg[i]) {
+            set_error("internal: neighbour-table row %llu holds %u of %u values", (unsigned long long)i, fill[i],
+                      deg[i]);
+            return SJ_ERR_INTERNAL;
+        }
     return SJ_OK;
 }
 

@@ -79,7 +79,8 @@ struct sj_join_args {
     int32_t *outKey, *outVal;   // batch output: keys by sj_expand_keys, values by the emission
     uint64_t capacity;          // pairs the output buffers hold
     unsigned long long *stat;   // [2] pairs (count pass), [3] run past capacity, [4] set hash,
-                                // [5] batches skipped for overflow, [6] emission record out of range
+                                // [5] batches skipped for overflow, [6] emission record out of range,
+                                // [7] CSR table row overflow
     unsigned long long *batchPairs;  // this batch's pair total (count pass adds, later passes read)
     uint32_t *taskHits;         // optional per-task measured pairs (count pass)
     // count-pass records consumed by the emission pass (null: not recorded).
@@ -148,6 +149,11 @@ cudaError_t sj_expand_keys(const uint32_t *excl, const uint32_t *total, uint64_t
                            const unsigned long long *batchPairs, uint64_t cap, void *longRuns, uint32_t longCap,
                            uint32_t *longCount, int numSM, cudaStream_t s);
 size_t sj_expand_long_slots(uint64_t cap);
+// appends a batch (values vals, key runs start[0..n], start[n] = *total) to a
+// device CSR table rowPtr[n+1] / cols[colsCap]; fill[n] are the rows' cursors
+cudaError_t sj_csr_append(const uint32_t *start, const uint32_t *total, uint64_t n, const int32_t *vals,
+                          const uint64_t *rowPtr, uint32_t *fill, int32_t *cols, uint64_t colsCap,
+                          unsigned long long *err, cudaStream_t s);
 
 // index build (sj_index.cu)
 cudaError_t sj_launch_minmax(const double *pts, uint64_t n, int D, double *minmax_dev, cudaStream_t s);

@@ -398,6 +398,45 @@ __global__ void __launch_bounds__(256) k_expand_long(int32_t *__restrict__ outKe
     }
 }
 
+// Appends a batch to a device CSR neighbour table: key k's run
+// [start[k], start[k+1]) of vals (start[n] = *total) goes to
+// cols[rowPtr[k] + fill[k] ...] and fill[k] grows by its length.  A warp takes
+// 32 consecutive keys and copies each run with all lanes.  A run that would
+// pass its row's end or the caller's capacity is not written and sets *err.
+__global__ void __launch_bounds__(256) k_csr_append(const uint32_t *__restrict__ start,
+                                                    const uint32_t *__restrict__ total, uint64_t n,
+                                                    const int32_t *__restrict__ vals,
+                                                    const uint64_t *__restrict__ rowPtr, uint32_t *__restrict__ fill,
+                                                    int32_t *__restrict__ cols, uint64_t colsCap,
+                                                    unsigned long long *__restrict__ err)
+{
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint64_t k0 = ((uint64_t)blockIdx.x * 256 + (threadIdx.x & ~31u));
+    if (k0 >= n) return;
+    const uint64_t k = k0 + lane;
+    const uint32_t tot = *total;
+    const uint32_t st = k < n ? start[k] : tot;
+    const uint32_t en = k + 1 < n ? start[k + 1] : tot;
+    unsigned long long dst = 0;
+    bool ok = true;
+    if (en > st) {
+        const uint64_t rowEnd = rowPtr[k + 1];
+        dst = rowPtr[k] + fill[k];
+        ok = dst + (en - st) <= rowEnd && rowEnd <= colsCap;
+        if (ok) fill[k] += en - st;
+        else atomicMax(err, 1ULL);
+    }
+    uint32_t live = __ballot_sync(0xffffffffu, en > st && ok);
+    while (live) {
+        const int i = __ffs(live) - 1;
+        live &= live - 1;
+        const uint32_t s0 = __shfl_sync(0xffffffffu, st, i);
+        const uint32_t e0 = __shfl_sync(0xffffffffu, en, i);
+        const unsigned long long d0 = __shfl_sync(0xffffffffu, dst, i);
+        for (uint32_t p = lane; p < e0 - s0; p += 32) cols[d0 + p] = vals[s0 + p];
+    }
+}
+
 }  // namespace
 
 cudaError_t sj_hash_pairs_dev(const int32_t *key, const int32_t *val, const unsigned long long *count, uint64_t cap,
@@ -423,6 +462,16 @@ cudaError_t sj_expand_keys(const uint32_t *excl, const uint32_t *total, uint64_t
     sj_note_launch();
     k_expand_long<<<(unsigned)(numSM * 8), 256, 0, s>>>(outKey, batchPairs, cap, (const uint4 *)longRuns, longCap,
                                                        longCount);
+    sj_note_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t sj_csr_append(const uint32_t *start, const uint32_t *total, uint64_t n, const int32_t *vals,
+                          const uint64_t *rowPtr, uint32_t *fill, int32_t *cols, uint64_t colsCap,
+                          unsigned long long *err, cudaStream_t s)
+{
+    if (n == 0) return cudaSuccess;
+    k_csr_append<<<(unsigned)ceil_div(n, 256), 256, 0, s>>>(start, total, n, vals, rowPtr, fill, cols, colsCap, err);
     sj_note_launch();
     return cudaGetLastError();
 }

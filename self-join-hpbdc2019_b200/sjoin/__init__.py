@@ -28,7 +28,7 @@ DELIVER_DEVICE, DELIVER_HOST, DELIVER_NONE = 0, 1, 2
 # Symbols declared in include/sj.h (checked by the tests against the library).
 EXPORTS = [
     "sj_params_default", "sj_create", "sj_destroy", "sj_import_csv", "sj_read_csv", "sj_set_points", "sj_build_index",
-    "sj_index_sizes", "sj_index_export", "sj_join", "sj_degrees", "sj_neighbor_table", "sj_free",
+    "sj_index_sizes", "sj_index_export", "sj_join", "sj_degrees", "sj_neighbor_table", "sj_neighbor_csr", "sj_free",
     "sj_get_stats", "sj_get_stream", "sj_mlp_num_params", "sj_set_estimator_weights", "sj_load_estimator",
     "sj_cell_features", "sj_mlp_train", "sj_mlp_loss_grad", "sj_mlp_forward", "sj_mlp_loss_grad_noalloc",
     "sj_status_string",
@@ -115,6 +115,7 @@ def load() -> C.CDLL:
     L.sj_join.argtypes = [vp, i32, BATCH_CB, vp]
     L.sj_degrees.argtypes = [vp, vp]
     L.sj_neighbor_table.argtypes = [vp, vp, C.POINTER(C.POINTER(C.c_int)), C.POINTER(u64)]
+    L.sj_neighbor_csr.argtypes = [vp, vp, vp, u64, C.POINTER(u64)]
     L.sj_free.argtypes = [vp]
     L.sj_free.restype = None
     L.sj_get_stats.argtypes = [vp, C.POINTER(Stats)]
@@ -326,6 +327,15 @@ class SelfJoin:
         finally:
             L.sj_free(C.cast(vals, C.c_void_p))
         return rows, v
+
+    def neighbor_csr(self, row_ptr: int, cols: int = 0, capacity: int = 0) -> int:
+        """Device CSR neighbour table: row_ptr / cols are device addresses
+        (n+1 uint64 and `capacity` int32, e.g. torch tensors' data_ptr());
+        cols = 0 only fills row_ptr.  Returns the number of values."""
+        tot = C.c_uint64()
+        _check(load().sj_neighbor_csr(self._h, C.c_void_p(row_ptr), C.c_void_p(cols or None), int(capacity),
+                                      C.byref(tot)))
+        return int(tot.value)
 
     def stream(self) -> int:
         """cudaStream_t of this context (for CUDA events around its work)."""

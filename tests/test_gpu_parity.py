@@ -228,3 +228,31 @@ def test_bad_input_and_call_order():
             sj.set_points(np.array([[0.1, np.nan], [0.2, 0.3]]))
             sj.build_index()
         assert e.value.status == sjoin.SJ_ERR_BAD_INPUT
+
+
+@pytest.mark.parametrize("name,mode,prec", [("exp2d_dense", 5, 0), ("exp4d", 10, 1), ("gauss16_k6", 3, 1)])
+def test_neighbor_csr_on_device(name, mode, prec):
+    # the device CSR table holds exactly the oracle's rows, with several batches
+    import torch
+    pts, eps, k, ix, (ok, ov) = _oracle_pairs(name)
+    n = len(pts)
+    deg = np.bincount(ok, minlength=n)
+    with sjoin.SelfJoin(pts.shape[1], eps, indexed_dims=k, mode=mode, precision=prec,
+                        capacity=max(65536, len(ok) // 3)) as sj:
+        sj.set_points(pts)
+        sj.build_index()
+        row_ptr = torch.zeros(n + 1, dtype=torch.int64, device="cuda")
+        total = sj.neighbor_csr(row_ptr.data_ptr())
+        assert total == len(ok)
+        assert np.array_equal(row_ptr.cpu().numpy(), np.concatenate([[0], np.cumsum(deg)]))
+        with pytest.raises(sjoin.SJError):
+            small = torch.empty(max(total - 1, 1), dtype=torch.int32, device="cuda")
+            sj.neighbor_csr(row_ptr.data_ptr(), small.data_ptr(), max(total - 1, 1))
+        cols = torch.full((total,), -1, dtype=torch.int32, device="cuda")
+        assert sj.neighbor_csr(row_ptr.data_ptr(), cols.data_ptr(), total) == total
+        st = sj.stats()
+    v = cols.cpu().numpy()
+    keys = np.repeat(np.arange(n, dtype=np.int32), deg)
+    order = np.lexsort((v, keys))
+    assert np.array_equal(v[order], ov)
+    assert st.num_batches >= 2 or len(ok) < 65536
