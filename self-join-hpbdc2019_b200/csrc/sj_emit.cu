@@ -31,10 +31,10 @@
 // key order, which sj_expand_keys writes sequentially (the emission's writes
 // land at scattered run positions, which HBM absorbs at a fraction of its
 // sequential rate, so writing the keys there too would cost more than the
-// separate sequential pass).  Every record index is checked
-// against its task's sizes; an index out of range (which a consistent count
-// pass never produces) skips the write and raises an error flag that the host
-// reports.  No distance is evaluated, so the pass is the same for both
+// separate sequential pass).  Every mask word is checked against its task's
+// sizes before it is decoded (bits past the stream end or for queries past the
+// tile, which a consistent count pass never sets, are dropped and raise an
+// error flag that the host reports), so the decoded entries need no checks.  No distance is evaluated, so the pass is the same for both
 // precisions.
 #include "sj_internal.h"
 
@@ -46,7 +46,6 @@ constexpr int EW = 256;             // threads per emission CTA (independent war
 constexpr int ENW = EW / 32;
 constexpr int EM_CAP = 1024;        // staged entries per warp: one window of 32 words x 32 bits
 constexpr uint32_t FULL = 0xffffffffu;
-constexpr uint32_t NO_SLOT = 0xffffffffu;
 #ifndef SJ_EMIT_UNROLL
 #define SJ_EMIT_UNROLL 4
 #endif
@@ -123,39 +122,46 @@ __device__ __forceinline__ void emit_rows(const sj_join_args &a, const UnitTask 
         uint32_t nextWord = lane < nw ? __ldg(wq + lane) : 0u;
         for (uint32_t ws = 0; ws < nw; ws += 32) {
             const uint32_t f = ws + lane;
-            const uint32_t word = nextWord;
+            uint32_t word = nextWord;
             // the next window's word is in flight while this one is written
             nextWord = f + 32 < nw ? __ldg(wq + f + 32) : 0u;
+            const uint32_t q = (uint32_t)(((uint64_t)f * magic) >> 32);
+            {
+                // the word's block must not extend past the stream end: bits
+                // there are never set by a consistent count pass
+                const uint32_t p0 = (c0 + (f - q * cb)) * 32u;
+                const uint32_t valid = p0 >= u.L ? 0u : (u.L - p0 >= 32u ? FULL : (1u << (u.L - p0)) - 1u);
+                if (word & ~valid) {
+                    atomicMax(&a.stat[6], 1ULL);
+                    word &= valid;
+                }
+            }
             const uint32_t cnt = __popc(word);
             const uint32_t incl = warp_incl_scan(cnt, lane);
             const uint32_t T = __shfl_sync(FULL, incl, 31);
             const uint32_t ex = incl - cnt;
-            const uint32_t q = (uint32_t)(((uint64_t)f * magic) >> 32);
             __syncwarp();   // the previous window's copy-out is done with ent / base
             // a query's first word: base = its chunk start slot minus its flat prefix
             if (f < nw && f == q * cb) w.base[q] = w.start[q] - (carry + ex);
             decode_bits(word, (q << 16) | ((f - q * cb) << 5), w.ent, ex);
             __syncwarp();
             // copy-out, CO entries per lane at a time: their candidate-id loads
-            // are all issued before any store
+            // are all issued before any store.  Every entry is valid by
+            // construction (words of queries < nq, bits inside the stream).
             for (uint32_t e0 = 0; e0 < T; e0 += 32 * CO) {
                 uint32_t slot[CO], pos[CO], val[CO];
 #pragma unroll
                 for (int i = 0; i < CO; i++) {
                     const uint32_t e = e0 + 32 * i + lane;
                     const uint32_t ent = w.ent[e < T ? e : 0];
-                    const uint32_t qe = ent >> 16;
                     pos[i] = c0 * 32 + (ent & 0xffffu);
-                    const bool ok = e < T && qe < nq && pos[i] < u.L;
-                    if (e < T && !ok) atomicMax(&a.stat[6], 1ULL);
-                    slot[i] = ok ? w.base[qe] + carry + e : NO_SLOT;
-                    if (!ok) pos[i] = 0;
+                    slot[i] = w.base[ent >> 16] + carry + e;
                 }
 #pragma unroll
                 for (int i = 0; i < CO; i++) val[i] = __ldg(cid + pos[i]);
 #pragma unroll
                 for (int i = 0; i < CO; i++)
-                    if (slot[i] != NO_SLOT) put(a, slot[i], (int32_t)val[i]);
+                    if (e0 + 32 * i + lane < T) put(a, slot[i], (int32_t)val[i]);
             }
             carry += T;
         }
@@ -184,8 +190,18 @@ __device__ __forceinline__ void emit_cols(const sj_join_args &a, const UnitTask 
     }
     uint32_t word = __ldg(cw);
     for (uint32_t g = 0; g < nG; g++) {
-        const uint32_t cur = word;
+        uint32_t cur = word;
         if (g + 1 < nG) word = __ldg(cw + (g + 1) * 32);
+        {
+            // positions past the stream end and queries past the tile have no
+            // bits in a consistent count pass
+            const uint32_t nq = u.qc - g * 32;
+            const uint32_t valid = s >= u.L ? 0u : (nq >= 32u ? FULL : (1u << nq) - 1u);
+            if (cur & ~valid) {
+                atomicMax(&a.stat[6], 1ULL);
+                cur &= valid;
+            }
+        }
         const uint32_t cnt = __popc(cur);
         const uint32_t incl = warp_incl_scan(cnt, lane);
         const uint32_t T = __shfl_sync(FULL, incl, 31);
@@ -201,18 +217,14 @@ __device__ __forceinline__ void emit_cols(const sj_join_args &a, const UnitTask 
             for (int i = 0; i < CO; i++) {
                 const uint32_t e = e0 + 32 * i + lane;
                 const uint32_t ent = w.ent[e < T ? e : 0];
-                const uint32_t owner = ent >> 5;
                 qi[i] = g * 32 + (ent & 31u);
-                const bool ok = e < T && b * 32 + owner < u.L && qi[i] < u.qc;
-                if (e < T && !ok) atomicMax(&a.stat[6], 1ULL);
-                slot[i] = ok ? w.base[owner] + e : NO_SLOT;
-                if (!ok) qi[i] = 0;
+                slot[i] = w.base[ent >> 5] + e;
             }
 #pragma unroll
             for (int i = 0; i < CO; i++) val[i] = __ldg(qids + qi[i]);
 #pragma unroll
             for (int i = 0; i < CO; i++)
-                if (slot[i] != NO_SLOT) put(a, slot[i], (int32_t)val[i]);
+                if (e0 + 32 * i + lane < T) put(a, slot[i], (int32_t)val[i]);
         }
         slot += cnt;
     }
