@@ -189,6 +189,11 @@ struct Ctx {
     // batch state
     DevBuf<uint32_t> keyCount, keyStart;
     DevBuf<int32_t> outKey, outVal;
+    // host delivery: second set of the device buffers a batch's copy reads, so
+    // the next batch's kernels need not wait for that copy
+    DevBuf<int32_t> outValAlt;
+    DevBuf<uint32_t> keyStartAlt;
+    std::vector<cudaEvent_t> syncEvents;   // stage boundaries of the synchronous phase
     DevBuf<uint8_t> scanTemp;
     DevBuf<uint32_t> total;
     DevBuf<unsigned long long> stat;   // see sj_join_args::stat
@@ -813,7 +818,7 @@ sj_status expand_keys(Ctx &c, const sj_join_args &a)
     const size_t slots = sj_expand_long_slots(a.capacity);
     CK(c.longRuns.ensure(slots));
     CK(c.longCount.ensure(1));
-    CK(sj_expand_keys(c.keyStart.p, c.total.p, c.n, a.outKey, a.batchPairs, a.capacity, c.longRuns.p,
+    CK(sj_expand_keys(a.keyStart, c.total.p, c.n, a.outKey, a.batchPairs, a.capacity, c.longRuns.p,
                       (uint32_t)std::min<size_t>(c.longRuns.n, 0xffffffffu), c.longCount.p, c.numSM, c.s));
     return SJ_OK;
 }
@@ -1030,13 +1035,13 @@ sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
     // into pinned memory.  A batch is handed to the callback after the next
     // batch's GPU work and copies have been queued, so the expansion and the
     // callback overlap them (double-buffered pinned sets).
-    Timer tb;
     unsigned long long *slot = c.batchTot.p + plan.size();
     struct Pending {
         bool live = false;
         uint64_t cnt = 0, index = 0;
         int sel = 0;
     } pend;
+    bool setUsed[2] = {false, false};
     auto finishPending = [&]() -> sj_status {
         if (!pend.live) return SJ_OK;
         pend.live = false;
@@ -1049,26 +1054,41 @@ sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
         }
         return SJ_OK;
     };
+    // stage times: six events per iteration, read after the loop
+    size_t iter = 0;
+    std::vector<int> iterFull;   // 1: the iteration ran all stages, 0: count + scan only (re-planned)
+    auto ev = [&](size_t k) -> cudaEvent_t { return c.syncEvents[6 * iter + k]; };
+    const bool hostDel = delivery == SJ_DELIVER_HOST;
+    if (hostDel) CK(c.keyStartAlt.ensure(n ? n : 1));
     while (!stack.empty() && result == SJ_OK) {
         BatchRange br = stack.back();
         stack.pop_back();
+        while (c.syncEvents.size() < 6 * (iter + 1)) {
+            cudaEvent_t e;
+            CK(cudaEventCreate(&e));
+            c.syncEvents.push_back(e);
+        }
+        // host delivery alternates between two buffer sets (the pinned sets' index)
+        const int sel = hostDel ? pinSel : 0;
+        uint32_t *const ksBuf = sel ? c.keyStartAlt.p : c.keyStart.p;
         a.taskBegin = br.t0;
         a.taskEnd = br.t1;
         a.batchPairs = slot;
         a.capacity = c.outKey.n;
+        a.keyStart = ksBuf;
         CK(cudaMemsetAsync(slot, 0, sizeof(unsigned long long), c.s));
-        tb.start(c.s);
+        CK(cudaEventRecord(ev(0), c.s));
         CKS(run_count(c, a, queue));
-        msCount += tb.stop(c.s);
-        tb.start(c.s);
-        // the previous batch's run offsets must be copied before the scan rewrites them
-        if (pend.live) CK(cudaStreamWaitEvent(c.s, c.evStart[pend.sel], 0));
-        CK(sj_exclusive_scan_u32_clear(c.keyCount.p, c.keyStart.p, n, c.scanTemp.p, c.total.p, c.s));
+        CK(cudaEventRecord(ev(1), c.s));
+        // this set's run offsets must have been copied out before the scan rewrites them
+        if (setUsed[sel]) CK(cudaStreamWaitEvent(c.s, c.evStart[sel], 0));
+        CK(sj_exclusive_scan_u32_clear(c.keyCount.p, ksBuf, n, c.scanTemp.p, c.total.p, c.s));
+        CK(cudaEventRecord(ev(2), c.s));
         unsigned long long cnt = 0;
         CK(cudaMemcpyAsync(c.pinTotal.p, slot, sizeof(unsigned long long), cudaMemcpyDeviceToHost, c.s));
         CK(cudaMemcpyAsync(hTaskHits.data() + br.t0, c.taskHits.p + br.t0, sizeof(uint32_t) * (br.t1 - br.t0),
                            cudaMemcpyDeviceToHost, c.s));
-        msScan += tb.stop(c.s);
+        CK(cudaStreamSynchronize(c.s));
         memcpy(&cnt, c.pinTotal.p, sizeof(cnt));
         if (cnt > cap) {
             // estimate too low: re-plan the batch from the measured per-task
@@ -1077,39 +1097,45 @@ sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
             CKS(replan_exact(br, hTaskHits, cap, parts));
             for (size_t i = parts.size(); i-- > 0;) stack.push_back(parts[i]);
             retries++;
+            iterFull.push_back(0);
+            iter++;
             continue;
         }
         if (cnt > 0) relErrSum += std::fabs(predOf(br) - (double)cnt) / (double)cnt;
         // output buffers follow the exact batch size (grow-only, 25% headroom, <= capacity)
         if (cnt > c.outKey.n) {
             CKS(finishPending());   // its copy may still read the old buffers
+            CK(cudaStreamSynchronize(c.cs));
             uint64_t want = std::min<uint64_t>(cap, std::max<uint64_t>(cnt, (uint64_t)(1.25 * (double)c.outKey.n)));
             CK(c.outKey.ensure(want));
             CK(c.outVal.ensure(want));
+            if (hostDel) CK(c.outValAlt.ensure(want));
         }
+        if (hostDel && c.outValAlt.n < c.outVal.n) {
+            CKS(finishPending());
+            CK(cudaStreamSynchronize(c.cs));
+            CK(c.outValAlt.ensure(c.outVal.n));
+        }
+        int32_t *const valBuf = sel ? c.outValAlt.p : c.outVal.p;
         a.outKey = c.outKey.p;
-        a.outVal = c.outVal.p;
-        a.capacity = c.outKey.n;
-        tb.start(c.s);
-        // the previous batch's values must be copied before the emission rewrites them
-        if (pend.live) CK(cudaStreamWaitEvent(c.s, c.evVals[pend.sel], 0));
+        a.outVal = valBuf;
+        a.capacity = std::min<uint64_t>(c.outKey.n, sel ? c.outValAlt.n : c.outVal.n);
         CKS(expand_keys(c, a));
-        msExpand += tb.stop(c.s);
-        tb.start(c.s);
+        CK(cudaEventRecord(ev(3), c.s));
+        // this set's values must have been copied out before the emission rewrites them
+        if (setUsed[sel]) CK(cudaStreamWaitEvent(c.s, c.evVals[sel], 0));
         CK(cudaMemsetAsync(c.queueHead.p, 0, sizeof(uint32_t), c.s));
         CK(sj_launch_emit(a, c.numSM, c.s));
-        msFill += tb.stop(c.s);
-        tb.start(c.s);
-        CK(sj_hash_pairs(c.outKey.p, c.outVal.p, cnt, c.stat.p + 4, c.s));
+        CK(cudaEventRecord(ev(4), c.s));
+        CK(sj_hash_pairs(c.outKey.p, valBuf, cnt, c.stat.p + 4, c.s));
         if (delivery == SJ_DELIVER_CSR) {
-            CK(sj_csr_append(c.keyStart.p, c.total.p, n, c.outVal.p, c.csrRowPtr, c.csrFill.p, c.csrCols, c.csrCap,
+            CK(sj_csr_append(ksBuf, c.total.p, n, valBuf, c.csrRowPtr, c.csrFill.p, c.csrCols, c.csrCap,
                              c.stat.p + 7, c.s));
         } else if (delivery == SJ_DELIVER_DEVICE && cb) {
             CK(cudaStreamSynchronize(c.s));
-            sj_batch b{batches, cnt, c.outKey.p, c.outVal.p, 1};
+            sj_batch b{batches, cnt, c.outKey.p, valBuf, 1};
             if (cb(&b, user)) result = SJ_ERR_ABORTED;
-        } else if (delivery == SJ_DELIVER_HOST) {
-            const int sel = pinSel;
+        } else if (hostDel) {
             const size_t vb = std::max<size_t>(cnt, 1) * sizeof(int32_t);
             if (vb > c.pinVal[sel].bytes) {
                 size_t want = std::max<size_t>(vb, (size_t)(1.25 * (double)c.pinVal[sel].bytes));
@@ -1120,11 +1146,11 @@ sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
             CK(c.pinStart[sel].ensure(n * sizeof(uint32_t)));
             CK(cudaEventRecord(c.evEmit, c.s));
             CK(cudaStreamWaitEvent(c.cs, c.evEmit, 0));
-            CK(cudaMemcpyAsync(c.pinStart[sel].p, c.keyStart.p, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, c.cs));
+            CK(cudaMemcpyAsync(c.pinStart[sel].p, ksBuf, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, c.cs));
             CK(cudaEventRecord(c.evStart[sel], c.cs));
-            if (cnt)
-                CK(cudaMemcpyAsync(c.pinVal[sel].p, c.outVal.p, cnt * sizeof(int32_t), cudaMemcpyDeviceToHost, c.cs));
+            if (cnt) CK(cudaMemcpyAsync(c.pinVal[sel].p, valBuf, cnt * sizeof(int32_t), cudaMemcpyDeviceToHost, c.cs));
             CK(cudaEventRecord(c.evVals[sel], c.cs));
+            setUsed[sel] = true;
             // the previous batch goes to the consumer while this one is copied
             sj_status ps = finishPending();
             if (ps != SJ_OK) {
@@ -1137,7 +1163,9 @@ sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
             pend.sel = sel;
             pinSel ^= 1;
         }
-        msDeliver += tb.stop(c.s);
+        CK(cudaEventRecord(ev(5), c.s));
+        iterFull.push_back(1);
+        iter++;
         pairsTotal += cnt;
         batches++;
     }
@@ -1149,6 +1177,23 @@ sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
         }
     }
     CK(cudaStreamSynchronize(c.cs));
+    CK(cudaStreamSynchronize(c.s));
+    for (size_t i = 0; i < iter; i++) {
+        float t01 = 0, t12 = 0, t23 = 0, t34 = 0, t45 = 0;
+        cudaEvent_t *e = c.syncEvents.data() + 6 * i;
+        cudaEventElapsedTime(&t01, e[0], e[1]);
+        cudaEventElapsedTime(&t12, e[1], e[2]);
+        msCount += t01;
+        msScan += t12;
+        if (iterFull[i]) {
+            cudaEventElapsedTime(&t23, e[2], e[3]);
+            cudaEventElapsedTime(&t34, e[3], e[4]);
+            cudaEventElapsedTime(&t45, e[4], e[5]);
+            msExpand += t23;
+            msFill += t34;
+            msDeliver += t45;
+        }
+    }
     unsigned long long hs[8];
     CK(cudaMemcpyAsync(hs, c.stat.p, sizeof(hs), cudaMemcpyDeviceToHost, c.s));
     CK(cudaStreamSynchronize(c.s));
@@ -1375,6 +1420,7 @@ sj_status sj_destroy(void *ctx)
     if (c->cs) cudaStreamSynchronize(c->cs);
     cudaStream_t s = c->s, cs = c->cs;
     for (cudaEvent_t e : c->events) cudaEventDestroy(e);
+    for (cudaEvent_t e : c->syncEvents) cudaEventDestroy(e);
     for (int i = 0; i < 2; i++) {
         if (c->evStart[i]) cudaEventDestroy(c->evStart[i]);
         if (c->evVals[i]) cudaEventDestroy(c->evVals[i]);

@@ -72,11 +72,17 @@ __device__ __forceinline__ uint32_t warp_incl_scan(uint32_t x, uint32_t lane)
 __device__ __forceinline__ void decode_bits(uint32_t m, uint32_t tag, uint32_t *buf, uint32_t k)
 {
     uint32_t *p = buf + k;
-    while (m) {
-        const uint32_t b = __ffs(m) - 1;
+    // two set bits per round (a lone last bit is written on its own)
+    while (m & (m - 1)) {
+        const uint32_t b0 = __ffs(m) - 1;
         m &= m - 1;
-        *p++ = tag | b;
+        const uint32_t b1 = __ffs(m) - 1;
+        m &= m - 1;
+        p[0] = tag | b0;
+        p[1] = tag | b1;
+        p += 2;
     }
+    if (m) *p = tag | (__ffs(m) - 1);
 }
 
 __device__ __forceinline__ void put(const sj_join_args &a, uint32_t slot, int32_t val)
