@@ -19,6 +19,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstdlib>
+#include <immintrin.h>
 #include <cstring>
 #include <mutex>
 #include <numeric>
@@ -771,16 +772,38 @@ uint64_t auto_capacity(Ctx &c)
     return std::max<uint64_t>(1 << 20, std::min<uint64_t>(byMem, 2000000000ULL));
 }
 
+// Fills key[b, e) with k using non-temporal 32-byte stores (the destination
+// is written once and read later by the consumer: streaming stores skip the
+// read-for-ownership of every line, which halves the host memory traffic
+// while the copy engine is writing the same memory).
+__attribute__((target("avx2"))) static void fill_run_stream(int32_t *key, uint64_t b, uint64_t e, int32_t k)
+{
+    uint64_t i = b;
+    while (i < e && (((uintptr_t)(key + i)) & 31u)) key[i++] = k;
+    const __m256i v = _mm256_set1_epi32(k);
+    for (; i + 8 <= e; i += 8) _mm256_stream_si256(reinterpret_cast<__m256i *>(key + i), v);
+    for (; i < e; i++) key[i] = k;
+}
+
 // Keys of a delivered batch from its run offsets: key k owns slots
 // [start[k], start[k+1]) (start[n] = cnt).  Parallel over keys on the host.
 void expand_keys_host(const uint32_t *start, uint64_t n, uint64_t cnt, int32_t *key)
 {
     if (cnt == 0) return;
-#pragma omp parallel for schedule(static)
-    for (int64_t k = 0; k < (int64_t)n; k++) {
-        const uint64_t b = start[k];
-        const uint64_t e = (k + 1 < (int64_t)n) ? start[k + 1] : cnt;
-        for (uint64_t i = b; i < e; i++) key[i] = (int32_t)k;
+    static const bool avx2 = __builtin_cpu_supports("avx2");
+#pragma omp parallel
+    {
+#pragma omp for schedule(static)
+        for (int64_t k = 0; k < (int64_t)n; k++) {
+            const uint64_t b = start[k];
+            const uint64_t e = (k + 1 < (int64_t)n) ? start[k + 1] : cnt;
+            if (avx2 && e - b >= 64) {
+                fill_run_stream(key, b, e, (int32_t)k);
+            } else {
+                for (uint64_t i = b; i < e; i++) key[i] = (int32_t)k;
+            }
+        }
+        _mm_sfence();   // streaming stores are visible before the consumer reads them
     }
 }
 
