@@ -70,3 +70,20 @@ def test_import_order_for_unit_cube_data(tmp_path, n):
     ref = _ref_import(str(f), 2)
     assert np.array_equal(sjoin.read_csv(str(f), 2), ref)
     assert np.array_equal(ref, pts) == (n <= 16)
+
+
+def test_import_parallel_ranges_match_reference(tmp_path):
+    # a file of several MB is parsed in one range per thread, cut after commas;
+    # the concatenated values and the replayed bin sort must still equal the
+    # reference's own import (mixed spacing and a trailing partial point)
+    rng = np.random.default_rng(9)
+    pts = rng.normal(0.5, 0.7, (250_000, 3))
+    lines = [f"{a!r}, {b!r},{c!r}" if i % 7 else f" {a!r} ,\t{b!r} , {c!r} "
+             for i, (a, b, c) in enumerate(pts.tolist())]
+    f = tmp_path / "big.csv"
+    f.write_text("\n".join(lines) + "\n0.25,0.5\n")
+    assert os.path.getsize(f) > 4 << 20
+    ref = _ref_import(str(f), 3)
+    got = sjoin.read_csv(str(f), 3)
+    assert got.shape == ref.shape == (250_000, 3)
+    assert np.array_equal(got.view(np.uint64), ref.view(np.uint64))
