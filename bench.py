@@ -112,6 +112,22 @@ def _dist():
     return ws, rank, local
 
 
+def combine_ranks(ms, pairs, pair_hash, device):
+    """(max step ms, summed pairs, summed set hash mod 2^64) over all ranks.
+
+    The set hash is a wrapping 64-bit sum over pairs, so the hashes of disjoint
+    shards add up (mod 2^64) to the hash of their union; it travels as int64,
+    whose two's-complement sum wraps the same way."""
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([ms], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    h = pair_hash - (1 << 64) if pair_hash >= (1 << 63) else pair_hash
+    v = torch.tensor([pairs, h], dtype=torch.int64, device=device)
+    dist.all_reduce(v)
+    return float(t.item()), int(v[0].item()), int(v[1].item()) % (1 << 64)
+
+
 def cpu_oracle_rate(pts, eps, k, target_s=12.0, threads=0):
     """Oracle grid join on a bounded sample of query points: (pairs/s, cores, sample text)."""
     import oracle
@@ -168,7 +184,7 @@ def _config(args, spec):
         "n": spec["n"], "dims": spec["D"], "indexed_dims": spec["k"], "eps": spec["eps"],
         "search_mode": spec["mode"], "batch_capacity_pairs": spec["capacity"],
         "l2": "flushed between steps (256 MiB write); outputs far exceed L2",
-        "parallelism": f"replicas x{_dist()[0]}",
+        "parallelism": (f"task shards x{_dist()[0]}" if getattr(args, "shard", False) else f"replicas x{_dist()[0]}"),
     }
 
 
@@ -181,15 +197,19 @@ def run_ours(args):
     if ws > 1:
         import datetime
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-    pts, eps, k, spec = sjoin.datasets.make(args.workload, n=args.n,
-                                            seed=sjoin.datasets.SEEDS[args.workload] + 1000 * rank)
+    # replicas (default): every rank joins its own seeded set (weak scaling);
+    # --shard: all ranks share one set and each runs one shard of its
+    # cost-ordered task list (strong scaling, no data-path exchange)
+    seed = sjoin.datasets.SEEDS[args.workload] + (0 if args.shard else 1000 * rank)
+    pts, eps, k, spec = sjoin.datasets.make(args.workload, n=args.n, seed=seed)
     if args.capacity is not None:
         spec["capacity"] = args.capacity
     prec = spec["precision"] if args.precision is None else args.precision
     flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device="cuda")
     sj = sjoin.SelfJoin(spec["D"], eps, indexed_dims=k, mode=spec["mode"], precision=prec,
                         scheduler=sjoin.SCHED_LEARNED if args.learned else sjoin.SCHED_SAMPLING,
-                        capacity=spec["capacity"], device=local)
+                        capacity=spec["capacity"], device=local,
+                        shard_index=rank if args.shard else 0, shard_count=ws if args.shard else 1)
     if args.learned:
         sj.load_estimator(args.learned)
     host = torch.from_numpy(pts).pin_memory()
@@ -226,13 +246,9 @@ def run_ours(args):
     clocks = sampler.stop()
     ms = statistics.mean(step_ms)
     pairs = stats[-1]["total_pairs"]
-    job_ms, job_pairs = ms, pairs
+    job_ms, job_pairs, job_hash = ms, pairs, stats[-1]["pair_hash"]
     if ws > 1:
-        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        p = torch.tensor([pairs], device="cuda", dtype=torch.float64)
-        torch.distributed.all_reduce(p)
-        job_ms, job_pairs = float(t.item()), float(p.item())
+        job_ms, job_pairs, job_hash = combine_ranks(ms, pairs, job_hash, "cuda")
 
     # end to end through the C ABI with host buffers: pinned H2D of the points,
     # index, join, and every batch copied device-to-host into pinned buffers
@@ -298,9 +314,10 @@ def run_ours(args):
     line = {
         "metric": "self-join pairs/s", "value": job_pairs / (job_ms / 1e3), "unit": "pairs/s", "n_gpus": ws,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": job_ms, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64" if prec == 0 else "f32+f64",
+        "scaling": "strong" if args.shard else "weak", "vs_baseline": None,
+        "dtype": "f64" if prec == 0 else "f32+f64",
         "data": "synthetic (seeded generator, same shapes and distributions)", "config": _config(args, spec),
-        "time_s": job_ms / 1e3, "pairs_per_step": pairs, "pair_hash": s["pair_hash"],
+        "time_s": job_ms / 1e3, "pairs_per_step": job_pairs, "pair_hash": job_hash,
         "roofline": {"bound": "hbm", "kernel": kdesc, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": (achieved / peak) if achieved else None, "peak_kind": peak_kind,
                      "algorithmic_bytes_per_launch": algo_bytes / nb, "launches": nb, "traffic": traffic,
@@ -332,6 +349,8 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", default="c2")
     ap.add_argument("--n", type=int, default=None)
+    ap.add_argument("--shard", action="store_true",
+                    help="N > 1: split one join over the ranks (strong scaling) instead of N replicas")
     ap.add_argument("--capacity", type=int, default=None, help="batch capacity in pairs (default: the workload's)")
     ap.add_argument("--precision", type=int, default=None)
     ap.add_argument("--learned", default=None,
