@@ -175,7 +175,7 @@ def run_reference(args):
 
 def _config(args, spec):
     mode_name = {3: "full stencil", 4: "Unicomp", 5: "B-Unicomp", 6: "linear-ID Unicomp", 7: "full stencil",
-                 9: "work queue", 10: "linear-ID Unicomp"}[spec["mode"]]
+                 8: "full stencil", 9: "work queue", 10: "linear-ID Unicomp"}[spec["mode"]]
     return {
         "workload": (f"{args.workload}: {spec['D']}-D {spec['kind']}, n={spec['n']}, eps={spec['eps']}, "
                      f"{mode_name} + workload-sorted work queue, "

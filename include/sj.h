@@ -53,7 +53,9 @@ typedef struct {
     int blocksize;            /* BLOCKSIZE: accepted for compatibility; the engine uses 128-thread CTAs */
     int threadperpoint;       /* THREADPERPOINT: accepted for compatibility (1) */
     int search_mode;          /* 3 full stencil, 4 Unicomp, 5 B-Unicomp (k=2,3), 6 linear-ID Unicomp,
-                                 7 full stencil in workload order, 9 work queue, 10 work queue + LID-Unicomp */
+                                 7 full stencil in workload order, 8 full stencil with work split by
+                                 workload (the reference's dynamic threads per point), 9 work queue,
+                                 10 work queue + LID-Unicomp */
     int sort_by_workload;     /* SORT_BY_WORKLOAD: order work by estimated cost, heaviest first */
     int precision;            /* sj_precision */
     int scheduler;            /* sj_scheduler: estimator used to size result batches */

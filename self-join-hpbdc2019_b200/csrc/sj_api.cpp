@@ -129,7 +129,11 @@ struct Timer {
 int pattern_of_mode(int mode)
 {
     switch (mode) {
-    case 3: case 7: case 9: return SJ_PAT_FULL;
+    // mode 8 (kernel.cu:2072-2188: heaviest points first, 1/3 of the batches
+    // each with NB_THREAD_THIRD{1,2,3} threads per point) is the full stencil
+    // in workload order; the engine's work split is its cost-proportional task
+    // chunking (a heavier cell is cut into more tasks), so it runs like 7 / 9
+    case 3: case 7: case 8: case 9: return SJ_PAT_FULL;
     case 4: return SJ_PAT_UNICOMP;
     case 5: return SJ_PAT_BUNICOMP;
     case 6: case 10: return SJ_PAT_LID;
@@ -253,7 +257,7 @@ sj_status check_params(const sj_params &p)
         return SJ_ERR_BAD_INPUT;
     }
     if (pattern_of_mode(p.search_mode) < 0) {
-        set_error("search_mode %d not supported (3,4,5,6,7,9,10)", p.search_mode);
+        set_error("search_mode %d not supported (3,4,5,6,7,8,9,10)", p.search_mode);
         return SJ_ERR_BAD_INPUT;
     }
     if (p.search_mode == 5 && p.numindexeddim != 2 && p.numindexeddim != 3) {
@@ -754,7 +758,7 @@ sj_status prepare_join(Ctx &c, int &pattern, bool &queue)
     }
     pattern = pattern_of_mode(c.p.search_mode);
     // work queue: modes 9/10, or any mode when work is ordered by workload
-    queue = (c.p.search_mode == 9 || c.p.search_mode == 10 || c.p.sort_by_workload != 0);
+    queue = (c.p.search_mode == 8 || c.p.search_mode == 9 || c.p.search_mode == 10 || c.p.sort_by_workload != 0);
     Timer tm;
     tm.start(c.s);
     CKS(build_neighbours(c, pattern));
@@ -864,8 +868,8 @@ sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
     {
         Timer tm;
         tm.start(c.s);
-        const bool byCost = c.p.sort_by_workload || c.p.search_mode == 7 || c.p.search_mode == 9 ||
-                            c.p.search_mode == 10;
+        const bool byCost = c.p.sort_by_workload || c.p.search_mode == 7 || c.p.search_mode == 8 ||
+                            c.p.search_mode == 9 || c.p.search_mode == 10;
         CKS(build_tasks(c, pattern, cap, byCost));
         CK(c.dTasks.ensure(c.tasks.size()));
         if (!c.tasks.empty())

@@ -170,7 +170,8 @@ def mlp_num_params() -> int:
 
 
 MODE_NAMES = {3: "full stencil", 4: "Unicomp", 5: "B-Unicomp", 6: "linear-ID Unicomp",
-              7: "full stencil, workload order", 9: "work queue", 10: "work queue + linear-ID Unicomp"}
+              7: "full stencil, workload order", 8: "full stencil, work split by workload", 9: "work queue",
+              10: "work queue + linear-ID Unicomp"}
 
 
 class SelfJoin:

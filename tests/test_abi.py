@@ -37,7 +37,7 @@ def test_params_default_follow_params_h():
 
 @pytest.mark.parametrize("field,value", [
     ("gpunumdim", 0), ("gpunumdim", 17), ("numindexeddim", 3), ("epsilon", 0.0), ("epsilon", float("nan")),
-    ("search_mode", 8), ("search_mode", 2), ("precision", 5), ("scheduler", 9), ("sample_rate", 0.0),
+    ("search_mode", 11), ("search_mode", 2), ("precision", 5), ("scheduler", 9), ("sample_rate", 0.0),
     ("shard_count", 0), ("batch_capacity_pairs", 1000),
 ])
 def test_bad_params_rejected_before_device(field, value):

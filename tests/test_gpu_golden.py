@@ -50,7 +50,7 @@ def test_engine_matches_reference_pairs(path, prec):
     pts, eps, k = f["pts"], float(f["eps"]), int(f["k"])
     ref_key = np.repeat(np.arange(len(pts), dtype=np.int32), f["deg"])
     ref_val = f["val"]
-    modes = [3, 4, 5, 6, 7, 9, 10] if k in (2, 3) else [3, 4, 6, 7, 9, 10]
+    modes = [3, 4, 5, 6, 7, 8, 9, 10] if k in (2, 3) else [3, 4, 6, 7, 8, 9, 10]
     for mode in modes:
         key, val, st = _join(pts, eps, k, mode, prec)
         assert st.total_pairs == len(ref_key), (mode, st.total_pairs, len(ref_key))

@@ -67,7 +67,7 @@ def _check_batches(batches, cap=None):
 
 
 def _modes_for(k):
-    return [3, 4, 5, 6, 7, 9, 10] if k in (2, 3) else [3, 4, 6, 7, 9, 10]
+    return [3, 4, 5, 6, 7, 8, 9, 10] if k in (2, 3) else [3, 4, 6, 7, 8, 9, 10]
 
 
 @pytest.mark.parametrize("name", sorted(_cases()))
