@@ -23,6 +23,8 @@
 #include <cstring>
 #include <mutex>
 #include <numeric>
+#include <omp.h>
+#include <parallel/algorithm>
 #include <string>
 #include <vector>
 
@@ -638,8 +640,6 @@ uint32_t cell_tasks(const Ctx &c, uint32_t A, bool sym, uint64_t cap, double pai
 // keep linear-id order.  Cells are processed in parallel on the host.
 sj_status build_tasks(Ctx &c, int pattern, uint64_t cap, bool byCost)
 {
-    Timer tm;
-    tm.start(c.s);
     const bool sym = pattern != SJ_PAT_FULL;
     const uint32_t nc = c.nCells;
     const double pairsPerTask = std::max(4096.0, (double)cap / 4096.0);
@@ -657,9 +657,12 @@ sj_status build_tasks(Ctx &c, int pattern, uint64_t cap, bool byCost)
     }
     std::vector<uint32_t> order(nc);
     std::iota(order.begin(), order.end(), 0u);
+    // heaviest first; equal costs keep cell order (the cell index breaks ties,
+    // so the parallel sort gives the order a stable sort would)
     if (byCost)
-        std::stable_sort(order.begin(), order.end(),
-                         [&](uint32_t x, uint32_t y) { return cellCost[x] > cellCost[y]; });
+        __gnu_parallel::sort(order.begin(), order.end(), [&](uint32_t x, uint32_t y) {
+            return cellCost[x] > cellCost[y] || (cellCost[x] == cellCost[y] && x < y);
+        });
     std::vector<uint64_t> off(nc + 1, 0);
     for (uint32_t i = 0; i < nc; i++) off[i + 1] = off[i] + cnt[order[i]];
     const uint64_t nt = off[nc];
@@ -693,7 +696,6 @@ sj_status build_tasks(Ctx &c, int pattern, uint64_t cap, bool byCost)
         c.taskEvals.resize(w);
         c.taskPred.resize(w);
     }
-    c.st.ms_tasks += tm.stop(c.s);
     return SJ_OK;
 }
 
@@ -721,17 +723,41 @@ sj_status task_offsets(Ctx &c)
     c.hRowOff.assign(nt + 1, 0);
     c.hCandOff.assign(nt + 1, 0);
     c.hUnitOff.assign(nt + 1, 0);
-    for (size_t i = 0; i < nt; i++) {
-        const sj_task &t = c.tasks[i];
-        const uint32_t len = t.sEnd - t.sBegin;
-        const bool sym = (t.flags & SJ_TASK_SYM) != 0;
-        const uint64_t blocks = ((uint64_t)len + 31) / 32;
-        const uint64_t groups = ((uint64_t)t.qCount + 31) / 32;
-        c.hMaskOff[i + 1] = c.hMaskOff[i] + blocks * t.qCount;
-        c.hColOff[i + 1] = c.hColOff[i] + (sym ? blocks * groups * 32 : 0);
-        c.hRowOff[i + 1] = c.hRowOff[i] + t.qCount;
-        c.hCandOff[i + 1] = c.hCandOff[i] + len;
-        c.hUnitOff[i + 1] = c.hUnitOff[i] + sj_task_units(t.qCount, len, sym);
+    // per-task sizes at [i + 1], then one prefix pass: per-thread range sums,
+    // their exclusive scan, and the ranges' prefixes from those bases
+    const int T = std::max(1, omp_get_max_threads());
+    std::vector<uint64_t> part(5 * (size_t)(T + 1), 0);
+#pragma omp parallel num_threads(T)
+    {
+        const int th = omp_get_thread_num(), nth = omp_get_num_threads();
+        const size_t b = nt * (size_t)th / (size_t)nth, e = nt * (size_t)(th + 1) / (size_t)nth;
+        uint64_t acc[5] = {0, 0, 0, 0, 0};
+        for (size_t i = b; i < e; i++) {
+            const sj_task &t = c.tasks[i];
+            const uint32_t len = t.sEnd - t.sBegin;
+            const bool sym = (t.flags & SJ_TASK_SYM) != 0;
+            const uint64_t blocks = ((uint64_t)len + 31) / 32;
+            const uint64_t groups = ((uint64_t)t.qCount + 31) / 32;
+            c.hMaskOff[i + 1] = acc[0] += blocks * t.qCount;
+            c.hColOff[i + 1] = acc[1] += (sym ? blocks * groups * 32 : 0);
+            c.hRowOff[i + 1] = acc[2] += t.qCount;
+            c.hCandOff[i + 1] = acc[3] += len;
+            c.hUnitOff[i + 1] = acc[4] += sj_task_units(t.qCount, len, sym);
+        }
+        for (int k = 0; k < 5; k++) part[5 * (size_t)(th + 1) + k] = acc[k];
+#pragma omp barrier
+#pragma omp single
+        for (int t2 = 1; t2 <= nth; t2++)
+            for (int k = 0; k < 5; k++) part[5 * (size_t)t2 + k] += part[5 * (size_t)(t2 - 1) + k];
+        const uint64_t *base = &part[5 * (size_t)th];
+        if (th > 0)
+            for (size_t i = b; i < e; i++) {
+                c.hMaskOff[i + 1] += base[0];
+                c.hColOff[i + 1] += base[1];
+                c.hRowOff[i + 1] += base[2];
+                c.hCandOff[i + 1] += base[3];
+                c.hUnitOff[i + 1] += base[4];
+            }
     }
     CK(c.dMaskOff.ensure(nt + 1));
     CK(c.dColOff.ensure(nt + 1));
