@@ -40,10 +40,10 @@ sys.path.insert(0, os.path.join(REPO, "self-join-hpbdc2019_b200"))
 import numpy as np  # noqa: E402
 
 # dram__bytes_read.sum + dram__bytes_write.sum per output pair of the emission
-# kernel (k_emit): 31.4 MB read + 114.1 MB written for a batch of ~28.5 M pairs
+# kernel (k_emit): 31.4 MB read + 115.2 MB written for a batch of ~28.8 M pairs
 # in one ncu capture of the c2 shape at n = 600,000 (profiles/k_emit_c2_n600k.md);
 # the traffic grows with the pairs, so a full-size launch is scaled by its pairs
-EMIT_TRAFFIC_BYTES_PER_PAIR = (31.4e6 + 114.1e6) / 28.5e6
+EMIT_TRAFFIC_BYTES_PER_PAIR = (31.4e6 + 115.2e6) / 28.8e6
 
 # CUDA-core lanes per SM (B200): FP64 FMA and FP32 FMA per clock
 FP64_LANES, FP32_LANES, NUM_SM = 64, 128, 148
