@@ -29,6 +29,7 @@ static const char *stats_file(int mode)
     case 5: return "gpu_b-unicomp_stats.txt";
     case 6: return "gpu_linID-unicomp_stats.txt";
     case 7: return "gpu_sorting-cells_stats.txt";
+    case 8: return "gpu_dynamic-threads-fixed_stats.txt";
     case 9: return "gpu_working-queue_stats.txt";
     case 10: return "gpu_working-queue_lid-unicomp_stats.txt";
     }

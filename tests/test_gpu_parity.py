@@ -27,6 +27,8 @@ def _cases():
         "exp6d": (exp_points(6000, 6, 6), 0.05, 6),
         "gauss16_k6": (_gauss16(4000, 5), 0.25, 6),
         "uniform5d_k3": (r(6).random((5000, 5)), 0.12, 3),
+        "exp8d_k4": (exp_points(4000, 8, 9), 0.06, 4),          # padded width 8
+        "uniform12d_k3": (r(10).random((3000, 12)) * 0.4, 0.3, 3),  # padded width 12
         "line1d": (r(7).random((5000, 1)), 0.0005, 1),
         "shell3d": (shell_points(3000, 3, 0.05, 8), 0.05, 3),
         "lattice2d": (lattice_points(60, 2, 0.1), 0.1, 2),
