@@ -1702,6 +1702,17 @@ sj_status sj_neighbor_csr(void *ctx, uint64_t *rowPtr, int32_t *cols, uint64_t c
     }
     Ctx &c = *as_ctx(ctx);
     CKS(bind(c));
+    // the table is written by kernels: both arrays must be memory the device can write
+    for (const void *ptr : {(const void *)rowPtr, (const void *)cols}) {
+        if (!ptr) continue;
+        cudaPointerAttributes at{};
+        if (cudaPointerGetAttributes(&at, ptr) != cudaSuccess ||
+            (at.type != cudaMemoryTypeDevice && at.type != cudaMemoryTypeManaged)) {
+            cudaGetLastError();
+            set_error("rowPtr and cols must be device (or managed) memory");
+            return SJ_ERR_BAD_INPUT;
+        }
+    }
     const uint64_t n = c.n;
     std::vector<uint32_t> deg(n);
     CKS(run_degrees(c, deg.data()));

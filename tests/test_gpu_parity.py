@@ -250,6 +250,10 @@ def test_neighbor_csr_on_device(name, mode, prec):
         with pytest.raises(sjoin.SJError):
             small = torch.empty(max(total - 1, 1), dtype=torch.int32, device="cuda")
             sj.neighbor_csr(row_ptr.data_ptr(), small.data_ptr(), max(total - 1, 1))
+        with pytest.raises(sjoin.SJError) as e:   # host memory is refused before any kernel runs
+            host_cols = np.zeros(total, np.int32)
+            sj.neighbor_csr(row_ptr.data_ptr(), host_cols.ctypes.data, total)
+        assert e.value.status == sjoin.SJ_ERR_BAD_INPUT
         cols = torch.full((total,), -1, dtype=torch.int32, device="cuda")
         assert sj.neighbor_csr(row_ptr.data_ptr(), cols.data_ptr(), total) == total
         st = sj.stats()
