@@ -68,29 +68,74 @@ __device__ __forceinline__ uint32_t warp_incl_scan(uint32_t x, uint32_t lane)
     return x;
 }
 
-// Appends tag | (index of each set bit of m), lowest bit first, to buf[k...].
-__device__ __forceinline__ void decode_bits(uint32_t m, uint32_t tag, uint32_t *buf, uint32_t k)
+// Index of the highest set bit of m (m != 0).
+__device__ __forceinline__ uint32_t top_bit(uint32_t m)
 {
-    uint32_t *p = buf + k;
-    // two set bits per round (a lone last bit is written on its own)
-    while (m & (m - 1)) {
-        const uint32_t b0 = __ffs(m) - 1;
-        m &= m - 1;
-        const uint32_t b1 = __ffs(m) - 1;
-        m &= m - 1;
-        p[0] = tag | b0;
-        p[1] = tag | b1;
-        p += 2;
-    }
-    if (m) *p = tag | (__ffs(m) - 1);
+    uint32_t b;
+    asm("bfind.u32 %0, %1;" : "=r"(b) : "r"(m));
+    return b;
 }
 
+// Writes tag | (index of each set bit of m) to buf[k .. k + n), lowest bit
+// first, where n = popc(m).  The bits are taken highest first and the entries
+// filled from the end, two per round (a lone last bit on its own).
+__device__ __forceinline__ void decode_bits(uint32_t m, uint32_t n, uint32_t tag, uint32_t *buf, uint32_t k)
+{
+    uint32_t *p = buf + k + n;
+    for (; n >= 2; n -= 2) {
+        const uint32_t b0 = top_bit(m);
+        m ^= 1u << b0;
+        const uint32_t b1 = top_bit(m);
+        m ^= 1u << b1;
+        p[-1] = tag | b0;
+        p[-2] = tag | b1;
+        p -= 2;
+    }
+    if (n) p[-1] = tag | top_bit(m);
+}
+
+// Stores one value.  FITS: the caller has shown that every slot of the window
+// is below the capacity; otherwise each slot is checked.
+template <bool FITS>
 __device__ __forceinline__ void put(const sj_join_args &a, uint32_t slot, int32_t val)
 {
-    if (slot < a.capacity) {
+    if (FITS || slot < a.capacity) {
         a.outVal[slot] = val;
     } else {
         atomicMax(&a.stat[3], 1ULL);
+    }
+}
+
+// Copies the window's T staged entries out: entry e goes to slot
+// slotOf(ent[e], e) with value src[srcOf(ent[e])].  Whole rounds of 32 * CO
+// entries issue all their loads before any store; the rest goes 32 at a time,
+// so a window never pays for more than 31 idle lane slots.
+template <bool FITS, class SlotOf, class SrcOf>
+__device__ __forceinline__ void copy_out(const sj_join_args &a, const uint32_t *ent, uint32_t T,
+                                         const uint32_t *__restrict__ src, uint32_t lane, SlotOf slotOf,
+                                         SrcOf srcOf)
+{
+    uint32_t e0 = 0;
+    for (; e0 + 32 * CO <= T; e0 += 32 * CO) {
+        uint32_t slot[CO], pos[CO], val[CO];
+#pragma unroll
+        for (int i = 0; i < CO; i++) {
+            const uint32_t e = e0 + 32 * i + lane;
+            const uint32_t en = ent[e];
+            pos[i] = srcOf(en);
+            slot[i] = slotOf(en, e);
+        }
+#pragma unroll
+        for (int i = 0; i < CO; i++) val[i] = __ldg(src + pos[i]);
+#pragma unroll
+        for (int i = 0; i < CO; i++) put<FITS>(a, slot[i], (int32_t)val[i]);
+    }
+    for (; e0 < T; e0 += 32) {
+        const uint32_t e = e0 + lane;
+        if (e < T) {
+            const uint32_t en = ent[e];
+            put<FITS>(a, slotOf(en, e), (int32_t)__ldg(src + srcOf(en)));
+        }
     }
 }
 
@@ -149,25 +194,28 @@ __device__ __forceinline__ void emit_rows(const sj_join_args &a, const UnitTask 
             __syncwarp();   // the previous window's copy-out is done with ent / base
             // a query's first word: base = its chunk start slot minus its flat prefix
             if (f < nw && f == q * cb) w.base[q] = w.start[q] - (carry + ex);
-            decode_bits(word, (q << 16) | ((f - q * cb) << 5), w.ent, ex);
+            decode_bits(word, cnt, (q << 16) | ((f - q * cb) << 5), w.ent, ex);
             __syncwarp();
-            // copy-out, CO entries per lane at a time: their candidate-id loads
-            // are all issued before any store.  Every entry is valid by
-            // construction (words of queries < nq, bits inside the stream).
-            for (uint32_t e0 = 0; e0 < T; e0 += 32 * CO) {
-                uint32_t slot[CO], pos[CO], val[CO];
-#pragma unroll
-                for (int i = 0; i < CO; i++) {
-                    const uint32_t e = e0 + 32 * i + lane;
-                    const uint32_t ent = w.ent[e < T ? e : 0];
-                    pos[i] = c0 * 32 + (ent & 0xffffu);
-                    slot[i] = w.base[ent >> 16] + carry + e;
-                }
-#pragma unroll
-                for (int i = 0; i < CO; i++) val[i] = __ldg(cid + pos[i]);
-#pragma unroll
-                for (int i = 0; i < CO; i++)
-                    if (e0 + 32 * i + lane < T) put(a, slot[i], (int32_t)val[i]);
+            // copy-out.  Every entry is valid by construction (words of queries
+            // < nq, bits inside the stream).  The window's largest slot is that
+            // of some lane's last entry: base + carry + incl - 1.
+            const uint32_t q0 = __shfl_sync(FULL, q, 0);
+            const uint32_t *const pcid = cid + c0 * 32;
+            const auto srcOf = [](uint32_t en) { return en & 0xffffu; };
+            if (ws - q0 * cb + min(32u, nw - ws) <= cb) {
+                // the whole window is one query's: one base for every entry
+                const uint32_t B = w.base[q0] + carry;
+                const auto slotOf = [B](uint32_t, uint32_t e) { return B + e; };
+                if ((uint64_t)B + T <= a.capacity) copy_out<true>(a, w.ent, T, pcid, lane, slotOf, srcOf);
+                else copy_out<false>(a, w.ent, T, pcid, lane, slotOf, srcOf);
+            } else {
+                const uint32_t *const base = w.base;
+                const uint32_t cy = carry;
+                // lanes past the group's words have no entries (and no query)
+                const bool fits = cnt == 0 || (uint64_t)base[q] + cy + incl <= a.capacity;
+                const auto slotOf = [base, cy](uint32_t en, uint32_t e) { return base[en >> 16] + cy + e; };
+                if (__all_sync(FULL, fits)) copy_out<true>(a, w.ent, T, pcid, lane, slotOf, srcOf);
+                else copy_out<false>(a, w.ent, T, pcid, lane, slotOf, srcOf);
             }
             carry += T;
         }
@@ -215,23 +263,15 @@ __device__ __forceinline__ void emit_cols(const sj_join_args &a, const UnitTask 
         const uint32_t ex = incl - cnt;
         __syncwarp();
         w.base[lane] = slot - ex;   // lane L's entries [ex_L, ex_L + cnt_L) go to slot_L onwards
-        decode_bits(cur, lane << 5, w.ent, ex);
+        decode_bits(cur, cnt, lane << 5, w.ent, ex);
         __syncwarp();
-        for (uint32_t e0 = 0; e0 < T; e0 += 32 * CO) {
-            uint32_t slot[CO], qi[CO], val[CO];
-#pragma unroll
-            for (int i = 0; i < CO; i++) {
-                const uint32_t e = e0 + 32 * i + lane;
-                const uint32_t ent = w.ent[e < T ? e : 0];
-                qi[i] = g * 32 + (ent & 31u);
-                slot[i] = w.base[ent >> 5] + e;
-            }
-#pragma unroll
-            for (int i = 0; i < CO; i++) val[i] = __ldg(qids + qi[i]);
-#pragma unroll
-            for (int i = 0; i < CO; i++)
-                if (e0 + 32 * i + lane < T) put(a, slot[i], (int32_t)val[i]);
-        }
+        const uint32_t *const base = w.base;
+        const auto slotOf = [base](uint32_t en, uint32_t e) { return base[en >> 5] + e; };
+        const auto srcOf = [](uint32_t en) { return en & 31u; };
+        if (__all_sync(FULL, (uint64_t)slot + cnt <= a.capacity))
+            copy_out<true>(a, w.ent, T, qids + g * 32, lane, slotOf, srcOf);
+        else
+            copy_out<false>(a, w.ent, T, qids + g * 32, lane, slotOf, srcOf);
         slot += cnt;
     }
 }

@@ -19,6 +19,10 @@ def _gauss16(n, seed):
 def _cases():
     r = np.random.default_rng
     dup = np.repeat(r(3).random((5, 2)), 700, axis=0)          # five heavy cells, exact duplicates
+    # far outlier in a non-indexed dimension: the FP32 filter's error band grows
+    # with the data's extent there, so nearly every evaluation is refined in FP64
+    outlier = r(11).random((3000, 5))
+    outlier[17, 4] = 3.0e5
     return {
         "uniform2d": (r(1).random((20000, 2)), 0.01, 2),
         "exp2d_dense": (exp_points(30000, 2, 2), 0.002, 2),
@@ -34,6 +38,9 @@ def _cases():
         "lattice2d": (lattice_points(60, 2, 0.1), 0.1, 2),
         "duplicates": (dup, 0.01, 2),
         "single": (np.array([[0.25, 0.5]]), 0.1, 2),
+        # coordinates far from zero (FP32 ulp there exceeds eps / 10)
+        "offset3d": (r(12).random((6000, 3)) * 0.5 + np.array([1.0e4, -2.5e4, 7.0e3]), 0.04, 3),
+        "outlier5d_k2": (outlier, 0.15, 2),
     }
 
 
