@@ -17,16 +17,22 @@
 //
 // Work is cut into warp units that any warp of any CTA takes from a counter:
 //   row unit    (task, group of 32 queries): the group's words of a chunk are
-//               contiguous; a window of 32 words (lane = word; one window
-//               spans several queries when the task has few blocks) is
-//               popcounted and scanned, its set bits are decoded into shared
-//               memory as (query, stream position) entries in slot order, and the warp
-//               copies the entries out: consecutive entries of one query go to
-//               consecutive slots, so the stores are coalesced.
+//               contiguous; a window of 64 words (lane L holds words L and
+//               32 + L; one window spans several queries when the task has
+//               few blocks) is popcounted and scanned (both halves' counts
+//               packed in one 32-bit scan), its set bits are decoded into
+//               shared memory as 16-bit (query, stream position) entries in
+//               slot order, and the warp copies the entries out: consecutive
+//               entries of one query go to consecutive slots, so the stores
+//               are coalesced.
 //   column unit (symmetric task, block of 32 stream positions): lane j is
 //               candidate j; per query group its word is decoded lane-major
 //               and copied out the same way, each lane's run continuing across
 //               groups.
+// A window without any set bit costs one ballot.  Measured on one B200 and
+// not kept: two query groups per column window (c3 emission +5 %), and row
+// windows aligned to one query's words when a chunk has >= 32 blocks (c3
+// +13 %, no gain elsewhere).
 // Only the values are written here: the keys of a batch are its key runs in
 // key order, which sj_expand_keys writes sequentially (the emission's writes
 // land at scattered run positions, which HBM absorbs at a fraction of its
@@ -44,7 +50,7 @@ namespace {
 
 constexpr int EW = 256;             // threads per emission CTA (independent warps)
 constexpr int ENW = EW / 32;
-constexpr int EM_CAP = 1024;        // staged entries per warp: one window of 32 words x 32 bits
+constexpr int EM_CAP = 2048;        // staged entries per warp: one window of 64 words x 32 bits
 constexpr uint32_t FULL = 0xffffffffu;
 #ifndef SJ_EMIT_UNROLL
 #define SJ_EMIT_UNROLL 4
@@ -52,7 +58,7 @@ constexpr uint32_t FULL = 0xffffffffu;
 constexpr int CO = SJ_EMIT_UNROLL;  // copy-out entries per lane whose loads are in flight together
 
 struct WarpSmem {
-    uint32_t ent[EM_CAP];   // staged entries in slot order: rows (query << 16) | chunk position,
+    uint16_t ent[EM_CAP];   // staged entries in slot order: rows (query << 11) | chunk position,
                             // columns (lane << 5) | query bit
     uint32_t base[32];      // slot of entry 0 of the window for each query (rows) / lane (columns)
     uint32_t start[32];     // rows: slot of each query's first pair of the chunk
@@ -79,19 +85,19 @@ __device__ __forceinline__ uint32_t top_bit(uint32_t m)
 // Writes tag | (index of each set bit of m) to buf[k .. k + n), lowest bit
 // first, where n = popc(m).  The bits are taken highest first and the entries
 // filled from the end, two per round (a lone last bit on its own).
-__device__ __forceinline__ void decode_bits(uint32_t m, uint32_t n, uint32_t tag, uint32_t *buf, uint32_t k)
+__device__ __forceinline__ void decode_bits(uint32_t m, uint32_t n, uint32_t tag, uint16_t *buf, uint32_t k)
 {
-    uint32_t *p = buf + k + n;
+    uint16_t *p = buf + k + n;
     for (; n >= 2; n -= 2) {
         const uint32_t b0 = top_bit(m);
         m ^= 1u << b0;
         const uint32_t b1 = top_bit(m);
         m ^= 1u << b1;
-        p[-1] = tag | b0;
-        p[-2] = tag | b1;
+        p[-1] = (uint16_t)(tag | b0);
+        p[-2] = (uint16_t)(tag | b1);
         p -= 2;
     }
-    if (n) p[-1] = tag | top_bit(m);
+    if (n) p[-1] = (uint16_t)(tag | top_bit(m));
 }
 
 // Stores one value.  FITS: the caller has shown that every slot of the window
@@ -111,7 +117,7 @@ __device__ __forceinline__ void put(const sj_join_args &a, uint32_t slot, int32_
 // entries issue all their loads before any store; the rest goes 32 at a time,
 // so a window never pays for more than 31 idle lane slots.
 template <bool FITS, class SlotOf, class SrcOf>
-__device__ __forceinline__ void copy_out(const sj_join_args &a, const uint32_t *ent, uint32_t T,
+__device__ __forceinline__ void copy_out(const sj_join_args &a, const uint16_t *ent, uint32_t T,
                                          const uint32_t *__restrict__ src, uint32_t lane, SlotOf slotOf,
                                          SrcOf srcOf)
 {
@@ -144,6 +150,18 @@ struct UnitTask {
     uint32_t t, qBegin, qc, L;
 };
 
+// Bits of a row word whose block starts at stream position p0 (< L) past the
+// stream end are never set by a consistent count pass: drop them and flag it.
+__device__ __forceinline__ uint32_t stream_checked(const sj_join_args &a, uint32_t word, uint32_t p0, uint32_t L)
+{
+    const uint32_t rem = L - p0;
+    if (rem < 32u && (word >> rem) != 0u) {
+        atomicMax(&a.stat[6], 1ULL);
+        word &= (1u << rem) - 1u;
+    }
+    return word;
+}
+
 // Row unit: queries 32g .. 32g+nq-1 of task u.t (key = query, value = candidate).
 __device__ __forceinline__ void emit_rows(const sj_join_args &a, const UnitTask &u, uint32_t g, WarpSmem &w,
                                           uint32_t lane)
@@ -165,55 +183,65 @@ __device__ __forceinline__ void emit_rows(const sj_join_args &a, const UnitTask 
         const uint32_t cb = min(64u, nBlk - c0);          // blocks of this chunk
         const uint32_t nw = nq * cb;                      // the group's words of this chunk
         const uint32_t *const wq = masks + (uint64_t)c0 * qc + (uint64_t)q0 * cb;
-        // floor(f / cb) = (f * magic) >> 32 for f < 2^11 (error < 2^-21 < 1/cb)
+        const uint32_t *const pcid = cid + c0 * 32;
+        const auto srcOf = [](uint32_t en) { return en & 0x7ffu; };
+        // floor(f / cb) = (f * magic) >> 32 for f < 2^26 (error < 2^-6 <= 1/cb)
         const uint64_t magic = ((1ULL << 32) + cb - 1) / cb;
         __syncwarp();
         w.start[lane] = next;
         uint32_t carry = 0;   // entries of earlier windows of this chunk
-        uint32_t nextWord = lane < nw ? __ldg(wq + lane) : 0u;
-        for (uint32_t ws = 0; ws < nw; ws += 32) {
-            const uint32_t f = ws + lane;
-            uint32_t word = nextWord;
-            // the next window's word is in flight while this one is written
-            nextWord = f + 32 < nw ? __ldg(wq + f + 32) : 0u;
-            const uint32_t q = (uint32_t)(((uint64_t)f * magic) >> 32);
-            {
-                // the word's block must not extend past the stream end: bits
-                // there are never set by a consistent count pass
-                const uint32_t p0 = (c0 + (f - q * cb)) * 32u;
-                const uint32_t valid = p0 >= u.L ? 0u : (u.L - p0 >= 32u ? FULL : (1u << (u.L - p0)) - 1u);
-                if (word & ~valid) {
-                    atomicMax(&a.stat[6], 1ULL);
-                    word &= valid;
-                }
+        // a window is 64 words: lane L holds words L and 32 + L (the next
+        // window's words are in flight while this one is written)
+        uint32_t n0 = lane < nw ? __ldg(wq + lane) : 0u;
+        uint32_t n1 = lane + 32 < nw ? __ldg(wq + lane + 32) : 0u;
+        for (uint32_t ws = 0; ws < nw; ws += 64) {
+            const uint32_t fa = ws + lane, fb = fa + 32;
+            uint32_t wa = n0, wb = n1;
+            n0 = fa + 64 < nw ? __ldg(wq + fa + 64) : 0u;
+            n1 = fb + 64 < nw ? __ldg(wq + fb + 64) : 0u;
+            const uint32_t qa = (uint32_t)(((uint64_t)fa * magic) >> 32);
+            const uint32_t qb = (uint32_t)(((uint64_t)fb * magic) >> 32);
+            const uint32_t ra = fa - qa * cb, rb = fb - qb * cb;   // block of each word in the chunk
+            // words past the group's end are zero; a word's block is inside the stream
+            if (wa) wa = stream_checked(a, wa, (c0 + ra) * 32u, u.L);
+            if (wb) wb = stream_checked(a, wb, (c0 + rb) * 32u, u.L);
+            const uint32_t ca = __popc(wa), cbt = __popc(wb);
+            if (__ballot_sync(FULL, ca | cbt) == 0) {
+                // no pair in the window: only the bases of queries that start in it
+                __syncwarp();
+                if (fa < nw && ra == 0) w.base[qa] = w.start[qa] - carry;
+                if (fb < nw && rb == 0) w.base[qb] = w.start[qb] - carry;
+                continue;
             }
-            const uint32_t cnt = __popc(word);
-            const uint32_t incl = warp_incl_scan(cnt, lane);
-            const uint32_t T = __shfl_sync(FULL, incl, 31);
-            const uint32_t ex = incl - cnt;
+            // one scan of both halves' counts (each total <= 1024 fits 16 bits):
+            // word fa's entries start at exA, word fb's at TA + exB
+            const uint32_t incl = warp_incl_scan(ca | (cbt << 16), lane);
+            const uint32_t tot = __shfl_sync(FULL, incl, 31);
+            const uint32_t TA = tot & 0xffffu, T = TA + (tot >> 16);
+            const uint32_t exA = (incl & 0xffffu) - ca, exB = TA + (incl >> 16) - cbt;
             __syncwarp();   // the previous window's copy-out is done with ent / base
             // a query's first word: base = its chunk start slot minus its flat prefix
-            if (f < nw && f == q * cb) w.base[q] = w.start[q] - (carry + ex);
-            decode_bits(word, cnt, (q << 16) | ((f - q * cb) << 5), w.ent, ex);
+            if (fa < nw && ra == 0) w.base[qa] = w.start[qa] - (carry + exA);
+            if (fb < nw && rb == 0) w.base[qb] = w.start[qb] - (carry + exB);
+            decode_bits(wa, ca, (qa << 11) | (ra << 5), w.ent, exA);
+            decode_bits(wb, cbt, (qb << 11) | (rb << 5), w.ent, exB);
             __syncwarp();
             // copy-out.  Every entry is valid by construction (words of queries
-            // < nq, bits inside the stream).  The window's largest slot is that
-            // of some lane's last entry: base + carry + incl - 1.
-            const uint32_t q0 = __shfl_sync(FULL, q, 0);
-            const uint32_t *const pcid = cid + c0 * 32;
-            const auto srcOf = [](uint32_t en) { return en & 0xffffu; };
-            if (ws - q0 * cb + min(32u, nw - ws) <= cb) {
+            // < nq, bits inside the stream).
+            const uint32_t qf = __shfl_sync(FULL, qa, 0);
+            if (ws - qf * cb + min(64u, nw - ws) <= cb) {
                 // the whole window is one query's: one base for every entry
-                const uint32_t B = w.base[q0] + carry;
+                const uint32_t B = w.base[qf] + carry;
                 const auto slotOf = [B](uint32_t, uint32_t e) { return B + e; };
                 if ((uint64_t)B + T <= a.capacity) copy_out<true>(a, w.ent, T, pcid, lane, slotOf, srcOf);
                 else copy_out<false>(a, w.ent, T, pcid, lane, slotOf, srcOf);
             } else {
                 const uint32_t *const base = w.base;
                 const uint32_t cy = carry;
-                // lanes past the group's words have no entries (and no query)
-                const bool fits = cnt == 0 || (uint64_t)base[q] + cy + incl <= a.capacity;
-                const auto slotOf = [base, cy](uint32_t en, uint32_t e) { return base[en >> 16] + cy + e; };
+                // each word's last entry has the largest slot of its run
+                const bool fits = (ca == 0 || (uint64_t)base[qa] + cy + exA + ca <= a.capacity) &&
+                                  (cbt == 0 || (uint64_t)base[qb] + cy + exB + cbt <= a.capacity);
+                const auto slotOf = [base, cy](uint32_t en, uint32_t e) { return base[en >> 11] + cy + e; };
                 if (__all_sync(FULL, fits)) copy_out<true>(a, w.ent, T, pcid, lane, slotOf, srcOf);
                 else copy_out<false>(a, w.ent, T, pcid, lane, slotOf, srcOf);
             }
@@ -227,7 +255,7 @@ __device__ __forceinline__ void emit_rows(const sj_join_args &a, const UnitTask 
 }
 
 // Column unit: stream positions 32b .. 32b+31 of symmetric task u.t (key =
-// candidate, value = query).
+// candidate, value = query).  A window is one query group: lane j's word of it.
 __device__ __forceinline__ void emit_cols(const sj_join_args &a, const UnitTask &u, uint32_t b, WarpSmem &w,
                                           uint32_t lane)
 {
@@ -245,7 +273,7 @@ __device__ __forceinline__ void emit_cols(const sj_join_args &a, const UnitTask 
     uint32_t word = __ldg(cw);
     for (uint32_t g = 0; g < nG; g++) {
         uint32_t cur = word;
-        if (g + 1 < nG) word = __ldg(cw + (g + 1) * 32);
+        if (g + 1 < nG) word = __ldg(cw + (g + 1) * 32);   // in flight while this group is written
         {
             // positions past the stream end and queries past the tile have no
             // bits in a consistent count pass
@@ -257,9 +285,9 @@ __device__ __forceinline__ void emit_cols(const sj_join_args &a, const UnitTask 
             }
         }
         const uint32_t cnt = __popc(cur);
+        if (__ballot_sync(FULL, cnt) == 0) continue;   // warp-uniform
         const uint32_t incl = warp_incl_scan(cnt, lane);
         const uint32_t T = __shfl_sync(FULL, incl, 31);
-        if (T == 0) continue;   // warp-uniform
         const uint32_t ex = incl - cnt;
         __syncwarp();
         w.base[lane] = slot - ex;   // lane L's entries [ex_L, ex_L + cnt_L) go to slot_L onwards
