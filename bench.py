@@ -128,9 +128,20 @@ def combine_ranks(ms, pairs, pair_hash, device):
     return float(t.item()), int(v[0].item()), int(v[1].item()) % (1 << 64)
 
 
+def host_threads() -> int:
+    """Host CPUs this process may run on.  Passed to the oracle explicitly:
+    torchrun sets OMP_NUM_THREADS=1 in every rank, which would otherwise leave
+    the CPU legs on one thread."""
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
 def cpu_oracle_rate(pts, eps, k, target_s=12.0, threads=0):
     """Oracle grid join on a bounded sample of query points: (pairs/s, cores, sample text)."""
     import oracle
+    threads = threads or host_threads()
     ix = oracle.OracleIndex(pts, eps, k)
     n = len(pts)
     stride = max(1, n // 2000)
@@ -142,14 +153,13 @@ def cpu_oracle_rate(pts, eps, k, target_s=12.0, threads=0):
         t0 = time.perf_counter()
         P, _, E = ix.stats(qstride=stride, threads=threads)
         dt = time.perf_counter() - t0
-    cores = threads or oracle.num_threads()
+    cores = threads
     nq = (n + stride - 1) // stride
     sample = f"every {stride}th query point ({nq} of {n}), full stencil, {E} candidate evaluations, {dt:.1f} s"
     return P / dt, cores, sample, dt
 
 
 def run_reference(args):
-    import oracle
     import sjoin
     ws, rank, _ = _dist()
     if rank != 0:
