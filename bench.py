@@ -198,11 +198,24 @@ def _config(args, spec):
     }
 
 
+def rank_host_threads() -> int:
+    """Host threads for one rank's engine (task preparation, host key
+    expansion): every usable CPU in a single process, an equal share of them
+    per rank under torchrun (which sets OMP_NUM_THREADS=1 in its ranks)."""
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    if ws <= 1:
+        return host_threads()
+    local_ws = int(os.environ.get("LOCAL_WORLD_SIZE", str(ws)))
+    return max(1, host_threads() // max(1, local_ws))
+
+
 def run_ours(args):
     import torch
 
     import sjoin
     ws, rank, local = _dist()
+    # the engine's OpenMP regions start on this thread and share torch's OpenMP runtime
+    torch.set_num_threads(rank_host_threads())
     torch.cuda.set_device(local)
     if ws > 1:
         import datetime
@@ -318,7 +331,7 @@ def run_ours(args):
     pipe_tflops = NUM_SM * lanes * 2 * mhz * 1e6 / 1e12
     dist_tflops = (3 * spec["D"] * s["distance_calcs"]) / (s["ms_count"] / 1e3) / 1e12 if s["ms_count"] > 0 else None
     cpu = None
-    if not args.no_cpu:
+    if not args.no_cpu and ws == 1:   # the CPU baseline is rank 0's at N = 1 only
         rate, cores, sample, _ = cpu_oracle_rate(pts, eps, k, target_s=args.cpu_seconds)
         cpu = {"value": rate, "unit": "pairs/s", "cores": cores, "kind": "port", "sample": sample}
     line = {
@@ -338,6 +351,7 @@ def run_ours(args):
                                    "peak_kind": "nominal lanes x sampled SM clock",
                                    "flops_per_candidate": 3 * spec["D"]},
         "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clocks,
+        "host_threads_per_rank": rank_host_threads(),
         "phases_ms": {k2: round(s[k2], 3) for k2 in ("ms_index", "ms_tasks", "ms_estimate", "ms_count", "ms_scan",
                                                      "ms_fill", "ms_expand", "ms_deliver", "ms_total")},
         "batches": s["num_batches"], "overflow_retries": s["overflow_retries"],

@@ -51,3 +51,18 @@ def test_reference_arm_under_torchrun_two_ranks():
     lines = _lines(r.stdout)
     assert len(lines) == 1          # rank 0 alone runs and prints
     _check(lines[0], 2)
+
+
+def test_rank_host_threads_share(monkeypatch):
+    # one process: every usable CPU; torchrun ranks on one node: an equal share
+    sys.path.insert(0, REPO)
+    import bench
+    n = _threads()
+    for var in ("WORLD_SIZE", "LOCAL_WORLD_SIZE"):
+        monkeypatch.delenv(var, raising=False)
+    assert bench.rank_host_threads() == n
+    monkeypatch.setenv("WORLD_SIZE", "4")
+    monkeypatch.setenv("LOCAL_WORLD_SIZE", "4")
+    assert bench.rank_host_threads() == max(1, n // 4)
+    monkeypatch.setenv("LOCAL_WORLD_SIZE", str(4 * n))
+    assert bench.rank_host_threads() == 1
