@@ -213,6 +213,10 @@ struct Ctx {
     std::vector<uint64_t> hMaskOff, hColOff, hRowOff, hCandOff, hUnitOff;
     DevBuf<uint64_t> dMaskOff, dColOff, dRowOff, dCandOff, dUnitOff;
     DevBuf<uint32_t> masks, colMasks, rowRel, candId, candRel;
+    // the count pass of batch i + 1 writes this second record set while the
+    // emission of batch i reads the first (device-fold pipeline)
+    DevBuf<uint32_t> masks2, colMasks2, rowRel2, candId2, candRel2;
+    DevBuf<uint32_t> emitHead;   // the emission's work counter when it runs beside a count pass
     // device CSR neighbour table under construction (sj_neighbor_csr): the
     // caller's arrays and the rows' fill cursors
     uint64_t *csrRowPtr = nullptr;
@@ -704,10 +708,11 @@ struct BatchRange {
     uint32_t t0, t1;
 };
 
-sj_status run_count(Ctx &c, sj_join_args &a, bool queue)
+sj_status run_count(Ctx &c, sj_join_args &a, bool queue, cudaStream_t st = nullptr)
 {
-    if (queue) CK(cudaMemsetAsync(c.queueHead.p, 0, sizeof(uint32_t), c.s));
-    CK(sj_launch_join(a, c.g, c.p.precision == SJ_PREC_FP32_REFINE ? 1 : 0, queue ? 1 : 0, c.numSM, c.s));
+    if (!st) st = c.s;
+    if (queue) CK(cudaMemsetAsync(c.queueHead.p, 0, sizeof(uint32_t), st));
+    CK(sj_launch_join(a, c.g, c.p.precision == SJ_PREC_FP32_REFINE ? 1 : 0, queue ? 1 : 0, c.numSM, st));
     return SJ_OK;
 }
 
@@ -866,13 +871,14 @@ sj_status replan_exact(const BatchRange &br, const std::vector<uint32_t> &taskHi
 }
 
 // Key array of the current batch (a.outKey, a.capacity) from keyStart.
-sj_status expand_keys(Ctx &c, const sj_join_args &a)
+sj_status expand_keys(Ctx &c, const sj_join_args &a, cudaStream_t st = nullptr)
 {
+    if (!st) st = c.s;
     const size_t slots = sj_expand_long_slots(a.capacity);
     CK(c.longRuns.ensure(slots));
     CK(c.longCount.ensure(1));
     CK(sj_expand_keys(a.keyStart, c.total.p, c.n, a.outKey, a.batchPairs, a.capacity, c.longRuns.p,
-                      (uint32_t)std::min<size_t>(c.longRuns.n, 0xffffffffu), c.longCount.p, c.numSM, c.s));
+                      (uint32_t)std::min<size_t>(c.longRuns.n, 0xffffffffu), c.longCount.p, c.numSM, st));
     return SJ_OK;
 }
 
@@ -1020,7 +1026,42 @@ sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
         a.outVal = c.outVal.p;
         a.capacity = bufCap;
         const size_t nplan = plan.size();
-        while (c.events.size() < 6 * nplan) {
+        // Two streams when the device has room for a second record set: the
+        // count pass and scan of each batch on the engine's stream, its key
+        // expansion, emission and fold on the second stream, so batch i + 1's
+        // count pass runs beside batch i's emission (and the launch tails of
+        // each stage fill with the other's work).  Batch i + 1's scan waits
+        // for batch i's emission: both use keyStart and the scan total.
+        bool pipe = nplan > 1;
+        if (pipe) {
+            cudaError_t e = c.masks2.ensure(maxMaskWords);
+            if (e == cudaSuccess) e = c.colMasks2.ensure(maxColWords);
+            if (e == cudaSuccess) e = c.rowRel2.ensure(maxRowWords);
+            if (e == cudaSuccess) e = c.candId2.ensure(maxCandRecs);
+            if (e == cudaSuccess) e = c.candRel2.ensure(maxCandRecs);
+            if (e == cudaSuccess) e = c.emitHead.ensure(1);
+            if (e != cudaSuccess) {
+                // no room for the second set: the batches run one after another
+                cudaGetLastError();
+                c.masks2.release();
+                c.colMasks2.release();
+                c.rowRel2.release();
+                c.candId2.release();
+                c.candRel2.release();
+                pipe = false;
+            }
+        }
+        cudaStream_t sA = c.s, sB = pipe ? c.cs : c.s;
+        // the second stream's work is waited for on every way out
+        struct Drain {
+            cudaStream_t s;
+            ~Drain()
+            {
+                if (s) cudaStreamSynchronize(s);
+            }
+        } drain{pipe ? sB : nullptr};
+        constexpr int EV = 8;   // events per batch
+        while (c.events.size() < EV * nplan) {
             cudaEvent_t e;
             CK(cudaEventCreate(&e));
             c.events.push_back(e);
@@ -1028,39 +1069,57 @@ sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
         cudaEvent_t *ev = c.events.data();
         for (size_t i = 0; i < nplan; i++) {
             const BatchRange &br = plan[nplan - 1 - i];   // plan is stored as a stack
-            a.taskBegin = br.t0;
-            a.taskEnd = br.t1;
-            a.batchPairs = c.batchTot.p + i;
-            CK(cudaEventRecord(ev[6 * i + 0], c.s));
-            CKS(run_count(c, a, queue));
-            CK(cudaEventRecord(ev[6 * i + 1], c.s));
-            CK(sj_exclusive_scan_u32_clear(c.keyCount.p, c.keyStart.p, n, c.scanTemp.p, c.total.p, c.s));
-            CK(cudaEventRecord(ev[6 * i + 2], c.s));
-            CKS(expand_keys(c, a));
-            CK(cudaEventRecord(ev[6 * i + 3], c.s));
-            CK(cudaMemsetAsync(c.queueHead.p, 0, sizeof(uint32_t), c.s));
-            CK(sj_launch_emit(a, c.numSM, c.s));
-            CK(cudaEventRecord(ev[6 * i + 4], c.s));
-            CK(sj_hash_pairs_dev(c.outKey.p, c.outVal.p, a.batchPairs, bufCap, bufCap, c.stat.p + 4, c.s));
-            CK(cudaEventRecord(ev[6 * i + 5], c.s));
+            cudaEvent_t *e = ev + EV * i;
+            sj_join_args b = a;
+            b.taskBegin = br.t0;
+            b.taskEnd = br.t1;
+            b.batchPairs = c.batchTot.p + i;
+            if (pipe && (i & 1)) {
+                b.masks = c.masks2.p;
+                b.colMasks = c.colMasks2.p;
+                b.rowRel = c.rowRel2.p;
+                b.candId = c.candId2.p;
+                b.candRel = c.candRel2.p;
+            }
+            CK(cudaEventRecord(e[0], sA));
+            CKS(run_count(c, b, queue, sA));
+            CK(cudaEventRecord(e[1], sA));
+            if (pipe && i > 0) CK(cudaStreamWaitEvent(sA, ev[EV * (i - 1) + 6], 0));   // previous emission done
+            CK(cudaEventRecord(e[2], sA));
+            CK(sj_exclusive_scan_u32_clear(c.keyCount.p, c.keyStart.p, n, c.scanTemp.p, c.total.p, sA));
+            CK(cudaEventRecord(e[3], sA));
+            if (pipe) CK(cudaStreamWaitEvent(sB, e[3], 0));
+            CK(cudaEventRecord(e[4], sB));
+            CKS(expand_keys(c, b, sB));
+            CK(cudaEventRecord(e[5], sB));
+            b.queueHead = pipe ? c.emitHead.p : c.queueHead.p;
+            CK(cudaMemsetAsync(b.queueHead, 0, sizeof(uint32_t), sB));
+            CK(sj_launch_emit(b, c.numSM, sB));
+            CK(cudaEventRecord(e[6], sB));
+            CK(sj_hash_pairs_dev(c.outKey.p, c.outVal.p, b.batchPairs, bufCap, bufCap, c.stat.p + 4, sB));
+            CK(cudaEventRecord(e[7], sB));
         }
+        if (pipe) CK(cudaStreamWaitEvent(sA, ev[EV * (nplan - 1) + 7], 0));
         std::vector<unsigned long long> tot(nplan);
         CK(cudaMemcpyAsync(tot.data(), c.batchTot.p, sizeof(unsigned long long) * nplan, cudaMemcpyDeviceToHost,
                            c.s));
         CK(cudaMemcpyAsync(hTaskHits.data(), c.taskHits.p, sizeof(uint32_t) * nt, cudaMemcpyDeviceToHost, c.s));
         CK(cudaStreamSynchronize(c.s));
+        // stage times per batch (with two streams, each stage's time includes
+        // sharing the device with the other stream's stage)
         for (size_t i = 0; i < nplan; i++) {
-            float t01, t12, t23, t34, t45;
-            cudaEventElapsedTime(&t01, ev[6 * i + 0], ev[6 * i + 1]);
-            cudaEventElapsedTime(&t12, ev[6 * i + 1], ev[6 * i + 2]);
-            cudaEventElapsedTime(&t23, ev[6 * i + 2], ev[6 * i + 3]);
-            cudaEventElapsedTime(&t34, ev[6 * i + 3], ev[6 * i + 4]);
-            cudaEventElapsedTime(&t45, ev[6 * i + 4], ev[6 * i + 5]);
-            msCount += t01;
-            msScan += t12;
-            msExpand += t23;
-            msFill += t34;
-            msDeliver += t45;
+            const cudaEvent_t *e = ev + EV * i;
+            float tc, ts, tx, tf, th;
+            cudaEventElapsedTime(&tc, e[0], e[1]);
+            cudaEventElapsedTime(&ts, e[2], e[3]);
+            cudaEventElapsedTime(&tx, e[4], e[5]);
+            cudaEventElapsedTime(&tf, e[5], e[6]);
+            cudaEventElapsedTime(&th, e[6], e[7]);
+            msCount += tc;
+            msScan += ts;
+            msExpand += tx;
+            msFill += tf;
+            msDeliver += th;
         }
         std::vector<BatchRange> redo;
         for (size_t i = 0; i < nplan; i++) {
