@@ -31,9 +31,6 @@
 
 #include <atomic>
 
-#ifndef SJ_PUSH_SIGN
-#define SJ_PUSH_SIGN 1      // sign-bit packing: 1 inline funnel shift, 2 shift+or, 0 intrinsic
-#endif
 #ifndef SJ_EVAL_UNROLL
 #define SJ_EVAL_UNROLL 2    // unrolling of the per-block candidate loop
 #endif
@@ -96,15 +93,9 @@ struct StageOf<DP, true> { using T = Stage32<DP>; };
 // inspected as a float, so no comparison is generated)
 __device__ __forceinline__ uint32_t push_sign(uint32_t mask, float v)
 {
-#if SJ_PUSH_SIGN == 1
     uint32_t r;
     asm("shf.l.wrap.b32 %0, %1, %2, 1;" : "=r"(r) : "r"(__float_as_uint(v)), "r"(mask));
     return r;
-#elif SJ_PUSH_SIGN == 2
-    return (mask << 1) | (__float_as_uint(v) >> 31);
-#else
-    return __funnelshift_l(__float_as_uint(v), mask, 1);
-#endif
 }
 
 // FP32 filter over one block of 32 staged candidates for slots 0..RR-1.
