@@ -30,14 +30,11 @@ import statistics
 import subprocess
 import sys
 import tempfile
-import threading
 import time
 
 REPO = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, REPO)
 sys.path.insert(0, os.path.join(REPO, "self-join-hpbdc2019_b200"))
-
-import numpy as np  # noqa: E402
 
 # dram__bytes_read.sum + dram__bytes_write.sum per output pair of the emission
 # kernel (k_emit): 31.4 MB read + 115.2 MB written for a batch of ~28.8 M pairs

@@ -7,8 +7,6 @@ import os
 import re
 import subprocess
 
-import pytest
-
 import sjoin
 
 REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))

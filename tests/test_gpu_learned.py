@@ -14,7 +14,6 @@ On a 6-D exponential set the trained network must
 """
 import os
 
-import numpy as np
 import pytest
 
 import sjoin
