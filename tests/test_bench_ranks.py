@@ -36,7 +36,7 @@ def _rank(rank, port, out):
 
 def test_combine_ranks_two_gloo_ranks():
     port = _free_port()
-    with mp.Manager() as m:
+    with mp.get_context("spawn").Manager() as m:   # no fork of this (threaded) process
         out = m.dict()
         mp.spawn(_rank, args=(port, out), nprocs=2, join=True)
         res = dict(out)
