@@ -178,8 +178,10 @@ sj_status sj_neighbor_csr(void *ctx, uint64_t *rowPtr, int32_t *cols, uint64_t c
 
 sj_status sj_get_stats(void *ctx, sj_stats *st);
 
-/* The CUDA stream (cudaStream_t) all of this context's work is ordered on, so
- * a caller can record events around sj_build_index / sj_join. */
+/* The CUDA stream (cudaStream_t) this context's work is ordered on, so a
+ * caller can record events around sj_build_index / sj_join.  Work the join runs
+ * on its internal second stream is joined back into this one before sj_join
+ * returns. */
 sj_status sj_get_stream(void *ctx, void **stream);
 
 /* Learned estimator.  Weights: SJ_MLP_NPARAM floats laid out W1[16x64], b1[64],
