@@ -223,7 +223,12 @@ sj_status sj_mlp_forward(const float *x, uint32_t m, const float *w, float *out,
  * before any stream capture begins.  All calls on a device share the one
  * array: calls whose work overlaps on the GPU (different streams, or
  * different threads on one device) race and corrupt each other's results, so
- * order them on one stream or serialise them. */
+ * order them on one stream or serialise them.  The array's address is looked
+ * up once per device and kept for the life of the process: after
+ * cudaDeviceReset on a device, this entry point must not be called on it
+ * again.  A CUDA error still pending from earlier work on the calling thread
+ * makes the call return SJ_ERR_CUDA without launching (the error is left for
+ * its owner to read). */
 #define SJ_MLP_NOALLOC_MAX_SAMPLES 8192
 sj_status sj_mlp_loss_grad_noalloc(const float *x, const float *y, uint32_t m, const float *w, float *loss,
                                    float *grad, void *stream);

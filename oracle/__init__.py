@@ -46,6 +46,7 @@ def lib():
         L.orc_index_export.argtypes = [vp, vp, vp, vp, vp, vp]
         L.orc_join_stats.argtypes = [vp, C.c_int, i64, i64, i64, C.c_int, u64p, u64p, u64p]
         L.orc_join_degrees.argtypes = [vp, C.c_int, C.c_int, vp]
+        L.orc_query_rows.argtypes = [vp, C.c_int, vp, i64, C.c_int, vp, vp, vp, vp, i64]
         L.orc_join_pairs.restype = i64
         L.orc_join_pairs.argtypes = [vp, C.c_int, vp, vp, i64]
         L.orc_brute_pairs.restype = i64
@@ -133,6 +134,25 @@ class OracleIndex:
         deg = np.zeros(self.n, np.uint32)
         lib().orc_join_degrees(self._h, fma_mode, threads, _ptr(deg))
         return deg
+
+    def query_rows(self, qids, fma_mode=1, threads=0, values=False):
+        """Neighbour-table rows of the query ids `qids`: (degrees uint32, row set
+        hashes uint64) and, with values=True, the rows' values as a list of
+        sorted int32 arrays."""
+        q = np.ascontiguousarray(qids, dtype=np.int64)
+        deg = np.zeros(len(q), np.uint32)
+        hs = np.zeros(len(q), np.uint64)
+        lib().orc_query_rows(self._h, fma_mode, _ptr(q), len(q), threads, _ptr(deg), _ptr(hs), None, None, 0)
+        if not values:
+            return deg, hs
+        off = np.zeros(len(q) + 1, np.int64)
+        off[1:] = np.cumsum(deg, dtype=np.int64)
+        vals = np.zeros(max(int(off[-1]), 1), np.int32)
+        deg2 = np.zeros(len(q), np.uint32)
+        r = lib().orc_query_rows(self._h, fma_mode, _ptr(q), len(q), threads, _ptr(deg2), None, _ptr(off),
+                                 _ptr(vals), len(vals))
+        assert r == 0 and np.array_equal(deg, deg2)
+        return deg, hs, [np.sort(vals[off[i]:off[i + 1]]) for i in range(len(q))]
 
     def pairs(self, fma_mode=1):
         """All pairs sorted by (key, value) as two int32 arrays."""

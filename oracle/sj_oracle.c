@@ -7,7 +7,7 @@
  *
  * Parity pin: the reference ships no tests, golden vectors or known-answer
  * cases.  This restatement is pinned against outputs of the reference itself,
- * built by oracle/build_ref.sh from its own sources into oracle/_ref and run on
+ * built by oracle/build_ref.py from its own sources into oracle/_ref and run on
  * a B200; the resulting pair sets are committed as fixtures under
  * tests/golden/ (see tests/golden/make_golden.py).
  *
@@ -400,6 +400,54 @@ int orc_join_degrees(const orc_index *ix, int fma_mode, int nthreads, uint32_t *
         free(nb);
     }
     return 0;
+}
+
+/* Rows of the neighbour table for the query ids qids[0..nq): per query its
+ * degree and the set hash of its row (sum of orc_pair_hash(query, value)).
+ * With off != NULL and vals != NULL, row i's values (unsorted) are also
+ * written to vals[off[i] .. off[i] + deg[i]) when that fits below cap (rows
+ * that do not fit leave deg[i] correct and set the return value to 1). */
+int orc_query_rows(const orc_index *ix, int fma_mode, const int64_t *qids, int64_t nq, int nthreads,
+                   uint32_t *deg, uint64_t *rowHash, const int64_t *off, int32_t *vals, int64_t cap)
+{
+    const int D = ix->g.D;
+    const double eps = ix->g.eps;
+    const double *pts = ix->pts;
+    int64_t scap = orc_stencil_cap(ix->g.k);
+    int overflow = 0;
+#ifdef _OPENMP
+    if (nthreads < 1) nthreads = omp_get_max_threads();
+#pragma omp parallel num_threads(nthreads) reduction(| : overflow)
+#endif
+    {
+        int64_t *nb = malloc(sizeof(int64_t) * (size_t)scap);
+#ifdef _OPENMP
+#pragma omp for schedule(dynamic, 4)
+#endif
+        for (int64_t i = 0; i < nq; i++) {
+            const int64_t p = qids[i];
+            const double *qp = pts + p * D;
+            int m = orc_stencil(ix, ix->pointCell[p], nb);
+            uint32_t d = 0;
+            uint64_t h = 0;
+            for (int b = 0; b < m; b++)
+                for (int32_t s = ix->cellMin[nb[b]]; s <= ix->cellMax[nb[b]]; s++) {
+                    const uint32_t q = ix->lookup[s];
+                    if (orc_within(orc_dist2(pts + (int64_t)q * D, qp, D, fma_mode), eps)) {
+                        if (off && vals) {
+                            if (off[i] + (int64_t)d < cap) vals[off[i] + d] = (int32_t)q;
+                            else overflow = 1;
+                        }
+                        d++;
+                        h += orc_pair_hash((int32_t)p, (int32_t)q);
+                    }
+                }
+            deg[i] = d;
+            if (rowHash) rowHash[i] = h;
+        }
+        free(nb);
+    }
+    return overflow;
 }
 
 static int orc_i32_cmp(const void *a, const void *b)

@@ -1096,7 +1096,7 @@ sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
             CK(cudaMemsetAsync(b.queueHead, 0, sizeof(uint32_t), sB));
             CK(sj_launch_emit(b, c.numSM, sB));
             CK(cudaEventRecord(e[6], sB));
-            CK(sj_hash_pairs_dev(c.outKey.p, c.outVal.p, b.batchPairs, bufCap, bufCap, c.stat.p + 4, sB));
+            CK(sj_hash_pairs_dev(c.outKey.p, c.outVal.p, b.batchPairs, bufCap, bufCap, c.numSM, c.stat.p + 4, sB));
             CK(cudaEventRecord(e[7], sB));
         }
         if (pipe) CK(cudaStreamWaitEvent(sA, ev[EV * (nplan - 1) + 7], 0));

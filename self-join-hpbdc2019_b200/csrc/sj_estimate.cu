@@ -293,6 +293,13 @@ extern "C" sj_status sj_mlp_loss_grad_noalloc(const float *x, const float *y, ui
         }
         scratch = g_noallocScratchPtr[dev];
     }
+    // an error left pending by earlier work on this thread is reported, not consumed,
+    // so the error checks after the launches below see this call's launches only
+    e = cudaPeekAtLastError();
+    if (e != cudaSuccess) {
+        sj_set_error_message("sj_mlp_loss_grad_noalloc: a CUDA error from earlier work is pending");
+        return SJ_ERR_CUDA;
+    }
     cudaStream_t s = (cudaStream_t)stream;
     float *H1 = scratch, *G1 = H1 + (size_t)m * SJ_HID, *H2 = G1 + (size_t)m * SJ_HID, *G2 = H2 + (size_t)m * SJ_HID,
           *G3 = G2 + (size_t)m * SJ_HID;
@@ -302,6 +309,9 @@ extern "C" sj_status sj_mlp_loss_grad_noalloc(const float *x, const float *y, ui
     if (e == cudaSuccess) {
         k_mlp_backprop<<<(m + 127) / 128, 128, 0, s>>>(x, y, m, w, H1, G1, H2, G2, G3, loss);
         sj_note_launch();
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) {
         k_mlp_wgrad<<<(NP + 255) / 256, 256, 0, s>>>(x, H1, H2, G1, G2, G3, m, grad);
         sj_note_launch();
         e = cudaGetLastError();

@@ -139,7 +139,7 @@ cudaError_t sj_hash_pairs(const int32_t *key, const int32_t *val, uint64_t m,
                           unsigned long long *hashOut, cudaStream_t s);
 // same, with the pair count read on the device (skipped when it exceeds cap)
 cudaError_t sj_hash_pairs_dev(const int32_t *key, const int32_t *val, const unsigned long long *count, uint64_t cap,
-                              uint64_t gridHint, unsigned long long *hashOut, cudaStream_t s);
+                              uint64_t gridHint, int numSM, unsigned long long *hashOut, cudaStream_t s);
 
 // keys of a batch from its row structure: key k owns [excl[k], excl[k+1])
 // (excl[n] = *total); skipped when the batch's count exceeds cap.  longRuns

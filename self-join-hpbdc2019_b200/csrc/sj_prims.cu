@@ -440,10 +440,10 @@ __global__ void __launch_bounds__(256) k_csr_append(const uint32_t *__restrict__
 }  // namespace
 
 cudaError_t sj_hash_pairs_dev(const int32_t *key, const int32_t *val, const unsigned long long *count, uint64_t cap,
-                              uint64_t gridHint, unsigned long long *hashOut, cudaStream_t s)
+                              uint64_t gridHint, int numSM, unsigned long long *hashOut, cudaStream_t s)
 {
     uint64_t blocks = ceil_div(gridHint ? gridHint : 1, 256 * 16);
-    if (blocks > 148 * 8) blocks = 148 * 8;
+    if (blocks > (uint64_t)numSM * 8) blocks = (uint64_t)numSM * 8;
     if (blocks == 0) blocks = 1;
     k_hash_pairs_dev<<<(unsigned)blocks, 256, 0, s>>>(key, val, count, cap, hashOut);
     sj_note_launch();

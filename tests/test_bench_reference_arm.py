@@ -9,7 +9,8 @@ import subprocess
 import sys
 
 REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-ARGS = ["--impl", "reference", "--workload", "c1", "--steps", "1", "--warmup", "0", "--ref-seconds", "0.5"]
+ARGS = ["--impl", "reference", "--workload", "c1", "--steps", "1", "--warmup", "0", "--ref-seconds", "0.5",
+        "--no-ref-cuda"]
 
 
 def _threads():

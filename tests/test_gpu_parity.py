@@ -110,6 +110,22 @@ def test_multi_batch_with_overflow_retries(mode, prec):
     assert st.num_batches == len(batches)
 
 
+@pytest.mark.parametrize("prec", [sjoin.PREC_FP64, sjoin.PREC_FP32_REFINE])
+@pytest.mark.parametrize("mode", [5, 10])
+def test_device_fold_pipeline_with_overflow_retries(mode, prec):
+    # on-device delivery runs every batch back to back on two streams and
+    # re-plans the batches whose count exceeds the buffer: alpha 0 and a tiny
+    # sample make underestimates certain at this capacity
+    pts, eps, k, ix, (ok, ov) = _oracle_pairs("exp2d_dense")
+    with sjoin.SelfJoin(2, eps, mode=mode, precision=prec, capacity=65536, alpha=0.0,
+                        sample_rate=0.002) as sj:
+        sj.set_points(pts)
+        sj.build_index()
+        st = sj.join(sjoin.DELIVER_NONE)
+    assert st.num_batches >= 2 and st.overflow_retries > 0
+    assert st.total_pairs == len(ok) and st.pair_hash == oracle.hash_pairs(ok, ov)
+
+
 def test_full_stencil_batches_hold_complete_rows():
     # with the full stencil every key is produced by one task's query tile, and
     # the count pass places all of a key's values together
