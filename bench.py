@@ -262,6 +262,8 @@ def _config(args, spec, prec, learned):
 def _spec_and_prec(args):
     import sjoin
     spec = dict(sjoin.datasets.WORKLOADS[args.workload])
+    if getattr(args, "mode", None) is not None:
+        spec["mode"] = args.mode
     prec = spec["precision"] if args.precision is None else args.precision
     learned = args.scheduler == "learned" if args.scheduler else (args.workload == "c4" and prec == 1)
     return spec, prec, learned
@@ -273,6 +275,8 @@ def run_reference(args):
     if rank != 0:
         return
     pts, eps, k, spec = sjoin.datasets.make(args.workload, n=args.n)
+    if args.mode is not None:
+        spec["mode"] = args.mode
     _, prec, learned = _spec_and_prec(args)
     times, rates = [], []
     for i in range(args.warmup + args.steps):
@@ -346,6 +350,8 @@ def run_ours(args):
     pts, eps, k, spec = sjoin.datasets.make(args.workload, n=args.n, seed=seed)
     if args.capacity is not None:
         spec["capacity"] = args.capacity
+    if args.mode is not None:
+        spec["mode"] = args.mode
     _, prec, learned = _spec_and_prec(args)
     flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device="cuda")
     host = torch.from_numpy(pts).pin_memory()
@@ -475,7 +481,7 @@ def run_ours(args):
         "host_threads_per_rank": rank_host_threads(),
         "phases_ms": {k2: round(s[k2], 3) for k2 in ("ms_index", "ms_tasks", "ms_estimate", "ms_count", "ms_scan",
                                                      "ms_fill", "ms_expand", "ms_deliver", "ms_total")},
-        "batches": s["num_batches"], "overflow_retries": s["overflow_retries"],
+        "batches": s["num_batches"], "overflow_retries": s["overflow_retries"], "tasks": s["num_tasks"],
         "distance_calcs": s["distance_calcs"], "full_stencil_calcs": s["full_stencil_calcs"],
         "refined_pairs": s["refined_pairs"], "step_ms": step_ms,
         "scheduler": "learned" if learned else "sampling", "estimated_pairs": s["estimated_pairs"],
@@ -528,6 +534,7 @@ def main():
                     help="N > 1: split one join over the ranks (strong scaling) instead of N replicas")
     ap.add_argument("--capacity", type=int, default=None, help="batch capacity in pairs (default: the workload's)")
     ap.add_argument("--precision", type=int, default=None, help="0 FP64, 1 FP32 filter + FP64 refine")
+    ap.add_argument("--mode", type=int, default=None, help="search mode (default: the workload's)")
     ap.add_argument("--scheduler", choices=["learned", "sampling"], default=None,
                     help="batch/queue estimator (default: learned for the mixed-precision c4 workload)")
     ap.add_argument("--weights", default=ESTIMATOR_WEIGHTS, help="learned-estimator weights file")

@@ -83,6 +83,11 @@ struct DevBuf {
         if (e == cudaSuccess) n = c;
         return e;
     }
+    void swap(DevBuf &o)
+    {
+        std::swap(p, o.p);
+        std::swap(n, o.n);
+    }
 };
 
 struct PinBuf {
@@ -180,38 +185,50 @@ struct Ctx {
     DevBuf<uint32_t> cellStart;
     DevBuf<uint64_t> cellLid;
     DevBuf<uint32_t> cellCoord;
-    std::vector<uint32_t> hCellStart;
     double dataMin[SJ_MAX_DIM], dataMax[SJ_MAX_DIM];
     // neighbour lists
     int nbrPattern = -1;
+    uint32_t nbrTotal = 0;
     DevBuf<uint32_t> nbrStart, nbrCell;
     DevBuf<uint64_t> candFull;
     DevBuf<float> feat;
-    std::vector<uint32_t> hNbrStart, hNbrCell;
-    std::vector<uint64_t> hCandFull;
-    // tasks
-    std::vector<sj_task> tasks;
-    std::vector<double> taskPred, taskEvals;
-    DevBuf<sj_task> dTasks;
+    // per-cell predicted hits per evaluation (learned or sampled)
+    DevBuf<float> rate;
+    // tasks, built on the device (sj_tasks.cu)
+    uint32_t nTasks = 0;
+    DevBuf<sj_task> dTasks, dTasksAlt;
+    DevBuf<float> dTaskPred, dTaskPredAlt;
+    DevBuf<uint32_t> tgGroupCnt, tgGroupBase, tgGroupLen, tgPosCnt, tgOrder, tgOrderAlt, tgItemCnt, tgItemStart,
+        tgItemTasks, tgItemTaskStart, tgTot32;
+    DevBuf<uint64_t> tgKeys, tgKeysAlt;
+    DevBuf<unsigned long long> tgPosEv, tgEvExcl, tgTotals, tgScan64;
+    DevBuf<uint8_t> tgWorkers;
+    // per-task record offsets (exclusive prefix sums, nTasks + 1 each): row-mask
+    // words, column-mask words, row offsets, candidate records, emission units,
+    // planned pairs, predicted pairs
+    DevBuf<unsigned long long> off[7];
+    DevBuf<unsigned long long> offTemp;
+    // batch plan
+    DevBuf<uint32_t> planNext, planStart, planCount;
+    DevBuf<unsigned long long> planStats;
     // batch state
-    DevBuf<uint32_t> keyCount, keyStart;
+    DevBuf<uint32_t> keyCount, keyStart, keyStart2;
     DevBuf<int32_t> outKey, outVal;
     // host delivery: second set of the device buffers a batch's copy reads, so
     // the next batch's kernels need not wait for that copy
     DevBuf<int32_t> outValAlt;
     DevBuf<uint32_t> keyStartAlt;
     std::vector<cudaEvent_t> syncEvents;   // stage boundaries of the synchronous phase
-    DevBuf<uint8_t> scanTemp;
-    DevBuf<uint32_t> total;
+    DevBuf<uint8_t> scanTemp, scanTemp2;
+    DevBuf<uint32_t> total, total2;
     DevBuf<unsigned long long> stat;   // see sj_join_args::stat
     DevBuf<uint32_t> queueHead;
     DevBuf<uint32_t> taskHits;
     DevBuf<uint32_t> dTaskEvals, dTaskRefined;   // per task, written by the count pass
+    DevBuf<unsigned long long> sums;   // task sums: evaluations, refined, measured pairs
+    DevBuf<double> errSum;             // sum over tasks of |predicted - measured pairs|
     // count-pass records for the emission pass: per task, row and column hit
-    // masks, per-query row-run offsets and per-position candidate records;
-    // offsets are prefix sums over all tasks, as are the emission units
-    std::vector<uint64_t> hMaskOff, hColOff, hRowOff, hCandOff, hUnitOff;
-    DevBuf<uint64_t> dMaskOff, dColOff, dRowOff, dCandOff, dUnitOff;
+    // masks, per-query row-run offsets and per-position candidate records
     DevBuf<uint32_t> masks, colMasks, rowRel, candId, candRel;
     // the count pass of batch i + 1 writes this second record set while the
     // emission of batch i reads the first (device-fold pipeline)
@@ -241,12 +258,12 @@ struct Ctx {
     DevBuf<uint32_t> sValsAlt, sFlags, sOne, sCnt;
     DevBuf<uint8_t> sTemp;
     DevBuf<float> sMlpOut;
-    DevBuf<unsigned long long> sHits, sCands;
-    std::vector<double> cellRate;      // predicted hits per evaluation, per cell
-    std::vector<double> measCellHits;  // from the last degrees/join run (full-stencil semantics)
+    DevBuf<unsigned long long> sHits, sCands, sScalars;
+    DevBuf<unsigned long long> dCellHits;   // measured hits per cell (after sj_degrees)
     bool haveMeas = false;
     sj_stats st{};
 };
+
 
 sj_status check_params(const sj_params &p)
 {
@@ -371,18 +388,25 @@ sj_status build_index(Ctx &c)
     CK(valsAlt.ensure(n));
     CK(flags.ensure(n));
     CK(tmp.ensure(std::max(sj_radix_temp_bytes(n), sj_scan_temp_bytes(n))));
-    CK(sj_launch_cell_keys(c.pts.p, n, g, keys.p, c.ids.p, c.s));
+    DevBuf<uint32_t> &nne = c.sOne;
+    CK(nne.ensure(2));   // [0] non-empty cells, [1] out-of-grid flag
+    CK(cudaMemsetAsync(nne.p + 1, 0, sizeof(uint32_t), c.s));
+    CK(sj_launch_cell_keys(c.pts.p, n, g, keys.p, c.ids.p, nne.p + 1, c.s));
     int inAlt = 0;
     CK(sj_radix_sort_u64_u32(keys.p, c.ids.p, keysAlt.p, valsAlt.p, n, bits, tmp.p, &inAlt, c.s));
     uint64_t *sk = inAlt ? keysAlt.p : keys.p;
     if (inAlt) CK(cudaMemcpyAsync(c.ids.p, valsAlt.p, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, c.s));
     CK(sj_launch_cell_flags(sk, n, flags.p, c.s));
-    DevBuf<uint32_t> &nne = c.sOne;
-    CK(nne.ensure(1));
     CK(sj_exclusive_scan_u32(flags.p, flags.p, n, tmp.p, nne.p, c.s));
-    uint32_t nCells = 0;
-    CK(cudaMemcpyAsync(&nCells, nne.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, c.s));
+    uint32_t hn[2] = {0, 0};
+    CK(cudaMemcpyAsync(hn, nne.p, sizeof(hn), cudaMemcpyDeviceToHost, c.s));
     CK(cudaStreamSynchronize(c.s));
+    if (hn[1]) {
+        // a cell coordinate past its dimension's cell count would alias another cell
+        set_error("internal: a point's cell coordinate lies outside the grid");
+        return SJ_ERR_INTERNAL;
+    }
+    const uint32_t nCells = hn[0];
     c.nCells = nCells;
     CK(c.cellStart.ensure(nCells + 1));
     CK(c.cellLid.ensure(nCells));
@@ -394,21 +418,6 @@ sj_status build_index(Ctx &c)
     // 4. cell-sorted coordinates
     CK(c.xs.ensure(n * (uint64_t)g.Dp));
     CK(sj_launch_gather(c.pts.p, c.ids.p, n, D, g.Dp, c.xs.p, c.s));
-    c.hCellStart.resize(nCells + 1);
-    CK(cudaMemcpyAsync(c.hCellStart.data(), c.cellStart.p, sizeof(uint32_t) * (nCells + 1), cudaMemcpyDeviceToHost,
-                       c.s));
-    CK(cudaStreamSynchronize(c.s));
-    // every cell coordinate must lie inside the grid (no linear-id aliasing)
-    {
-        std::vector<uint32_t> coord((size_t)nCells * k);
-        // the last cell carries the largest linear id; coordinates are checked on a sample of cells
-        CK(cudaMemcpy(coord.data(), c.cellCoord.p, coord.size() * sizeof(uint32_t), cudaMemcpyDeviceToHost));
-        for (size_t i = 0; i < coord.size(); i++)
-            if (coord[i] >= g.nCells[i % k]) {
-                set_error("internal: cell coordinate outside the grid");
-                return SJ_ERR_INTERNAL;
-            }
-    }
     c.indexed = true;
     c.nbrPattern = -1;
     c.haveMeas = false;
@@ -428,31 +437,27 @@ sj_status build_neighbours(Ctx &c, int pattern)
     CK(c.feat.ensure((size_t)nc * SJ_NFEAT));
     DevBuf<uint32_t> &cnt = c.sCnt;
     CK(cnt.ensure(nc + 1));
+    DevBuf<unsigned long long> &sc = c.sScalars;
+    CK(sc.ensure(4));
+    CK(cudaMemsetAsync(sc.p, 0, sizeof(unsigned long long), c.s));
     CK(sj_launch_neighbours(c.cellLid.p, c.cellCoord.p, c.cellStart.p, nc, c.g, pattern, nullptr, cnt.p,
-                            c.candFull.p, c.feat.p, 0, c.s));
+                            c.candFull.p, sc.p, c.feat.p, 0, c.s));
     DevBuf<uint8_t> &tmp = c.sTemp;
-    DevBuf<uint32_t> &tot = c.sOne;
-    CK(tot.ensure(1));
     CK(tmp.ensure(sj_scan_temp_bytes(nc)));
-    CK(sj_exclusive_scan_u32(cnt.p, c.nbrStart.p, nc, tmp.p, tot.p, c.s));
-    uint32_t total = 0;
-    CK(cudaMemcpyAsync(&total, tot.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, c.s));
+    CK(sj_exclusive_scan_u32(cnt.p, c.nbrStart.p, nc, tmp.p, c.nbrStart.p + nc, c.s));
+    // the list length sizes the list; the candidate total is the work unit
+    struct {
+        uint32_t total;
+        unsigned long long full;
+    } h{};
+    CK(cudaMemcpyAsync(&h.total, c.nbrStart.p + nc, sizeof(uint32_t), cudaMemcpyDeviceToHost, c.s));
+    CK(cudaMemcpyAsync(&h.full, sc.p, sizeof(unsigned long long), cudaMemcpyDeviceToHost, c.s));
     CK(cudaStreamSynchronize(c.s));
-    CK(cudaMemcpyAsync(c.nbrStart.p + nc, &total, sizeof(uint32_t), cudaMemcpyHostToDevice, c.s));
-    CK(c.nbrCell.ensure(total));
+    CK(c.nbrCell.ensure(h.total));
     CK(sj_launch_neighbours(c.cellLid.p, c.cellCoord.p, c.cellStart.p, nc, c.g, pattern, c.nbrStart.p, c.nbrCell.p,
-                            nullptr, nullptr, 1, c.s));
-    c.hNbrStart.resize(nc + 1);
-    c.hNbrCell.resize(total);
-    c.hCandFull.resize(nc);
-    CK(cudaMemcpyAsync(c.hNbrStart.data(), c.nbrStart.p, sizeof(uint32_t) * (nc + 1), cudaMemcpyDeviceToHost, c.s));
-    if (total)
-        CK(cudaMemcpyAsync(c.hNbrCell.data(), c.nbrCell.p, sizeof(uint32_t) * total, cudaMemcpyDeviceToHost, c.s));
-    CK(cudaMemcpyAsync(c.hCandFull.data(), c.candFull.p, sizeof(uint64_t) * nc, cudaMemcpyDeviceToHost, c.s));
-    CK(cudaStreamSynchronize(c.s));
-    uint64_t full = 0;
-    for (uint64_t v : c.hCandFull) full += v;
-    c.st.full_stencil_calcs = full;
+                            nullptr, nullptr, nullptr, 1, c.s));
+    c.nbrTotal = h.total;
+    c.st.full_stencil_calcs = h.full;
     c.nbrPattern = pattern;
     return SJ_OK;
 }
@@ -511,201 +516,10 @@ FilterBounds filter_bounds(const Ctx &c)
     return b;
 }
 
-// ------------------------------------------------------------ estimate --
-sj_status estimate_rates(Ctx &c)
-{
-    Timer tm;
-    tm.start(c.s);
-    const uint32_t nc = c.nCells;
-    c.cellRate.assign(nc, 0.0);
-    if (c.p.scheduler == SJ_SCHED_LEARNED && !c.mlpW.empty()) {
-        DevBuf<float> &out = c.sMlpOut;
-        CK(out.ensure((size_t)nc * SJ_NOUT));
-        CK(c.dMlpW.ensure(SJ_MLP_NPARAM));
-        CK(cudaMemcpyAsync(c.dMlpW.p, c.mlpW.data(), sizeof(float) * SJ_MLP_NPARAM, cudaMemcpyHostToDevice, c.s));
-        CK(sj_launch_mlp_infer(c.feat.p, nc, c.dMlpW.p, out.p, c.s));
-        std::vector<float> h((size_t)nc * SJ_NOUT);
-        CK(cudaMemcpyAsync(h.data(), out.p, h.size() * sizeof(float), cudaMemcpyDeviceToHost, c.s));
-        CK(cudaStreamSynchronize(c.s));
-        for (uint32_t i = 0; i < nc; i++) {
-            double hits = std::exp2((double)h[(size_t)i * SJ_NOUT + 1]) - 1.0;
-            double calcs = (double)c.hCandFull[i];
-            double r = calcs > 0 ? hits / calcs : 0.0;
-            c.cellRate[i] = std::min(1.0, std::max(r, 0.0));
-        }
-    } else {
-        DevBuf<unsigned long long> &hits = c.sHits, &cands = c.sCands;
-        CK(hits.ensure(nc));
-        CK(cands.ensure(nc));
-        CK(cudaMemsetAsync(hits.p, 0, sizeof(unsigned long long) * nc, c.s));
-        CK(cudaMemsetAsync(cands.p, 0, sizeof(unsigned long long) * nc, c.s));
-        sj_join_args a;
-        join_args_base(c, a);
-        a.taskEnd = (uint32_t)c.n;   // number of cell-sorted positions
-        uint32_t stride = (uint32_t)std::max(1.0, std::floor(1.0 / c.p.sample_rate + 0.5));
-        CK(sj_launch_sample(a, c.g, stride, hits.p, cands.p, nc, c.s));
-        std::vector<unsigned long long> hh(nc), hc(nc);
-        CK(cudaMemcpyAsync(hh.data(), hits.p, sizeof(unsigned long long) * nc, cudaMemcpyDeviceToHost, c.s));
-        CK(cudaMemcpyAsync(hc.data(), cands.p, sizeof(unsigned long long) * nc, cudaMemcpyDeviceToHost, c.s));
-        CK(cudaStreamSynchronize(c.s));
-        double sh = 0, sc = 0;
-        for (uint32_t i = 0; i < nc; i++) { sh += (double)hh[i]; sc += (double)hc[i]; }
-        double global = sc > 0 ? sh / sc : 1.0;
-        for (uint32_t i = 0; i < nc; i++) c.cellRate[i] = hc[i] ? (double)hh[i] / (double)hc[i] : global;
-    }
-    c.st.ms_estimate = tm.stop(c.s);
-    return SJ_OK;
-}
-
 // --------------------------------------------------------------- tasks --
-// Evaluations of a chunk [s0, s1) of a symmetric home segment for query
-// indices 0..q-1: only candidates at stream offset >= query index count.
-double diag_evals(uint64_t s0, uint64_t s1, uint64_t q)
-{
-    // sum over i in [0, q) of max(0, s1 - max(s0, i))
-    if (s1 <= s0) return 0.0;
-    double e = (double)std::min(q, s0) * (double)(s1 - s0);
-    const uint64_t a = s0, b = std::min(q, s1);
-    if (b > a) e += (double)(b - a) * (double)s1 - 0.5 * (double)(a + b - 1) * (double)(b - a);
-    return e;
-}
-
-// Tasks of one cell: query tiles of <= SJ_CTA * R points (R query slots per
-// join thread, sj_query_slots) x chunks of the cell's
-// candidate stream (home segment + owned neighbours, <= SJ_MAX_SEG segments per
-// group).  With emit == nullptr only counts them.  Returns the number of tasks
-// and adds their evaluations / predicted pairs to *evals / *pred.
-template <class Emit>
-uint32_t cell_tasks(const Ctx &c, uint32_t A, bool sym, uint64_t cap, double pairsPerTask, Emit emit)
-{
-    const uint32_t aStart = c.hCellStart[A], aEnd = c.hCellStart[A + 1];
-    const uint32_t occ = aEnd - aStart;
-    const uint32_t nb0 = c.hNbrStart[A], nb1 = c.hNbrStart[A + 1];
-    const uint32_t nSegAll = 1 + (nb1 - nb0);
-    const double rate = c.cellRate.empty() ? 0.0 : c.cellRate[A];
-    const uint32_t tile = SJ_CTA * (uint32_t)sj_query_slots(c.g.Dp, c.p.precision == SJ_PREC_FP32_REFINE);
-    uint32_t made = 0;
-    for (uint32_t q0 = 0; q0 < occ; q0 += tile) {
-        const uint32_t qc = std::min<uint32_t>(tile, occ - q0);
-        const uint32_t qBegin = aStart + q0;
-        // chunk length from the predicted pair density of this cell, and never
-        // more candidates than keep the worst case (every candidate a hit, both
-        // directions) inside one batch
-        const double perEval = std::max(rate, 1e-6) * (sym ? 2.0 : 1.0);
-        const double chunk = pairsPerTask / (perEval * qc);
-        uint32_t sChunk = (uint32_t)std::min(65536.0, std::max(256.0, chunk));
-        const uint64_t worst = cap / ((sym ? 2ULL : 1ULL) * qc);
-        if (sChunk > worst) sChunk = (uint32_t)worst;
-        sChunk = std::max<uint32_t>(32, (sChunk / 32) * 32);
-        for (uint32_t g0 = 0; g0 < nSegAll; g0 += SJ_MAX_SEG) {
-            const uint32_t gc = std::min<uint32_t>(SJ_MAX_SEG, nSegAll - g0);
-            uint64_t homeLen = 0, L = 0;
-            for (uint32_t sgi = 0; sgi < gc; sgi++) {
-                const uint32_t gs = g0 + sgi;
-                uint64_t len;
-                if (gs == 0) {
-                    len = sym ? (aEnd - qBegin) : occ;
-                    homeLen = len;
-                } else {
-                    const uint32_t B = c.hNbrCell[nb0 + gs - 1];
-                    len = c.hCellStart[B + 1] - c.hCellStart[B];
-                }
-                L += len;
-            }
-            for (uint64_t s0 = 0; s0 < L; s0 += sChunk) {
-                const uint64_t s1 = std::min<uint64_t>(L, s0 + sChunk);
-                double ev;
-                if (sym && g0 == 0 && s0 < homeLen) {
-                    const uint64_t h1 = std::min<uint64_t>(s1, homeLen);
-                    ev = diag_evals(s0, h1, qc) + (double)qc * (double)(s1 - h1);
-                } else {
-                    ev = (double)qc * (double)(s1 - s0);
-                }
-                sj_task t;
-                t.cell = A;
-                t.qBegin = qBegin;
-                t.qCount = qc;
-                t.segBase = g0;
-                t.segCount = gc;
-                t.sBegin = (uint32_t)s0;
-                t.sEnd = (uint32_t)s1;
-                t.flags = (sym ? SJ_TASK_SYM : 0u) | (g0 == 0 ? SJ_TASK_HOME : 0u);
-                emit(made, t, ev, ev * rate * (sym ? 2.0 : 1.0));
-                made++;
-            }
-        }
-    }
-    return made;
-}
-
-// Builds the task list in queue order.  With byCost the cells are ordered by
-// their mean predicted task cost (evaluations + a write cost per predicted
-// pair), heaviest first, and each cell's tasks stay together; otherwise cells
-// keep linear-id order.  Cells are processed in parallel on the host.
-sj_status build_tasks(Ctx &c, int pattern, uint64_t cap, bool byCost)
-{
-    const bool sym = pattern != SJ_PAT_FULL;
-    const uint32_t nc = c.nCells;
-    const double pairsPerTask = std::max(4096.0, (double)cap / 4096.0);
-    std::vector<uint32_t> cnt(nc);
-    std::vector<double> cellCost(nc);
-#pragma omp parallel for schedule(dynamic, 64)
-    for (int64_t Ai = 0; Ai < (int64_t)nc; Ai++) {
-        const uint32_t A = (uint32_t)Ai;
-        double ev = 0, pr = 0;
-        cnt[A] = cell_tasks(c, A, sym, cap, pairsPerTask, [&](uint32_t, const sj_task &, double e, double p) {
-            ev += e;
-            pr += p;
-        });
-        cellCost[A] = cnt[A] ? (ev + 4.0 * pr) / cnt[A] : 0.0;
-    }
-    std::vector<uint32_t> order(nc);
-    std::iota(order.begin(), order.end(), 0u);
-    // heaviest first; equal costs keep cell order (the cell index breaks ties,
-    // so the parallel sort gives the order a stable sort would)
-    if (byCost)
-        __gnu_parallel::sort(order.begin(), order.end(), [&](uint32_t x, uint32_t y) {
-            return cellCost[x] > cellCost[y] || (cellCost[x] == cellCost[y] && x < y);
-        });
-    std::vector<uint64_t> off(nc + 1, 0);
-    for (uint32_t i = 0; i < nc; i++) off[i + 1] = off[i] + cnt[order[i]];
-    const uint64_t nt = off[nc];
-    if (nt > 0xffffffffULL) {
-        set_error("%llu tasks exceed the 32-bit task index", (unsigned long long)nt);
-        return SJ_ERR_BAD_INPUT;
-    }
-    c.tasks.resize(nt);
-    c.taskEvals.resize(nt);
-    c.taskPred.resize(nt);
-#pragma omp parallel for schedule(dynamic, 64)
-    for (int64_t i = 0; i < (int64_t)nc; i++) {
-        const uint64_t base = off[i];
-        cell_tasks(c, order[i], sym, cap, pairsPerTask, [&](uint32_t j, const sj_task &t, double e, double p) {
-            c.tasks[base + j] = t;
-            c.taskEvals[base + j] = e;
-            c.taskPred[base + j] = p;
-        });
-    }
-    if (c.p.shard_count > 1) {
-        // round-robin over the ordered list: each shard gets a similar cost mix
-        size_t w = 0;
-        for (size_t i = 0; i < c.tasks.size(); i++)
-            if ((int)(i % (size_t)c.p.shard_count) == c.p.shard_index) {
-                c.tasks[w] = c.tasks[i];
-                c.taskEvals[w] = c.taskEvals[i];
-                c.taskPred[w] = c.taskPred[i];
-                w++;
-            }
-        c.tasks.resize(w);
-        c.taskEvals.resize(w);
-        c.taskPred.resize(w);
-    }
-    return SJ_OK;
-}
-
-// ---------------------------------------------------------------- join --
 struct BatchRange {
     uint32_t t0, t1;
+    double pred;   // planned batch: its predicted pairs; a part re-planned after an overflow: -1
 };
 
 sj_status run_count(Ctx &c, sj_join_args &a, bool queue, cudaStream_t st = nullptr)
@@ -716,71 +530,243 @@ sj_status run_count(Ctx &c, sj_join_args &a, bool queue, cudaStream_t st = nullp
     return SJ_OK;
 }
 
-// Per-task record offsets of the count pass: per block of 32 stream
-// positions one row-mask word per query and (symmetric tasks) one column-mask
-// word per candidate and group of 32 queries; one row-run offset per query;
-// one candidate record per stream position.  Also the emission units.
-sj_status task_offsets(Ctx &c)
-{
-    const size_t nt = c.tasks.size();
-    c.hMaskOff.assign(nt + 1, 0);
-    c.hColOff.assign(nt + 1, 0);
-    c.hRowOff.assign(nt + 1, 0);
-    c.hCandOff.assign(nt + 1, 0);
-    c.hUnitOff.assign(nt + 1, 0);
-    // per-task sizes at [i + 1], then one prefix pass: per-thread range sums,
-    // their exclusive scan, and the ranges' prefixes from those bases
-    const int T = std::max(1, omp_get_max_threads());
-    std::vector<uint64_t> part(5 * (size_t)(T + 1), 0);
-#pragma omp parallel num_threads(T)
-    {
-        const int th = omp_get_thread_num(), nth = omp_get_num_threads();
-        const size_t b = nt * (size_t)th / (size_t)nth, e = nt * (size_t)(th + 1) / (size_t)nth;
-        uint64_t acc[5] = {0, 0, 0, 0, 0};
-        for (size_t i = b; i < e; i++) {
-            const sj_task &t = c.tasks[i];
-            const uint32_t len = t.sEnd - t.sBegin;
-            const bool sym = (t.flags & SJ_TASK_SYM) != 0;
-            const uint64_t blocks = ((uint64_t)len + 31) / 32;
-            const uint64_t groups = ((uint64_t)t.qCount + 31) / 32;
-            c.hMaskOff[i + 1] = acc[0] += blocks * t.qCount;
-            c.hColOff[i + 1] = acc[1] += (sym ? blocks * groups * 32 : 0);
-            c.hRowOff[i + 1] = acc[2] += t.qCount;
-            c.hCandOff[i + 1] = acc[3] += len;
-            c.hUnitOff[i + 1] = acc[4] += sj_task_units(t.qCount, len, sym);
-        }
-        for (int k = 0; k < 5; k++) part[5 * (size_t)(th + 1) + k] = acc[k];
-#pragma omp barrier
-#pragma omp single
-        for (int t2 = 1; t2 <= nth; t2++)
-            for (int k = 0; k < 5; k++) part[5 * (size_t)t2 + k] += part[5 * (size_t)(t2 - 1) + k];
-        const uint64_t *base = &part[5 * (size_t)th];
-        if (th > 0)
-            for (size_t i = b; i < e; i++) {
-                c.hMaskOff[i + 1] += base[0];
-                c.hColOff[i + 1] += base[1];
-                c.hRowOff[i + 1] += base[2];
-                c.hCandOff[i + 1] += base[3];
-                c.hUnitOff[i + 1] += base[4];
-            }
-    }
-    CK(c.dMaskOff.ensure(nt + 1));
-    CK(c.dColOff.ensure(nt + 1));
-    CK(c.dRowOff.ensure(nt + 1));
-    CK(c.dCandOff.ensure(nt + 1));
-    CK(c.dUnitOff.ensure(nt + 1));
-    CK(cudaMemcpyAsync(c.dMaskOff.p, c.hMaskOff.data(), sizeof(uint64_t) * (nt + 1), cudaMemcpyHostToDevice, c.s));
-    CK(cudaMemcpyAsync(c.dColOff.p, c.hColOff.data(), sizeof(uint64_t) * (nt + 1), cudaMemcpyHostToDevice, c.s));
-    CK(cudaMemcpyAsync(c.dRowOff.p, c.hRowOff.data(), sizeof(uint64_t) * (nt + 1), cudaMemcpyHostToDevice, c.s));
-    CK(cudaMemcpyAsync(c.dCandOff.p, c.hCandOff.data(), sizeof(uint64_t) * (nt + 1), cudaMemcpyHostToDevice, c.s));
-    CK(cudaMemcpyAsync(c.dUnitOff.p, c.hUnitOff.data(), sizeof(uint64_t) * (nt + 1), cudaMemcpyHostToDevice, c.s));
-    return SJ_OK;
-}
-
 // Hit-mask words (row or column) one batch may record (4 bytes each); a batch
 // is also cut when its masks would exceed this.
 constexpr uint64_t SJ_MASK_BATCH_WORDS = 1ULL << 29;
 
+// The task list, built on the device (sj_tasks.cu): per-cell workload and cost
+// key, the cost order (stable radix sort, heaviest first, ties in cell order),
+// one work item per (cell, segment group, query tile) and its tasks.  policy:
+// 0 cost-proportional stream chunks (needs c.rate), 1 fixed chunks, 2 the
+// mode-8 split by thirds of the work.  sampleRate > 0 builds the sampling
+// estimator's tasks.  With `shard`, keeps this context's shard of the list.
+// Sets c.nTasks; the tasks are in c.dTasks, their predicted pairs in c.dTaskPred.
+sj_status build_tasks_dev(Ctx &c, bool sym, uint64_t cap, bool byCost, int policy, float sampleRate, bool shard)
+{
+    const uint32_t nc = c.nCells;
+    cudaStream_t s = c.s;
+    sj_taskgen g{};
+    g.cellStart = c.cellStart.p;
+    g.nbrStart = c.nbrStart.p;
+    g.nbrCell = c.nbrCell.p;
+    g.rate = policy == 0 ? c.rate.p : nullptr;
+    g.nCells = nc;
+    g.tile = SJ_CTA * (uint32_t)sj_query_slots(c.g.Dp, c.p.precision == SJ_PREC_FP32_REFINE);
+    g.cap = cap;
+    // predicted pairs per task: about 4096 tasks per full batch.  SJ_TASK_PAIRS
+    // overrides it (a tuning knob: profiling runs at a reduced batch capacity
+    // use it to keep the task shapes of the full-capacity run)
+    g.pairsPerTask = std::max(4096.0, (double)cap / 4096.0);
+    if (const char *ev = getenv("SJ_TASK_PAIRS")) {
+        const double v = atof(ev);
+        if (v >= 1.0) g.pairsPerTask = v;
+    }
+    g.sym = sym ? 1 : 0;
+    g.policy = policy;
+    g.sampleRate = sampleRate;
+    DevBuf<uint8_t> &tmp = c.sTemp;
+    CK(tmp.ensure(std::max(sj_scan_temp_bytes(nc + 1), sj_radix_temp_bytes(nc))));
+    CK(c.tgTot32.ensure(2));
+    CK(c.tgTotals.ensure(4));
+    CK(cudaMemsetAsync(c.tgTotals.p, 0, sizeof(unsigned long long) * 4, s));
+    // segment groups of every cell and their slots (at most one group per
+    // SJ_MAX_SEG owned neighbours, plus one per cell)
+    CK(c.tgGroupCnt.ensure(nc + 1));
+    CK(c.tgGroupBase.ensure(nc + 1));
+    CK(c.tgGroupLen.ensure((size_t)nc + c.nbrTotal / SJ_MAX_SEG + 1));
+    CK(sj_tg_groups(g, c.tgGroupCnt.p, s));
+    CK(sj_exclusive_scan_u32(c.tgGroupCnt.p, c.tgGroupBase.p, nc, tmp.p, c.tgTot32.p, s));
+    g.groupBase = c.tgGroupBase.p;
+    g.groupLen = c.tgGroupLen.p;
+    // per-cell task counts, evaluations and cost keys, in cell order
+    CK(c.tgPosCnt.ensure(nc + 1));
+    CK(c.tgPosEv.ensure(nc + 1));
+    CK(c.tgKeys.ensure(nc));
+    CK(c.tgKeysAlt.ensure(nc));
+    CK(c.tgOrder.ensure(nc));
+    CK(c.tgOrderAlt.ensure(nc));
+    CK(sj_tg_cells(g, nullptr, nullptr, c.tgPosCnt.p, c.tgPosEv.p,
+                   byCost ? reinterpret_cast<unsigned long long *>(c.tgKeys.p) : nullptr, c.tgTotals.p, s));
+    CK(sj_iota_u32(c.tgOrder.p, nc, s));
+    uint32_t *order = c.tgOrder.p;
+    if (byCost && nc > 1) {
+        int inAlt = 0;
+        CK(sj_radix_sort_u64_u32(c.tgKeys.p, c.tgOrder.p, c.tgKeysAlt.p, c.tgOrderAlt.p, nc, 64, tmp.p, &inAlt, s));
+        if (inAlt) order = c.tgOrderAlt.p;
+    }
+    const uint8_t *workers = nullptr;
+    unsigned long long *taskTotal = c.tgTotals.p;
+    if (policy == 2) {
+        // mode 8: the evaluations in cost order decide each cell's third of the
+        // work, which sets how many tasks share each of its tiles' streams
+        CK(sj_tg_cells(g, order, nullptr, c.tgPosCnt.p, c.tgPosEv.p, nullptr, c.tgTotals.p + 2, s));
+        CK(c.tgEvExcl.ensure(nc + 1));
+        CK(c.tgScan64.ensure(sj_scan64_temp(nc)));
+        CK(sj_exclusive_scan_u64(c.tgPosEv.p, c.tgEvExcl.p, nc, c.tgScan64.p, s));
+        CK(c.tgWorkers.ensure(nc));
+        CK(sj_tg_thirds(c.tgEvExcl.p, nc, c.tgWorkers.p, s));
+        workers = c.tgWorkers.p;
+        CK(cudaMemsetAsync(c.tgTotals.p + 2, 0, sizeof(unsigned long long) * 2, s));
+        CK(sj_tg_cells(g, order, workers, c.tgPosCnt.p, c.tgPosEv.p, nullptr, c.tgTotals.p + 2, s));
+        taskTotal = c.tgTotals.p + 2;
+    }
+    // work items in order and their first tasks
+    CK(c.tgItemCnt.ensure(nc + 1));
+    CK(c.tgItemStart.ensure(nc + 1));
+    CK(sj_tg_item_counts(g, order, c.tgItemCnt.p, s));
+    CK(sj_exclusive_scan_u32(c.tgItemCnt.p, c.tgItemStart.p, nc, tmp.p, c.tgTot32.p, s));
+    struct {
+        uint32_t items;
+        unsigned long long tasks;
+    } h{};
+    CK(cudaMemcpyAsync(&h.items, c.tgTot32.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(&h.tasks, taskTotal, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    if (h.tasks > 0xffffffffULL) {
+        set_error("%llu tasks exceed the 32-bit task index", h.tasks);
+        return SJ_ERR_BAD_INPUT;
+    }
+    const uint32_t nItems = h.items;
+    CK(c.tgItemTasks.ensure((size_t)nItems + 1));
+    CK(c.tgItemTaskStart.ensure((size_t)nItems + 1));
+    CK(tmp.ensure(sj_scan_temp_bytes((uint64_t)nItems + 1)));
+    CK(sj_tg_item_tasks(g, order, workers, c.tgItemStart.p, nItems, c.tgItemTasks.p, s));
+    CK(sj_exclusive_scan_u32(c.tgItemTasks.p, c.tgItemTaskStart.p, nItems, tmp.p, c.tgTot32.p + 1, s));
+    uint32_t nt = 0;
+    CK(cudaMemcpyAsync(&nt, c.tgTot32.p + 1, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    if (nt != h.tasks) {
+        set_error("internal: task builder counted %llu tasks per cell but %u per item", h.tasks, nt);
+        return SJ_ERR_INTERNAL;
+    }
+    CK(c.dTasks.ensure(nt ? nt : 1));
+    CK(c.dTaskPred.ensure(nt ? nt : 1));
+    CK(sj_tg_item_write(g, order, workers, c.tgItemStart.p, nItems, c.tgItemTaskStart.p, c.dTasks.p, c.dTaskPred.p, s));
+    if (shard && c.p.shard_count > 1) {
+        // round-robin over the ordered list: each shard gets a similar cost mix
+        const uint32_t idx = (uint32_t)c.p.shard_index, cnt = (uint32_t)c.p.shard_count;
+        const uint32_t nOut = nt > idx ? (nt - idx + cnt - 1) / cnt : 0u;
+        CK(c.dTasksAlt.ensure(nOut ? nOut : 1));
+        CK(c.dTaskPredAlt.ensure(nOut ? nOut : 1));
+        CK(sj_tg_shard(c.dTasks.p, c.dTaskPred.p, nOut, idx, cnt, c.dTasksAlt.p, c.dTaskPredAlt.p, s));
+        c.dTasks.swap(c.dTasksAlt);
+        c.dTaskPred.swap(c.dTaskPredAlt);
+        nt = nOut;
+    }
+    c.nTasks = nt;
+    return SJ_OK;
+}
+
+// Record offsets of c's task list (c.off[0..6], see Ctx).
+sj_status task_offsets_dev(Ctx &c)
+{
+    const uint32_t nt = c.nTasks;
+    unsigned long long *out[7];
+    for (int k = 0; k < 7; k++) {
+        CK(c.off[k].ensure((size_t)nt + 1));
+        out[k] = c.off[k].p;
+    }
+    CK(c.offTemp.ensure(sj_task_offsets_temp(nt)));
+    CK(sj_task_offsets(c.dTasks.p, c.dTaskPred.p, nt, c.p.alpha, c.offTemp.p, out, c.s));
+    return SJ_OK;
+}
+
+// Greedy batch plan on the device: consecutive tasks whose planned pairs
+// (predicted x (1 + alpha)) fit `cap` and whose hit masks fit their limit.
+// Returns the batches with their predicted pairs, the largest record sizes
+// of any batch (row-mask words, column-mask words, row offsets, candidate
+// records) and the predicted total.
+sj_status plan_dev(Ctx &c, uint64_t cap, std::vector<BatchRange> &plan, uint64_t (&maxes)[4], double &predTotal)
+{
+    const uint32_t nt = c.nTasks;
+    plan.clear();
+    for (int k = 0; k < 4; k++) maxes[k] = 1;
+    unsigned long long *off[7];
+    for (int k = 0; k < 7; k++) off[k] = c.off[k].p;
+    CK(c.planNext.ensure(nt ? nt : 1));
+    CK(c.planStart.ensure((size_t)nt + 1));
+    CK(c.planCount.ensure(1));
+    CK(sj_plan_batches(off, nt, cap, SJ_MASK_BATCH_WORDS, c.planNext.p, c.planStart.p, c.planCount.p, c.s));
+    struct {
+        uint32_t nb;
+        unsigned long long pred;
+    } h{};
+    CK(cudaMemcpyAsync(&h.nb, c.planCount.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, c.s));
+    CK(cudaMemcpyAsync(&h.pred, c.off[6].p + nt, sizeof(unsigned long long), cudaMemcpyDeviceToHost, c.s));
+    CK(cudaStreamSynchronize(c.s));
+    predTotal = (double)h.pred;
+    const uint32_t nb = h.nb;
+    if (nb == 0) return SJ_OK;
+    CK(c.planStats.ensure((size_t)nb * 5));
+    CK(sj_plan_stats(c.planStart.p, nb, off, c.planStats.p, c.s));
+    std::vector<uint32_t> start(nb + 1);
+    std::vector<unsigned long long> st((size_t)nb * 5);
+    CK(cudaMemcpyAsync(start.data(), c.planStart.p, sizeof(uint32_t) * (nb + 1), cudaMemcpyDeviceToHost, c.s));
+    CK(cudaMemcpyAsync(st.data(), c.planStats.p, sizeof(unsigned long long) * nb * 5, cudaMemcpyDeviceToHost, c.s));
+    CK(cudaStreamSynchronize(c.s));
+    plan.resize(nb);
+    for (uint32_t b = 0; b < nb; b++) {
+        plan[b] = {start[b], start[b + 1], (double)st[(size_t)b * 5]};
+        for (int k = 0; k < 4; k++) maxes[k] = std::max<uint64_t>(maxes[k], st[(size_t)b * 5 + 1 + k]);
+    }
+    return SJ_OK;
+}
+
+// ------------------------------------------------------------ estimate --
+// Per-cell predicted hits per evaluation (c.rate), which sizes the tasks,
+// orders the queue and plans the batches.  Learned: the MLP on the cell
+// features.  Sampling: the count pass over tasks for about sample_rate of
+// every cell's points against the cell's whole candidate stream
+// (GPU.cu:854-1065 samples every 100th point the same way); cells without a
+// sampled point take the global rate.
+sj_status estimate_rates(Ctx &c)
+{
+    Timer tm;
+    tm.start(c.s);
+    const uint32_t nc = c.nCells;
+    CK(c.rate.ensure(nc ? nc : 1));
+    if (c.p.scheduler == SJ_SCHED_LEARNED && !c.mlpW.empty()) {
+        DevBuf<float> &out = c.sMlpOut;
+        CK(out.ensure((size_t)nc * SJ_NOUT));
+        CK(c.dMlpW.ensure(SJ_MLP_NPARAM));
+        CK(cudaMemcpyAsync(c.dMlpW.p, c.mlpW.data(), sizeof(float) * SJ_MLP_NPARAM, cudaMemcpyHostToDevice, c.s));
+        CK(sj_launch_mlp_infer(c.feat.p, nc, c.dMlpW.p, out.p, c.s));
+        CK(sj_rates_mlp(out.p, reinterpret_cast<const unsigned long long *>(c.candFull.p), nc, c.rate.p, c.s));
+    } else {
+        CKS(build_tasks_dev(c, false, 0xffffffffULL, false, 1, (float)c.p.sample_rate, false));
+        const uint32_t nt = c.nTasks;
+        CK(c.keyCount.ensure(c.n));
+        CK(c.stat.ensure(8));
+        CK(c.queueHead.ensure(1));
+        CK(c.taskHits.ensure(nt ? nt : 1));
+        CK(c.dTaskEvals.ensure(nt ? nt : 1));
+        CK(c.dTaskRefined.ensure(nt ? nt : 1));
+        sj_join_args a;
+        join_args_base(c, a);
+        a.tasks = c.dTasks.p;
+        a.queueHead = c.queueHead.p;
+        a.keyCount = c.keyCount.p;   // cleared before the join's first count pass
+        a.stat = c.stat.p;
+        a.taskHits = c.taskHits.p;
+        a.taskEvals = c.dTaskEvals.p;
+        a.taskRefined = c.dTaskRefined.p;
+        const FilterBounds fb = filter_bounds(c);
+        a.margin = fb.margin;
+        a.delta = fb.delta;
+        a.taskBegin = 0;
+        a.taskEnd = nt;
+        CKS(run_count(c, a, true));
+        CK(c.sHits.ensure(nc ? nc : 1));
+        CK(c.sCands.ensure(nc ? nc : 1));
+        CK(c.sScalars.ensure(4));
+        CK(sj_sample_rates(c.dTasks.p, nt, c.taskHits.p, c.dTaskEvals.p, c.sHits.p, c.sCands.p, c.sScalars.p + 2, nc,
+                           c.rate.p, c.s));
+    }
+    c.st.ms_estimate = tm.stop(c.s);
+    return SJ_OK;
+}
+
+// ---------------------------------------------------------------- join --
 sj_status prepare_join(Ctx &c, int &pattern, bool &queue)
 {
     if (!c.indexed) {
@@ -859,25 +845,27 @@ sj_status replan_exact(const BatchRange &br, const std::vector<uint32_t> &taskHi
             return SJ_ERR_INTERNAL;
         }
         if (t > t0 && acc + h > cap) {
-            parts.push_back({t0, t});
+            parts.push_back({t0, t, -1.0});
             t0 = t;
             acc = 0;
         }
         acc += h;
     }
-    parts.push_back({t0, br.t1});
+    parts.push_back({t0, br.t1, -1.0});
     out.insert(out.end(), parts.begin(), parts.end());
     return SJ_OK;
 }
 
-// Key array of the current batch (a.outKey, a.capacity) from keyStart.
-sj_status expand_keys(Ctx &c, const sj_join_args &a, cudaStream_t st = nullptr)
+// Key array of the current batch (a.outKey, a.capacity) from a.keyStart and
+// the batch's scan total (default: c.total).
+sj_status expand_keys(Ctx &c, const sj_join_args &a, cudaStream_t st = nullptr, const uint32_t *scanTotal = nullptr)
 {
     if (!st) st = c.s;
+    if (!scanTotal) scanTotal = c.total.p;
     const size_t slots = sj_expand_long_slots(a.capacity);
     CK(c.longRuns.ensure(slots));
     CK(c.longCount.ensure(1));
-    CK(sj_expand_keys(a.keyStart, c.total.p, c.n, a.outKey, a.batchPairs, a.capacity, c.longRuns.p,
+    CK(sj_expand_keys(a.keyStart, scanTotal, c.n, a.outKey, a.batchPairs, a.capacity, c.longRuns.p,
                       (uint32_t)std::min<size_t>(c.longRuns.n, 0xffffffffu), c.longCount.p, c.numSM, st));
     return SJ_OK;
 }
@@ -897,21 +885,25 @@ sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
     const uint64_t n = c.n;
     uint64_t cap = auto_capacity(c);
     if (cap > 0xffffffffULL) cap = 0xffffffffULL;
+    std::vector<BatchRange> plan;
+    uint64_t maxes[4];
+    double predTotal = 0;
     {
         Timer tm;
         tm.start(c.s);
         const bool byCost = c.p.sort_by_workload || c.p.search_mode == 7 || c.p.search_mode == 8 ||
                             c.p.search_mode == 9 || c.p.search_mode == 10;
-        CKS(build_tasks(c, pattern, cap, byCost));
-        CK(c.dTasks.ensure(c.tasks.size()));
-        if (!c.tasks.empty())
-            CK(cudaMemcpyAsync(c.dTasks.p, c.tasks.data(), sizeof(sj_task) * c.tasks.size(), cudaMemcpyHostToDevice,
-                               c.s));
-        CKS(task_offsets(c));
+        // mode 8 splits each tile's stream by the third of the work its cell is in
+        CKS(build_tasks_dev(c, pattern != SJ_PAT_FULL, cap, byCost, c.p.search_mode == 8 ? 2 : 0, 0.0f, true));
+        CKS(task_offsets_dev(c));
+        // greedy batch plan on predicted pairs (and on hit-mask words)
+        CKS(plan_dev(c, cap, plan, maxes, predTotal));
         c.st.ms_tasks += tm.stop(c.s);
     }
-    const uint32_t nt = (uint32_t)c.tasks.size();
+    const uint32_t nt = c.nTasks;
     c.st.num_tasks = nt;
+    c.st.estimated_pairs = predTotal;
+    const uint64_t maxMaskWords = maxes[0], maxColWords = maxes[1], maxRowWords = maxes[2], maxCandRecs = maxes[3];
     CK(c.keyCount.ensure(n));
     CK(c.keyStart.ensure(n));
     CK(c.scanTemp.ensure(sj_scan_temp_bytes(n)));
@@ -926,36 +918,7 @@ sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
     CK(cudaMemsetAsync(c.dTaskRefined.p, 0, sizeof(uint32_t) * (nt ? nt : 1), c.s));
     CK(c.pinTotal.ensure(64));
     CK(cudaMemsetAsync(c.stat.p, 0, sizeof(unsigned long long) * 8, c.s));
-    double predTotal = 0;
-    for (double v : c.taskPred) predTotal += v;
-    c.st.estimated_pairs = predTotal;
 
-    // greedy batch plan on predicted pairs (and on hit-mask words)
-    std::vector<BatchRange> plan;
-    uint64_t maxMaskWords = 1, maxColWords = 1, maxRowWords = 1, maxCandRecs = 1;
-    {
-        const double alpha = c.p.alpha;
-        uint32_t t0 = 0;
-        double acc = 0;
-        for (uint32_t t = 0; t < nt; t++) {
-            double v = c.taskPred[t] * (1.0 + alpha);
-            if (t > t0 && (acc + v > (double)cap || c.hMaskOff[t + 1] - c.hMaskOff[t0] > SJ_MASK_BATCH_WORDS ||
-                           c.hColOff[t + 1] - c.hColOff[t0] > SJ_MASK_BATCH_WORDS ||
-                           c.hUnitOff[t + 1] - c.hUnitOff[t0] > 0xffffffffULL)) {
-                plan.push_back({t0, t});
-                t0 = t;
-                acc = 0;
-            }
-            acc += v;
-        }
-        if (nt > t0) plan.push_back({t0, nt});
-        for (const BatchRange &br : plan) {
-            maxMaskWords = std::max<uint64_t>(maxMaskWords, c.hMaskOff[br.t1] - c.hMaskOff[br.t0]);
-            maxColWords = std::max<uint64_t>(maxColWords, c.hColOff[br.t1] - c.hColOff[br.t0]);
-            maxRowWords = std::max<uint64_t>(maxRowWords, c.hRowOff[br.t1] - c.hRowOff[br.t0]);
-            maxCandRecs = std::max<uint64_t>(maxCandRecs, c.hCandOff[br.t1] - c.hCandOff[br.t0]);
-        }
-    }
     std::reverse(plan.begin(), plan.end());   // used as a stack
     CK(c.masks.ensure(maxMaskWords));
     CK(c.colMasks.ensure(maxColWords));
@@ -977,15 +940,15 @@ sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
     a.taskEvals = c.dTaskEvals.p;
     a.taskRefined = c.dTaskRefined.p;
     a.masks = c.masks.p;
-    a.maskOff = c.dMaskOff.p;
+    a.maskOff = reinterpret_cast<const uint64_t *>(c.off[0].p);
     a.colMasks = c.colMasks.p;
-    a.colOff = c.dColOff.p;
+    a.colOff = reinterpret_cast<const uint64_t *>(c.off[1].p);
     a.rowRel = c.rowRel.p;
-    a.rowOff = c.dRowOff.p;
+    a.rowOff = reinterpret_cast<const uint64_t *>(c.off[2].p);
     a.candId = c.candId.p;
     a.candRel = c.candRel.p;
-    a.candOff = c.dCandOff.p;
-    a.unitOff = c.dUnitOff.p;
+    a.candOff = reinterpret_cast<const uint64_t *>(c.off[3].p);
+    a.unitOff = reinterpret_cast<const uint64_t *>(c.off[4].p);
     {
         const FilterBounds fb = filter_bounds(c);
         a.margin = fb.margin;
@@ -993,7 +956,7 @@ sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
     }
 
     std::vector<uint32_t> hTaskHits(nt);
-    uint64_t pairsTotal = 0, batches = 0, retries = 0;
+    uint64_t pairsTotal = 0, batches = 0, retries = 0, errBatches = 0;
     double relErrSum = 0;
     float msCount = 0, msScan = 0, msFill = 0, msDeliver = 0, msExpand = 0;
     int pinSel = 0;
@@ -1001,10 +964,12 @@ sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
     CK(c.batchTot.ensure(plan.size() + 1));
     CK(cudaMemsetAsync(c.batchTot.p, 0, sizeof(unsigned long long) * (plan.size() + 1), c.s));
     CK(cudaMemsetAsync(c.keyCount.p, 0, sizeof(uint32_t) * n, c.s));   // each scan clears it again
-    auto predOf = [&](const BatchRange &br) {
-        double p = 0;
-        for (uint32_t t = br.t0; t < br.t1; t++) p += c.taskPred[t];
-        return p;
+    // estimator error of a planned batch against its measured pairs
+    auto noteErr = [&](const BatchRange &br, uint64_t measured) {
+        if (br.pred >= 0 && measured > 0) {
+            relErrSum += std::fabs(br.pred - (double)measured) / (double)measured;
+            errBatches++;
+        }
     };
 
     // ---- asynchronous phase: batches folded on the device (no host delivery).
@@ -1014,7 +979,7 @@ sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
     std::vector<BatchRange> stack;
     if (delivery == SJ_DELIVER_NONE && !plan.empty()) {
         double maxPred = 0;
-        for (const BatchRange &br : plan) maxPred = std::max(maxPred, predOf(br) * (1.0 + c.p.alpha));
+        for (const BatchRange &br : plan) maxPred = std::max(maxPred, br.pred * (1.0 + c.p.alpha));
         uint64_t bufCap = c.p.batch_capacity_pairs ? cap
                                                    : std::min<uint64_t>(cap, (uint64_t)(1.25 * maxPred) + 65536);
         if (bufCap > c.outKey.n) {
@@ -1029,9 +994,11 @@ sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
         // Two streams when the device has room for a second record set: the
         // count pass and scan of each batch on the engine's stream, its key
         // expansion, emission and fold on the second stream, so batch i + 1's
-        // count pass runs beside batch i's emission (and the launch tails of
-        // each stage fill with the other's work).  Batch i + 1's scan waits
-        // for batch i's emission: both use keyStart and the scan total.
+        // count pass and scan run beside batch i's emission (and the launch
+        // tails of each stage fill with the other's work).  Batches alternate
+        // between two sets of count-pass records and two sets of key offsets
+        // and scan totals; batch i's count pass waits for batch i - 2's
+        // emission, the last reader of the set it reuses.
         bool pipe = nplan > 1;
         if (pipe) {
             cudaError_t e = c.masks2.ensure(maxMaskWords);
@@ -1040,6 +1007,8 @@ sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
             if (e == cudaSuccess) e = c.candId2.ensure(maxCandRecs);
             if (e == cudaSuccess) e = c.candRel2.ensure(maxCandRecs);
             if (e == cudaSuccess) e = c.emitHead.ensure(1);
+            if (e == cudaSuccess) e = c.keyStart2.ensure(n);
+            if (e == cudaSuccess) e = c.total2.ensure(1);
             if (e != cudaSuccess) {
                 // no room for the second set: the batches run one after another
                 cudaGetLastError();
@@ -1048,6 +1017,7 @@ sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
                 c.rowRel2.release();
                 c.candId2.release();
                 c.candRel2.release();
+                c.keyStart2.release();
                 pipe = false;
             }
         }
@@ -1074,23 +1044,27 @@ sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
             b.taskBegin = br.t0;
             b.taskEnd = br.t1;
             b.batchPairs = c.batchTot.p + i;
-            if (pipe && (i & 1)) {
+            const bool second = pipe && (i & 1);
+            uint32_t *const scanTot = second ? c.total2.p : c.total.p;
+            if (second) {
                 b.masks = c.masks2.p;
                 b.colMasks = c.colMasks2.p;
                 b.rowRel = c.rowRel2.p;
                 b.candId = c.candId2.p;
                 b.candRel = c.candRel2.p;
+                b.keyStart = c.keyStart2.p;
             }
+            if (pipe && i > 1) CK(cudaStreamWaitEvent(sA, ev[EV * (i - 2) + 6], 0));   // set reused: emission i-2 done
             CK(cudaEventRecord(e[0], sA));
             CKS(run_count(c, b, queue, sA));
             CK(cudaEventRecord(e[1], sA));
-            if (pipe && i > 0) CK(cudaStreamWaitEvent(sA, ev[EV * (i - 1) + 6], 0));   // previous emission done
             CK(cudaEventRecord(e[2], sA));
-            CK(sj_exclusive_scan_u32_clear(c.keyCount.p, c.keyStart.p, n, c.scanTemp.p, c.total.p, sA));
+            CK(sj_exclusive_scan_u32_clear(c.keyCount.p, const_cast<uint32_t *>(b.keyStart), n, c.scanTemp.p, scanTot,
+                                           sA));
             CK(cudaEventRecord(e[3], sA));
             if (pipe) CK(cudaStreamWaitEvent(sB, e[3], 0));
             CK(cudaEventRecord(e[4], sB));
-            CKS(expand_keys(c, b, sB));
+            CKS(expand_keys(c, b, sB, scanTot));
             CK(cudaEventRecord(e[5], sB));
             b.queueHead = pipe ? c.emitHead.p : c.queueHead.p;
             CK(cudaMemsetAsync(b.queueHead, 0, sizeof(uint32_t), sB));
@@ -1124,6 +1098,7 @@ sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
         std::vector<BatchRange> redo;
         for (size_t i = 0; i < nplan; i++) {
             const BatchRange &br = plan[nplan - 1 - i];
+            noteErr(br, tot[i]);   // the count pass measured the batch exactly, overflowed or not
             if (tot[i] > bufCap) {
                 // the count pass measured every task's pairs: re-plan this
                 // batch's tasks exactly, so the re-runs cannot overflow again
@@ -1131,7 +1106,6 @@ sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
                 retries++;
                 continue;
             }
-            if (tot[i] > 0) relErrSum += std::fabs(predOf(br) - (double)tot[i]) / (double)tot[i];
             pairsTotal += tot[i];
             batches++;
         }
@@ -1202,6 +1176,7 @@ sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
                            cudaMemcpyDeviceToHost, c.s));
         CK(cudaStreamSynchronize(c.s));
         memcpy(&cnt, c.pinTotal.p, sizeof(cnt));
+        noteErr(br, cnt);
         if (cnt > cap) {
             // estimate too low: re-plan the batch from the measured per-task
             // pairs (the scan already cleared the counts)
@@ -1213,7 +1188,6 @@ sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
             iter++;
             continue;
         }
-        if (cnt > 0) relErrSum += std::fabs(predOf(br) - (double)cnt) / (double)cnt;
         // output buffers follow the exact batch size (grow-only, 25% headroom, <= capacity)
         if (cnt > c.outKey.n) {
             CKS(finishPending());   // its copy may still read the old buffers
@@ -1316,33 +1290,26 @@ sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
         return SJ_ERR_INTERNAL;
     }
     {
-        std::vector<uint32_t> ev(nt), rf(nt);
-        if (nt) {
-            CK(cudaMemcpyAsync(ev.data(), c.dTaskEvals.p, sizeof(uint32_t) * nt, cudaMemcpyDeviceToHost, c.s));
-            CK(cudaMemcpyAsync(rf.data(), c.dTaskRefined.p, sizeof(uint32_t) * nt, cudaMemcpyDeviceToHost, c.s));
-            CK(cudaStreamSynchronize(c.s));
-        }
-        uint64_t se = 0, sr = 0;
-        for (uint32_t t = 0; t < nt; t++) {
-            se += ev[t];
-            sr += rf[t];
-        }
-        c.st.distance_calcs = se;
-        c.st.refined_pairs = sr;
+        // evaluations, FP32 re-evaluations, measured pairs and the predicted
+        // pairs' error, summed over the tasks on the device
+        CK(c.sums.ensure(3));
+        CK(c.errSum.ensure(1));
+        CK(sj_task_sums(c.dTaskEvals.p, c.dTaskRefined.p, c.taskHits.p, c.dTaskPred.p, nt, c.sums.p, c.errSum.p,
+                        c.numSM, c.s));
+        unsigned long long sm[3];
+        double err = 0;
+        CK(cudaMemcpyAsync(sm, c.sums.p, sizeof(sm), cudaMemcpyDeviceToHost, c.s));
+        CK(cudaMemcpyAsync(&err, c.errSum.p, sizeof(double), cudaMemcpyDeviceToHost, c.s));
+        CK(cudaStreamSynchronize(c.s));
+        c.st.distance_calcs = sm[0];
+        c.st.refined_pairs = sm[1];
+        c.st.estimator_task_rel_err = sm[2] ? err / (double)sm[2] : 0.0;
     }
     c.st.total_pairs = pairsTotal;
     c.st.pair_hash = hs[4];
     c.st.num_batches = batches;
     c.st.overflow_retries = retries;
-    c.st.estimator_mean_abs_rel_err = batches ? relErrSum / (double)batches : 0.0;
-    {
-        double num = 0, den = 0;
-        for (uint32_t t = 0; t < nt; t++) {
-            num += std::fabs(c.taskPred[t] - (double)hTaskHits[t]);
-            den += (double)hTaskHits[t];
-        }
-        c.st.estimator_task_rel_err = den > 0 ? num / den : 0.0;
-    }
+    c.st.estimator_mean_abs_rel_err = errBatches ? relErrSum / (double)errBatches : 0.0;
     c.st.ms_count = msCount;
     c.st.ms_scan = msScan;
     c.st.ms_fill = msFill;
@@ -1362,10 +1329,8 @@ sj_status run_degrees(Ctx &c, uint32_t *degHost)
     bool queue;
     CKS(prepare_join(c, pattern, queue));
     const uint64_t n = c.n;
-    CKS(build_tasks(c, pattern, 0xffffffffULL, false));
-    const uint32_t nt = (uint32_t)c.tasks.size();
-    CK(c.dTasks.ensure(nt));
-    if (nt) CK(cudaMemcpyAsync(c.dTasks.p, c.tasks.data(), sizeof(sj_task) * nt, cudaMemcpyHostToDevice, c.s));
+    CKS(build_tasks_dev(c, pattern != SJ_PAT_FULL, 0xffffffffULL, false, 0, 0.0f, true));
+    const uint32_t nt = c.nTasks;
     CK(c.keyCount.ensure(n));
     CK(c.stat.ensure(8));
     CK(c.queueHead.ensure(1));
@@ -1389,37 +1354,23 @@ sj_status run_degrees(Ctx &c, uint32_t *degHost)
     a.taskBegin = 0;
     a.taskEnd = nt;
     CKS(run_count(c, a, true));
-    std::vector<uint32_t> ev(nt), rf(nt);
-    if (nt) {
-        CK(cudaMemcpyAsync(ev.data(), c.dTaskEvals.p, sizeof(uint32_t) * nt, cudaMemcpyDeviceToHost, c.s));
-        CK(cudaMemcpyAsync(rf.data(), c.dTaskRefined.p, sizeof(uint32_t) * nt, cudaMemcpyDeviceToHost, c.s));
-    }
+    // per-cell measured hits (the sum of the cell's points' degrees)
+    CK(c.dCellHits.ensure(c.nCells ? c.nCells : 1));
+    CK(sj_cell_hits(c.cellStart.p, c.ids.p, c.keyCount.p, c.nCells, c.dCellHits.p, c.s));
+    CK(c.sums.ensure(3));
+    CK(sj_task_sums(c.dTaskEvals.p, c.dTaskRefined.p, nullptr, nullptr, nt, c.sums.p, nullptr, c.numSM, c.s));
     std::vector<uint32_t> deg(n);
     CK(cudaMemcpyAsync(deg.data(), c.keyCount.p, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost, c.s));
-    std::vector<uint32_t> ids(n);
-    CK(cudaMemcpyAsync(ids.data(), c.ids.p, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost, c.s));
-    unsigned long long hs[8];
-    CK(cudaMemcpyAsync(hs, c.stat.p, sizeof(hs), cudaMemcpyDeviceToHost, c.s));
+    unsigned long long sm[3];
+    CK(cudaMemcpyAsync(sm, c.sums.p, sizeof(sm), cudaMemcpyDeviceToHost, c.s));
     CK(cudaStreamSynchronize(c.s));
     if (degHost) memcpy(degHost, deg.data(), sizeof(uint32_t) * n);
-    // per-cell measured hits (sum of the cell's points' degrees)
-    c.measCellHits.assign(c.nCells, 0.0);
-    for (uint32_t A = 0; A < c.nCells; A++) {
-        double s = 0;
-        for (uint32_t p = c.hCellStart[A]; p < c.hCellStart[A + 1]; p++) s += deg[ids[p]];
-        c.measCellHits[A] = s;
-    }
     c.haveMeas = true;
     uint64_t tot = 0;
     for (uint64_t i = 0; i < n; i++) tot += deg[i];
     c.st.total_pairs = tot;
-    uint64_t se = 0, sr = 0;
-    for (uint32_t t = 0; t < nt; t++) {
-        se += ev[t];
-        sr += rf[t];
-    }
-    c.st.distance_calcs = se;
-    c.st.refined_pairs = sr;
+    c.st.distance_calcs = sm[0];
+    c.st.refined_pairs = sm[1];
     return SJ_OK;
 }
 
@@ -1638,11 +1589,14 @@ sj_status sj_index_export(void *ctx, unsigned int *indexLookupArr, sj_grid *grid
     CKS(bind(c));
     const uint32_t nc = c.nCells;
     if (indexLookupArr) CK(cudaMemcpy(indexLookupArr, c.ids.p, sizeof(uint32_t) * c.n, cudaMemcpyDeviceToHost));
-    if (grid)
+    if (grid) {
+        std::vector<uint32_t> cs(nc + 1);
+        CK(cudaMemcpy(cs.data(), c.cellStart.p, sizeof(uint32_t) * (nc + 1), cudaMemcpyDeviceToHost));
         for (uint32_t i = 0; i < nc; i++) {
-            grid[i].indexmin = (int)c.hCellStart[i];
-            grid[i].indexmax = (int)c.hCellStart[i + 1] - 1;
+            grid[i].indexmin = (int)cs[i];
+            grid[i].indexmax = (int)cs[i + 1] - 1;
         }
+    }
     if (lookup) {
         std::vector<uint64_t> lid(nc);
         CK(cudaMemcpy(lid.data(), c.cellLid.p, sizeof(uint64_t) * nc, cudaMemcpyDeviceToHost));
@@ -1869,14 +1823,20 @@ sj_status sj_cell_features(void *ctx, float *feat, double *hits, double *calcs)
     if (c.nbrPattern < 0) CKS(build_neighbours(c, pattern_of_mode(c.p.search_mode)));
     if (feat)
         CK(cudaMemcpy(feat, c.feat.p, sizeof(float) * (size_t)c.nCells * SJ_NFEAT, cudaMemcpyDeviceToHost));
-    if (calcs)
-        for (uint32_t i = 0; i < c.nCells; i++) calcs[i] = (double)c.hCandFull[i];
+    const uint32_t nc = c.nCells;
+    if (calcs) {
+        std::vector<uint64_t> v(nc);
+        CK(cudaMemcpy(v.data(), c.candFull.p, sizeof(uint64_t) * nc, cudaMemcpyDeviceToHost));
+        for (uint32_t i = 0; i < nc; i++) calcs[i] = (double)v[i];
+    }
     if (hits) {
         if (!c.haveMeas) {
             set_error("no measured counts: run sj_degrees first");
             return SJ_ERR_STATE;
         }
-        for (uint32_t i = 0; i < c.nCells; i++) hits[i] = c.measCellHits[i];
+        std::vector<unsigned long long> v(nc);
+        CK(cudaMemcpy(v.data(), c.dCellHits.p, sizeof(unsigned long long) * nc, cudaMemcpyDeviceToHost));
+        for (uint32_t i = 0; i < nc; i++) hits[i] = (double)v[i];
     }
     return SJ_OK;
 }

@@ -56,6 +56,16 @@ constexpr uint32_t FULL = 0xffffffffu;
 #define SJ_EMIT_UNROLL 4
 #endif
 constexpr int CO = SJ_EMIT_UNROLL;  // copy-out entries per lane whose loads are in flight together
+// Mask windows (rows) / query groups (columns) whose words are loaded ahead of
+// the one being decoded: the emission reads the hit masks once, in order, so
+// its loads can run this far ahead of the decode.
+#ifndef SJ_EMIT_PF
+#define SJ_EMIT_PF 4
+#endif
+constexpr int PF = SJ_EMIT_PF;
+#ifndef SJ_EMIT_MINB
+#define SJ_EMIT_MINB 4
+#endif
 
 struct WarpSmem {
     uint16_t ent[EM_CAP];   // staged entries in slot order: rows (query << 11) | chunk position,
@@ -190,15 +200,28 @@ __device__ __forceinline__ void emit_rows(const sj_join_args &a, const UnitTask 
         __syncwarp();
         w.start[lane] = next;
         uint32_t carry = 0;   // entries of earlier windows of this chunk
-        // a window is 64 words: lane L holds words L and 32 + L (the next
-        // window's words are in flight while this one is written)
-        uint32_t n0 = lane < nw ? __ldg(wq + lane) : 0u;
-        uint32_t n1 = lane + 32 < nw ? __ldg(wq + lane + 32) : 0u;
+        // a window is 64 words: lane L holds words L and 32 + L; the words of
+        // the next PF windows are in flight while this one is written
+        uint32_t pw[PF][2];
+#pragma unroll
+        for (int k = 0; k < PF; k++) {
+            const uint32_t f = 64u * k + lane;
+            pw[k][0] = f < nw ? __ldg(wq + f) : 0u;
+            pw[k][1] = f + 32 < nw ? __ldg(wq + f + 32) : 0u;
+        }
         for (uint32_t ws = 0; ws < nw; ws += 64) {
             const uint32_t fa = ws + lane, fb = fa + 32;
-            uint32_t wa = n0, wb = n1;
-            n0 = fa + 64 < nw ? __ldg(wq + fa + 64) : 0u;
-            n1 = fb + 64 < nw ? __ldg(wq + fb + 64) : 0u;
+            uint32_t wa = pw[0][0], wb = pw[0][1];
+#pragma unroll
+            for (int k = 0; k + 1 < PF; k++) {
+                pw[k][0] = pw[k + 1][0];
+                pw[k][1] = pw[k + 1][1];
+            }
+            {
+                const uint32_t f = fa + 64u * PF;
+                pw[PF - 1][0] = f < nw ? __ldg(wq + f) : 0u;
+                pw[PF - 1][1] = f + 32 < nw ? __ldg(wq + f + 32) : 0u;
+            }
             const uint32_t qa = (uint32_t)(((uint64_t)fa * magic) >> 32);
             const uint32_t qb = (uint32_t)(((uint64_t)fb * magic) >> 32);
             const uint32_t ra = fa - qa * cb, rb = fb - qb * cb;   // block of each word in the chunk
@@ -270,10 +293,15 @@ __device__ __forceinline__ void emit_cols(const sj_join_args &a, const UnitTask 
     if (s < u.L) {
         slot = a.keyStart[a.candId[rec + s]] + a.candRel[rec + s];
     }
-    uint32_t word = __ldg(cw);
+    // the words of the next PF query groups are in flight while one is written
+    uint32_t pw[PF];
+#pragma unroll
+    for (int k = 0; k < PF; k++) pw[k] = (uint32_t)k < nG ? __ldg(cw + k * 32) : 0u;
     for (uint32_t g = 0; g < nG; g++) {
-        uint32_t cur = word;
-        if (g + 1 < nG) word = __ldg(cw + (g + 1) * 32);   // in flight while this group is written
+        uint32_t cur = pw[0];
+#pragma unroll
+        for (int k = 0; k + 1 < PF; k++) pw[k] = pw[k + 1];
+        pw[PF - 1] = g + PF < nG ? __ldg(cw + (uint64_t)(g + PF) * 32) : 0u;
         {
             // positions past the stream end and queries past the tile have no
             // bits in a consistent count pass
@@ -304,7 +332,7 @@ __device__ __forceinline__ void emit_cols(const sj_join_args &a, const UnitTask 
     }
 }
 
-__global__ void __launch_bounds__(EW, 5) k_emit(sj_join_args a)
+__global__ void __launch_bounds__(EW, SJ_EMIT_MINB) k_emit(sj_join_args a)
 {
     __shared__ WarpSmem smem[ENW];
     const uint32_t lane = threadIdx.x & 31u;

@@ -1,63 +1,14 @@
-// Result-size estimators that size the result batches and order the work.
-//
-// Sampling estimator: the reference counts the full-stencil hits of every
-// 100th point (kernelNDGridIndexBatchEstimatorOLD, kernel.cu:602-781;
-// GPU.cu:854-1065) and scales the total.  Here the sampled points also give a
-// per-cell hit rate (hits per candidate evaluation over the cell's own
-// candidate stream), which the planner multiplies by each task's exact
-// evaluation count.
-//
-// Learned estimator: a 16 -> 64 -> 64 -> 2 ReLU MLP on per-cell features
-// predicts log2(1 + distance calcs) and log2(1 + hits) of a cell.  Forward,
-// backward and Adam are plain FP32 CUDA-core kernels (the network is tiny).
+// Learned result-size estimator: a 16 -> 64 -> 64 -> 2 ReLU MLP on per-cell
+// features predicts log2(1 + distance calcs) and log2(1 + hits) of a cell.
+// Forward, backward and Adam are plain FP32 CUDA-core kernels (the network is
+// tiny).  The sampling estimator it replaces (GPU.cu:854-1065, which counts
+// the hits of every 100th point) runs as the join's own count pass over
+// tasks for the sampled points (sj_tasks.cu builds them, sj_api.cpp runs it).
 #include <mutex>
 
 #include "sj_internal.h"
 
 namespace {
-
-// One warp per sampled query position; lanes stride over the candidate stream
-// (whole home cell + owned neighbour cells).
-__global__ void __launch_bounds__(256) k_sample(sj_join_args a, sj_grid_dev g, uint32_t stride, uint32_t nPoints,
-                                                uint32_t nCells, unsigned long long *cellHits,
-                                                unsigned long long *cellCands)
-{
-    uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    uint32_t lane = threadIdx.x & 31u;
-    uint64_t pos = (uint64_t)gw * stride;
-    if (pos >= nPoints) return;
-    // cell of this position: largest c with cellStart[c] <= pos
-    uint32_t lo = 0, hi = nCells;
-    while (hi - lo > 1) {
-        uint32_t mid = (lo + hi) >> 1;
-        if (a.cellStart[mid] <= pos) lo = mid; else hi = mid;
-    }
-    const uint32_t A = lo;
-    double q[SJ_MAX_DIM];
-    for (int l = 0; l < g.Dp; l++) q[l] = a.xs[pos * g.Dp + l];
-    unsigned long long hits = 0, cands = 0;
-    uint32_t nn = a.nbrStart[A + 1] - a.nbrStart[A];
-    for (uint32_t s = 0; s <= nn; s++) {
-        uint32_t B = (s == 0) ? A : a.nbrCell[a.nbrStart[A] + s - 1];
-        uint32_t b0 = a.cellStart[B], b1 = a.cellStart[B + 1];
-        for (uint32_t c = b0 + lane; c < b1; c += 32) {
-            const double *x = a.xs + (uint64_t)c * g.Dp;
-            double acc = 0.0;   // estimate only: plain fma chain
-            for (int l = 0; l < g.Dp; l++) {
-                double d = __dsub_rn(x[l], q[l]);
-                acc = __fma_rn(d, d, acc);
-            }
-            hits += (acc <= g.thresh);
-        }
-        cands += (b1 - b0);
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) hits += __shfl_xor_sync(0xffffffffu, hits, o);
-    if (lane == 0) {
-        atomicAdd(&cellHits[A], hits);
-        atomicAdd(&cellCands[A], cands);
-    }
-}
 
 // ------------------------------------------------------------------ MLP ----
 // parameter offsets
@@ -194,17 +145,7 @@ __global__ void k_adam(float *__restrict__ w, const float *__restrict__ g, float
 
 }  // namespace
 
-cudaError_t sj_launch_sample(const sj_join_args &a, const sj_grid_dev &g, uint32_t sampleStride,
-                             unsigned long long *cellHits, unsigned long long *cellCands, uint32_t nCells,
-                             cudaStream_t s)
-{
-    uint32_t nPoints = a.taskEnd;   // caller passes n here
-    uint64_t nSamples = (nPoints + (uint64_t)sampleStride - 1) / sampleStride;
-    if (nSamples == 0) return cudaSuccess;
-    uint64_t blocks = (nSamples * 32 + 255) / 256;
-    k_sample<<<(unsigned)blocks, 256, 0, s>>>(a, g, sampleStride, nPoints, nCells, cellHits, cellCands); sj_note_launch();
-    return cudaGetLastError();
-}
+
 
 cudaError_t sj_launch_mlp_infer(const float *feat, uint32_t nCells, const float *weights, float *out, cudaStream_t s)
 {

@@ -76,8 +76,12 @@ __global__ void k_minmax_decode(unsigned long long *mm, int D)
 }
 
 // Cell coordinate (main.cu:294, kernel.cu:1457) and linear id (main.cu:423-439).
+// A coordinate at or past its dimension's cell count (which the grid's eps
+// margins rule out up to rounding) would alias another cell's linear id: it
+// sets *outOfGrid, and the host refuses the index.
 __global__ void __launch_bounds__(256) k_cell_keys(const double *__restrict__ pts, uint64_t n, sj_grid_dev g,
-                                                   uint64_t *__restrict__ keys, uint32_t *__restrict__ vals)
+                                                   uint64_t *__restrict__ keys, uint32_t *__restrict__ vals,
+                                                   uint32_t *__restrict__ outOfGrid)
 {
     uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -85,6 +89,7 @@ __global__ void __launch_bounds__(256) k_cell_keys(const double *__restrict__ pt
     for (int j = 0; j < g.k; j++) {
         double x = pts[i * g.D + j];
         unsigned c = __double2uint_rz(__ddiv_rn(__dsub_rn(x, g.minArr[j]), g.eps));
+        if (c >= g.nCells[j]) atomicOr(outOfGrid, 1u);
         lid += (unsigned long long)c * mul;
         mul *= g.nCells[j];
     }
@@ -154,9 +159,9 @@ cudaError_t sj_launch_minmax(const double *pts, uint64_t n, int D, double *minma
 }
 
 cudaError_t sj_launch_cell_keys(const double *pts, uint64_t n, sj_grid_dev g, uint64_t *keys, uint32_t *vals,
-                                cudaStream_t s)
+                                uint32_t *outOfGrid, cudaStream_t s)
 {
-    k_cell_keys<<<blocks_for(n, 256), 256, 0, s>>>(pts, n, g, keys, vals); sj_note_launch();
+    k_cell_keys<<<blocks_for(n, 256), 256, 0, s>>>(pts, n, g, keys, vals, outOfGrid); sj_note_launch();
     return cudaGetLastError();
 }
 

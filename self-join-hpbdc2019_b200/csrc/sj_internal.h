@@ -115,6 +115,23 @@ __host__ __device__ inline uint64_t sj_row_mask_index(uint32_t b, uint32_t qi, u
     return (uint64_t)64 * c * qc + (uint64_t)qi * cb + (b & 63);
 }
 
+// Parameters of the device task builder (sj_tasks.cu).
+struct sj_taskgen {
+    const uint32_t *cellStart;   // nCells+1
+    const uint32_t *nbrStart;    // nCells+1, owned neighbour lists
+    const uint32_t *nbrCell;
+    const float *rate;           // per cell predicted hits per evaluation (null: 0)
+    const uint32_t *groupBase;   // per cell: first slot in groupLen (exclusive scan of segment groups)
+    uint32_t *groupLen;          // per segment group: stream length without the home segment
+    uint32_t nCells;
+    uint32_t tile;               // query points per task (SJ_CTA x query slots)
+    uint64_t cap;                // batch capacity: a task's worst case must fit
+    double pairsPerTask;         // chunking target of policy 0
+    int sym;                     // symmetric traversal (owned neighbours, both directions emitted)
+    int policy;                  // 0 cost-proportional chunks, 1 fixed 65536, 2 mode-8 split by thirds of the work
+    float sampleRate;            // > 0: tasks for the sampled queries of each cell only (sampling estimator)
+};
+
 // Kernel launches made by this library since load (every launcher calls
 // sj_note_launch() after each <<<...>>>; bench and tests read the total).
 void sj_note_launch();
@@ -158,7 +175,7 @@ cudaError_t sj_csr_append(const uint32_t *start, const uint32_t *total, uint64_t
 // index build (sj_index.cu)
 cudaError_t sj_launch_minmax(const double *pts, uint64_t n, int D, double *minmax_dev, cudaStream_t s);
 cudaError_t sj_launch_cell_keys(const double *pts, uint64_t n, sj_grid_dev g, uint64_t *keys, uint32_t *vals,
-                                cudaStream_t s);
+                                uint32_t *outOfGrid, cudaStream_t s);
 cudaError_t sj_launch_cell_flags(const uint64_t *keys, uint64_t n, uint32_t *flags, cudaStream_t s);
 cudaError_t sj_launch_cell_build(const uint64_t *keys, const uint32_t *cellIdxExcl, uint64_t n,
                                  uint32_t *cellStart, uint64_t *cellLid, cudaStream_t s);
@@ -168,10 +185,12 @@ cudaError_t sj_launch_cell_coords(const uint64_t *cellLid, uint32_t nCells, sj_g
                                   cudaStream_t s);
 
 // neighbour lists and features (sj_stencil.cu)
+// pass 0: owned-neighbour counts, full-stencil candidates per cell (and their
+// total, added to *candTotal) and features; pass 1: the owned lists
 cudaError_t sj_launch_neighbours(const uint64_t *cellLid, const uint32_t *cellCoord, const uint32_t *cellStart,
                                  uint32_t nCells, sj_grid_dev g, int pattern, const uint32_t *nbrStart,
-                                 uint32_t *nbrCountOrCell, uint64_t *candFull, float *feat, int pass,
-                                 cudaStream_t s);
+                                 uint32_t *nbrCountOrCell, uint64_t *candFull, unsigned long long *candTotal,
+                                 float *feat, int pass, cudaStream_t s);
 
 // join (sj_join.cu): the count pass (per-key pair counts, hit masks)
 cudaError_t sj_launch_join(const sj_join_args &a, const sj_grid_dev &g, int fp32, int queue, int numSM,
@@ -187,10 +206,54 @@ __host__ __device__ inline uint32_t sj_task_units(uint32_t qCount, uint32_t stre
     return (qCount + 31) / 32 + (sym ? (streamLen + 31) / 32 : 0u);
 }
 
+// device task builder (sj_tasks.cu)
+cudaError_t sj_tg_groups(const sj_taskgen &g, uint32_t *cnt, cudaStream_t s);
+cudaError_t sj_tg_cells(const sj_taskgen &g, const uint32_t *order, const uint8_t *workersAt, uint32_t *posCnt,
+                        unsigned long long *posEv, unsigned long long *costKey, unsigned long long *totals,
+                        cudaStream_t s);
+cudaError_t sj_iota_u32(uint32_t *v, uint32_t n, cudaStream_t s);
+// mode 8: workers per position from the exclusive prefix of the evaluations
+// in cost order (evExcl[n] = total): 16, 8 or 2 by third of the work
+cudaError_t sj_tg_thirds(const unsigned long long *evExcl, uint32_t n, uint8_t *workers, cudaStream_t s);
+cudaError_t sj_tg_item_counts(const sj_taskgen &g, const uint32_t *order, uint32_t *items, cudaStream_t s);
+cudaError_t sj_tg_item_tasks(const sj_taskgen &g, const uint32_t *order, const uint8_t *workersAt,
+                             const uint32_t *itemStart, uint32_t nItems, uint32_t *itemTasks, cudaStream_t s);
+cudaError_t sj_tg_item_write(const sj_taskgen &g, const uint32_t *order, const uint8_t *workersAt,
+                             const uint32_t *itemStart, uint32_t nItems, const uint32_t *itemTaskStart,
+                             sj_task *tasks, float *pred, cudaStream_t s);
+cudaError_t sj_tg_shard(const sj_task *in, const float *predIn, uint32_t nOut, uint32_t idx, uint32_t cnt,
+                        sj_task *out, float *predOut, cudaStream_t s);
+// record offsets of a task list: out[0..6] = row-mask words, column-mask words,
+// row offsets, candidate records, emission units, planned pairs
+// (ceil(pred * (1 + alpha))), predicted pairs (rounded); each nt+1 entries
+// (exclusive prefix, total last).  temp: sj_task_offsets_temp(nt) entries.
+size_t sj_task_offsets_temp(uint32_t nt);
+cudaError_t sj_task_offsets(const sj_task *tasks, const float *pred, uint32_t nt, double alpha,
+                            unsigned long long *temp, unsigned long long *const out[7], cudaStream_t s);
+// greedy batch plan over the offsets: start[0..nb] (start[nb] = nt), *nBatches
+cudaError_t sj_plan_batches(unsigned long long *const off[7], uint32_t nt, unsigned long long cap,
+                            unsigned long long maskLim, uint32_t *next, uint32_t *start, uint32_t *nBatches,
+                            cudaStream_t s);
+// per batch: predicted pairs, row-mask words, column-mask words, row offsets, candidate records
+cudaError_t sj_plan_stats(const uint32_t *start, uint32_t nb, unsigned long long *const off[7],
+                          unsigned long long *stats, cudaStream_t s);
+cudaError_t sj_rates_mlp(const float *out, const unsigned long long *candFull, uint32_t nCells, float *rate,
+                         cudaStream_t s);
+cudaError_t sj_sample_rates(const sj_task *tasks, uint32_t nt, const uint32_t *taskHits, const uint32_t *taskEvals,
+                            unsigned long long *cellHits, unsigned long long *cellEvals, unsigned long long *totals,
+                            uint32_t nCells, float *rate, cudaStream_t s);
+// sums[0] evaluations, [1] refined, [2] measured pairs; *errSum = sum |pred - measured|
+cudaError_t sj_task_sums(const uint32_t *taskEvals, const uint32_t *taskRefined, const uint32_t *taskHits,
+                         const float *pred, uint32_t nt, unsigned long long *sums, double *errSum, int numSM,
+                         cudaStream_t s);
+cudaError_t sj_cell_hits(const uint32_t *cellStart, const uint32_t *ids, const uint32_t *deg, uint32_t nCells,
+                         unsigned long long *hits, cudaStream_t s);
+// exclusive scan of n u64 values (out has n+1 entries, out[n] = total); temp: sj_scan64_temp(n) entries
+size_t sj_scan64_temp(uint64_t n);
+cudaError_t sj_exclusive_scan_u64(const unsigned long long *in, unsigned long long *out, uint64_t n,
+                                  unsigned long long *temp, cudaStream_t s);
+
 // estimators (sj_estimate.cu)
-cudaError_t sj_launch_sample(const sj_join_args &a, const sj_grid_dev &g, uint32_t sampleStride,
-                             unsigned long long *cellHits, unsigned long long *cellCands, uint32_t nCells,
-                             cudaStream_t s);
 cudaError_t sj_launch_mlp_infer(const float *feat, uint32_t nCells, const float *weights, float *out,
                                 cudaStream_t s);
 cudaError_t sj_launch_mlp_train_step(const float *x, const float *y, uint32_t m, float *weights, float *grad,

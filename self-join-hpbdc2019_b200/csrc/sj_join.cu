@@ -100,14 +100,17 @@ __device__ __forceinline__ uint32_t push_sign(uint32_t mask, float v)
 
 // FP32 filter over one block of 32 staged candidates for slots 0..RR-1.
 //   y = (|b|^2 - tLo) + sum_l (-2 a_l) b_l      (packed f32x2: two candidates per op)
-//   z = y - delta
-// hit bit  <- sign(y): y <= 0 proves the FP64 predicate true;
-// near bit <- sign(z): z >= 0 proves it false; near & ~hit is the borderline band.
-// Bits are shifted in from candidate 31 down to 0, so bit i is candidate i.
+// hit bit <- sign(y): y < 0 proves the FP64 predicate true; y >= delta proves
+// it false; 0 <= y < delta is the borderline band.  Bits are shifted in from
+// candidate 31 down to 0, so bit i is candidate i.  Instead of a second
+// comparison per candidate, lo[r] keeps the smallest bit pattern of y over the
+// block: a y in [0, delta) has a smaller pattern than delta's (non-negative
+// floats order like their bits; negative ones have the sign bit and never win
+// the unsigned minimum), so ymin < bits(delta) tells that the block has a
+// borderline candidate, which near_bits() then finds.
 template <int DP, int RR, int R>
 __device__ __forceinline__ void eval_block_f32(const Stage32<DP> &st, uint32_t pb, const float2 (&qa)[R][DP],
-                                               const float2 (&nt)[R], float2 nd, uint32_t (&hit)[R],
-                                               uint32_t (&near)[R])
+                                               const float2 (&nt)[R], uint32_t (&hit)[R], uint32_t (&ymin)[R])
 {
     constexpr int CW2 = Stage32<DP>::CW2;
 #pragma unroll kEvalUnroll
@@ -141,13 +144,34 @@ __device__ __forceinline__ void eval_block_f32(const Stage32<DP> &st, uint32_t p
         }
 #pragma unroll
         for (int r = 0; r < RR; r++) {
-            const float2 z = __fadd2_rn(y[r], nd);
             hit[r] = push_sign(hit[r], y[r].y);
             hit[r] = push_sign(hit[r], y[r].x);
-            near[r] = push_sign(near[r], z.y);
-            near[r] = push_sign(near[r], z.x);
+            ymin[r] = min(ymin[r], min(__float_as_uint(y[r].x), __float_as_uint(y[r].y)));
         }
     }
+}
+
+// Borderline candidates of one block for the query of slot qa/nt: the same
+// FP32 operations as eval_block_f32 in the same order (so y is bitwise the
+// same), one candidate at a time; bit i set when 0 <= y_i < delta.  Runs only
+// for blocks whose minimum says that such a candidate exists.
+template <int DP>
+__device__ __forceinline__ uint32_t near_bits(const Stage32<DP> &st, uint32_t pb, const float2 (&qa)[DP], float2 nt,
+                                           float delta)
+{
+    constexpr int CW2 = Stage32<DP>::CW2;
+    uint32_t m = 0;
+    for (int p = 0; p < 16; p++) {
+        const float *row = reinterpret_cast<const float *>(&st.c[pb + p][0]);
+        for (int h = 0; h < 2; h++) {
+            float y = __fadd_rn(row[h], nt.x);
+#pragma unroll
+            for (int l = 0; l < DP; l++) y = __fmaf_rn(qa[l].x, row[2 * (1 + l) + h], y);
+            if (__float_as_uint(y) < __float_as_uint(delta)) m |= 1u << (2 * p + h);
+        }
+    }
+    (void)CW2;
+    return m;
 }
 
 // FP64 predicate over one block of 32 staged candidates for slots 0..RR-1, in
@@ -359,7 +383,6 @@ __global__ void __launch_bounds__(SJ_CTA, F32 ? SJ_JOIN_MIN_BLOCKS_F32 : SJ_JOIN
                 nt[r] = make_float2(0.f, 0.f);
             }
         }
-        const float2 nd = make_float2(-a.delta, -a.delta);
         const long long T1 = __double_as_longlong(T) + 1;
         uint32_t *const maskBase = a.masks ? a.masks + (a.maskOff[t] - a.maskOff[a.taskBegin]) : nullptr;
         uint32_t *const colBase = (a.colMasks && sym) ? a.colMasks + (a.colOff[t] - a.colOff[a.taskBegin]) : nullptr;
@@ -416,14 +439,14 @@ __global__ void __launch_bounds__(SJ_CTA, F32 ? SJ_JOIN_MIN_BLOCKS_F32 : SJ_JOIN
             for (uint32_t jb = 0; nAct != 0 && jb < nIn; jb += 32) {
                 const uint32_t nb = min(32u, nIn - jb);
                 const uint32_t inRange = (nb == 32) ? 0xffffffffu : ((1u << nb) - 1u);
-                uint32_t hits[R], near[R];
+                uint32_t hits[R], ymin[R];
 #pragma unroll
-                for (int r = 0; r < R; r++) { hits[r] = 0; near[r] = 0; }
+                for (int r = 0; r < R; r++) { hits[r] = 0; ymin[r] = 0xffffffffu; }
                 // branch-free evaluation of the warp's active slots (a partly
                 // active slot set rounds up; the extra slots are ignored below)
                 if constexpr (F32) {
-                    if (nAct == 1) eval_block_f32<DP, 1, R>(st, jb >> 1, qa, nt, nd, hits, near);
-                    else eval_block_f32<DP, R, R>(st, jb >> 1, qa, nt, nd, hits, near);
+                    if (nAct == 1) eval_block_f32<DP, 1, R>(st, jb >> 1, qa, nt, hits, ymin);
+                    else eval_block_f32<DP, R, R>(st, jb >> 1, qa, nt, hits, ymin);
                 } else {
                     if (nAct == 1) eval_block_f64<DP, 1, R>(st, jb, q64, T1, hits);
                     else eval_block_f64<DP, R, R>(st, jb, q64, T1, hits);
@@ -443,20 +466,22 @@ __global__ void __launch_bounds__(SJ_CTA, F32 ? SJ_JOIN_MIN_BLOCKS_F32 : SJ_JOIN
                     const bool qValid = qi < task.qCount;
                     const uint32_t rowValid = qValid ? (hb ? (inRange & row_keep(qi, blk, hb)) : inRange) : 0u;
                     uint32_t h = hits[r];
-                    if (F32) {
-                        uint32_t bm = near[r] & ~h & rowValid;
-                        while (bm) {
-                            const int jj = __ffs(bm) - 1;
-                            bm &= bm - 1;
-                            const uint32_t s = blk + jj;
-                            uint32_t lo = 0, hi = nSeg;
-                            while (hi - lo > 1) {
-                                const uint32_t mid = (lo + hi) >> 1;
-                                if (segPre[mid] <= s) lo = mid; else hi = mid;
+                    if constexpr (F32) {
+                        if (ymin[r] < __float_as_uint(a.delta)) {
+                            uint32_t bm = near_bits<DP>(st, jb >> 1, qa[r], nt[r], a.delta) & ~h & rowValid;
+                            while (bm) {
+                                const int jj = __ffs(bm) - 1;
+                                bm &= bm - 1;
+                                const uint32_t s = blk + jj;
+                                uint32_t lo = 0, hi = nSeg;
+                                while (hi - lo > 1) {
+                                    const uint32_t mid = (lo + hi) >> 1;
+                                    if (segPre[mid] <= s) lo = mid; else hi = mid;
+                                }
+                                const uint32_t cpos = segStart[lo] + (s - segPre[lo]);
+                                refined++;
+                                if (exact_hit<DP>(a.xs, cpos, task.qBegin + qi, T)) h |= 1u << jj;
                             }
-                            const uint32_t cpos = segStart[lo] + (s - segPre[lo]);
-                            refined++;
-                            if (exact_hit<DP>(a.xs, cpos, task.qBegin + qi, T)) h |= 1u << jj;
                         }
                     }
                     evals += __popc(rowValid);

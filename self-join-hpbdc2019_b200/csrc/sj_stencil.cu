@@ -68,8 +68,9 @@ __global__ void __launch_bounds__(128) k_neighbours(const uint64_t *__restrict__
                                                     const uint32_t *__restrict__ cellStart, uint32_t nCells,
                                                     sj_grid_dev g, int pattern,
                                                     const uint32_t *__restrict__ nbrStart, uint32_t *__restrict__ out,
-                                                    uint64_t *__restrict__ candFull, float *__restrict__ feat,
-                                                    int pass)
+                                                    uint64_t *__restrict__ candFull,
+                                                    unsigned long long *__restrict__ candTotal,
+                                                    float *__restrict__ feat, int pass)
 {
     uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= nCells) return;
@@ -135,6 +136,7 @@ __global__ void __launch_bounds__(128) k_neighbours(const uint64_t *__restrict__
     if (pass == 0) {
         out[c] = owned;
         candFull[c] = stencilOcc * (unsigned long long)myOcc;
+        if (candTotal) atomicAdd(candTotal, stencilOcc * (unsigned long long)myOcc);
         if (feat) {
             float *f = feat + (uint64_t)c * SJ_NFEAT;
             float nst = 1.0f;
@@ -157,10 +159,12 @@ __global__ void __launch_bounds__(128) k_neighbours(const uint64_t *__restrict__
 
 cudaError_t sj_launch_neighbours(const uint64_t *cellLid, const uint32_t *cellCoord, const uint32_t *cellStart,
                                  uint32_t nCells, sj_grid_dev g, int pattern, const uint32_t *nbrStart,
-                                 uint32_t *nbrCountOrCell, uint64_t *candFull, float *feat, int pass, cudaStream_t s)
+                                 uint32_t *nbrCountOrCell, uint64_t *candFull, unsigned long long *candTotal,
+                                 float *feat, int pass, cudaStream_t s)
 {
     if (nCells == 0) return cudaSuccess;
     k_neighbours<<<(nCells + 127) / 128, 128, 0, s>>>(cellLid, cellCoord, cellStart, nCells, g, pattern, nbrStart,
-                                                      nbrCountOrCell, candFull, feat, pass); sj_note_launch();
+                                                      nbrCountOrCell, candFull, candTotal, feat, pass);
+    sj_note_launch();
     return cudaGetLastError();
 }

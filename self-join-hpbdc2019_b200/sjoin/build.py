@@ -22,7 +22,7 @@ CUDA = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 NVCC = os.path.join(CUDA, "bin", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
-CU_SOURCES = ["sj_prims.cu", "sj_index.cu", "sj_stencil.cu", "sj_join.cu", "sj_emit.cu", "sj_estimate.cu"]
+CU_SOURCES = ["sj_prims.cu", "sj_index.cu", "sj_stencil.cu", "sj_tasks.cu", "sj_join.cu", "sj_emit.cu", "sj_estimate.cu"]
 CPP_SOURCES = ["sj_api.cpp", "sj_csv.cpp"]
 
 

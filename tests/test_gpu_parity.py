@@ -126,6 +126,23 @@ def test_device_fold_pipeline_with_overflow_retries(mode, prec):
     assert st.total_pairs == len(ok) and st.pair_hash == oracle.hash_pairs(ok, ov)
 
 
+def test_mode8_splits_streams_by_thirds_of_the_work():
+    # mode 8 (the reference's dynamic threads per point): each query tile's
+    # candidate stream is shared by 16, 8 or 2 tasks by the third of the work
+    # its cell falls in; mode 9 chunks streams by predicted pairs instead
+    pts, eps, k, ix, (ok, ov) = _oracle_pairs("exp4d")
+    st = {}
+    for mode in (8, 9):
+        with sjoin.SelfJoin(4, eps, mode=mode) as sj:
+            sj.set_points(pts)
+            sj.build_index()
+            st[mode] = sj.join(sjoin.DELIVER_NONE)
+    h = oracle.hash_pairs(ok, ov)
+    for mode in (8, 9):
+        assert st[mode].total_pairs == len(ok) and st[mode].pair_hash == h
+    assert st[8].num_tasks > st[9].num_tasks
+
+
 def test_full_stencil_batches_hold_complete_rows():
     # with the full stencil every key is produced by one task's query tile, and
     # the count pass places all of a key's values together
