@@ -506,13 +506,14 @@ def _pipe_roofline(s, prec, D, clocks):
     """Distance loop (count pass) against the CUDA-core pipe it runs on.
 
     Operations per candidate evaluation on that pipe: FP64 predicate 2*D (D
-    subtractions, D-1 FMAs and one multiply); FP32 filter D + 2 (the norm add,
-    D FMAs, the band add; a packed f32x2 instruction counts as two).  Peak =
-    lanes x SM clock sampled during the timed steps (nominal lanes: 64 FP64 and
-    128 FP32 FMA per SM per clock)."""
+    subtractions, D-1 FMAs and one multiply); FP32 filter D + 1 (the norm add
+    and D FMAs; a packed f32x2 instruction counts as two; the borderline-band
+    test is an integer minimum on the ALU pipe).  Peak = lanes x SM clock
+    sampled during the timed steps (nominal lanes: 64 FP64 and 128 FP32 FMA
+    per SM per clock)."""
     mhz = clocks.get("sm_mhz") or 1965.0
     lanes = FP64_LANES if prec == 0 else FP32_LANES
-    ops = 2 * D if prec == 0 else D + 2
+    ops = 2 * D if prec == 0 else D + 1
     peak = NUM_SM * lanes * mhz * 1e6 / 1e12
     t = s["ms_count"] / 1e3
     ach = ops * s["distance_calcs"] / t / 1e12 if t > 0 else None

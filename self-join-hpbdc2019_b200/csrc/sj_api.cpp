@@ -438,7 +438,7 @@ sj_status build_neighbours(Ctx &c, int pattern)
     DevBuf<uint32_t> &cnt = c.sCnt;
     CK(cnt.ensure(nc + 1));
     DevBuf<unsigned long long> &sc = c.sScalars;
-    CK(sc.ensure(4));
+    CK(sc.ensure(2 + sj_sample_totals_len()));
     CK(cudaMemsetAsync(sc.p, 0, sizeof(unsigned long long), c.s));
     CK(sj_launch_neighbours(c.cellLid.p, c.cellCoord.p, c.cellStart.p, nc, c.g, pattern, nullptr, cnt.p,
                             c.candFull.p, sc.p, c.feat.p, 0, c.s));
@@ -758,9 +758,9 @@ sj_status estimate_rates(Ctx &c)
         CKS(run_count(c, a, true));
         CK(c.sHits.ensure(nc ? nc : 1));
         CK(c.sCands.ensure(nc ? nc : 1));
-        CK(c.sScalars.ensure(4));
-        CK(sj_sample_rates(c.dTasks.p, nt, c.taskHits.p, c.dTaskEvals.p, c.sHits.p, c.sCands.p, c.sScalars.p + 2, nc,
-                           c.rate.p, c.s));
+        CK(c.sScalars.ensure(2 + sj_sample_totals_len()));
+        CK(sj_sample_rates(c.dTasks.p, nt, c.taskHits.p, c.dTaskEvals.p, c.cellStart.p, c.sHits.p, c.sCands.p,
+                           c.sScalars.p + 2, nc, c.rate.p, c.s));
     }
     c.st.ms_estimate = tm.stop(c.s);
     return SJ_OK;

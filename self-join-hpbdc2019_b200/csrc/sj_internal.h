@@ -239,9 +239,13 @@ cudaError_t sj_plan_stats(const uint32_t *start, uint32_t nb, unsigned long long
                           unsigned long long *stats, cudaStream_t s);
 cudaError_t sj_rates_mlp(const float *out, const unsigned long long *candFull, uint32_t nCells, float *rate,
                          cudaStream_t s);
+// sampling estimator: per-cell rates from the sampled tasks' hits and
+// evaluations; totals has sj_sample_totals_len() entries (global and per
+// occupancy class, for the cells without a sample)
+size_t sj_sample_totals_len();
 cudaError_t sj_sample_rates(const sj_task *tasks, uint32_t nt, const uint32_t *taskHits, const uint32_t *taskEvals,
-                            unsigned long long *cellHits, unsigned long long *cellEvals, unsigned long long *totals,
-                            uint32_t nCells, float *rate, cudaStream_t s);
+                            const uint32_t *cellStart, unsigned long long *cellHits, unsigned long long *cellEvals,
+                            unsigned long long *totals, uint32_t nCells, float *rate, cudaStream_t s);
 // sums[0] evaluations, [1] refined, [2] measured pairs; *errSum = sum |pred - measured|
 cudaError_t sj_task_sums(const uint32_t *taskEvals, const uint32_t *taskRefined, const uint32_t *taskHits,
                          const float *pred, uint32_t nt, unsigned long long *sums, double *errSum, int numSM,

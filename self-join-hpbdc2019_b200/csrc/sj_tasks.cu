@@ -515,11 +515,21 @@ __global__ void __launch_bounds__(256) k_rates_mlp(const float *__restrict__ out
     rate[c] = (float)fmin(1.0, fmax(r, 0.0));
 }
 
-// Sampling estimator: hits and evaluations of the sampled queries, per cell
-// and in total.
+// Sampling estimator: hits and evaluations of the sampled queries, per cell,
+// per occupancy class of the cell (floor(log2(occupancy)), 32 classes) and in
+// total.  totals: [0] hits, [1] evaluations, [2 + 2b] / [3 + 2b] class b's.
+constexpr int SAMPLE_BINS = 32;
+
+__device__ __forceinline__ uint32_t occ_bin(const uint32_t *__restrict__ cellStart, uint32_t c)
+{
+    const uint32_t occ = cellStart[c + 1] - cellStart[c];
+    return occ ? 31u - __clz(occ) : 0u;
+}
+
 __global__ void __launch_bounds__(256) k_sample_sums(const sj_task *__restrict__ tasks, uint32_t nt,
                                                      const uint32_t *__restrict__ taskHits,
                                                      const uint32_t *__restrict__ taskEvals,
+                                                     const uint32_t *__restrict__ cellStart,
                                                      unsigned long long *__restrict__ cellHits,
                                                      unsigned long long *__restrict__ cellEvals,
                                                      unsigned long long *__restrict__ totals)
@@ -528,22 +538,37 @@ __global__ void __launch_bounds__(256) k_sample_sums(const sj_task *__restrict__
     if (t >= nt) return;
     const uint32_t c = tasks[t].cell;
     const uint32_t h = taskHits[t], e = taskEvals[t];
-    if (h) atomicAdd(&cellHits[c], (unsigned long long)h);
-    if (e) atomicAdd(&cellEvals[c], (unsigned long long)e);
-    if (h) atomicAdd(&totals[0], (unsigned long long)h);
-    if (e) atomicAdd(&totals[1], (unsigned long long)e);
+    const uint32_t b = occ_bin(cellStart, c);
+    if (h) {
+        atomicAdd(&cellHits[c], (unsigned long long)h);
+        atomicAdd(&totals[0], (unsigned long long)h);
+        atomicAdd(&totals[2 + 2 * b], (unsigned long long)h);
+    }
+    if (e) {
+        atomicAdd(&cellEvals[c], (unsigned long long)e);
+        atomicAdd(&totals[1], (unsigned long long)e);
+        atomicAdd(&totals[3 + 2 * b], (unsigned long long)e);
+    }
 }
 
-// Cells without a sampled query take the global rate.
+// A cell without a sampled query takes the rate of the sampled cells of its
+// occupancy class, or the global rate when that class has none.
 __global__ void __launch_bounds__(256) k_sample_rates(const unsigned long long *__restrict__ cellHits,
                                                       const unsigned long long *__restrict__ cellEvals,
-                                                      const unsigned long long *__restrict__ totals, uint32_t nCells,
+                                                      const unsigned long long *__restrict__ totals,
+                                                      const uint32_t *__restrict__ cellStart, uint32_t nCells,
                                                       float *__restrict__ rate)
 {
     const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= nCells) return;
+    if (cellEvals[c]) {
+        rate[c] = (float)((double)cellHits[c] / (double)cellEvals[c]);
+        return;
+    }
+    const uint32_t b = occ_bin(cellStart, c);
+    const unsigned long long bh = totals[2 + 2 * b], be = totals[3 + 2 * b];
     const double global = totals[1] ? (double)totals[0] / (double)totals[1] : 1.0;
-    rate[c] = cellEvals[c] ? (float)((double)cellHits[c] / (double)cellEvals[c]) : (float)global;
+    rate[c] = (float)(be ? (double)bh / (double)be : global);
 }
 
 // ------------------------------------------------------------ statistics --
@@ -798,20 +823,23 @@ cudaError_t sj_rates_mlp(const float *out, const unsigned long long *candFull, u
     return cudaGetLastError();
 }
 
+size_t sj_sample_totals_len() { return 2 + 2 * SAMPLE_BINS; }
+
 cudaError_t sj_sample_rates(const sj_task *tasks, uint32_t nt, const uint32_t *taskHits, const uint32_t *taskEvals,
-                            unsigned long long *cellHits, unsigned long long *cellEvals, unsigned long long *totals,
-                            uint32_t nCells, float *rate, cudaStream_t s)
+                            const uint32_t *cellStart, unsigned long long *cellHits, unsigned long long *cellEvals,
+                            unsigned long long *totals, uint32_t nCells, float *rate, cudaStream_t s)
 {
     cudaError_t e = cudaMemsetAsync(cellHits, 0, sizeof(unsigned long long) * nCells, s);
     if (e == cudaSuccess) e = cudaMemsetAsync(cellEvals, 0, sizeof(unsigned long long) * nCells, s);
-    if (e == cudaSuccess) e = cudaMemsetAsync(totals, 0, sizeof(unsigned long long) * 2, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(totals, 0, sizeof(unsigned long long) * sj_sample_totals_len(), s);
     if (e != cudaSuccess) return e;
     if (nt) {
-        k_sample_sums<<<blocks_for(nt, 256), 256, 0, s>>>(tasks, nt, taskHits, taskEvals, cellHits, cellEvals, totals);
+        k_sample_sums<<<blocks_for(nt, 256), 256, 0, s>>>(tasks, nt, taskHits, taskEvals, cellStart, cellHits,
+                                                          cellEvals, totals);
         sj_note_launch();
     }
     if (nCells) {
-        k_sample_rates<<<blocks_for(nCells, 256), 256, 0, s>>>(cellHits, cellEvals, totals, nCells, rate);
+        k_sample_rates<<<blocks_for(nCells, 256), 256, 0, s>>>(cellHits, cellEvals, totals, cellStart, nCells, rate);
         sj_note_launch();
     }
     return cudaGetLastError();

@@ -1,16 +1,24 @@
 """Trains the learned batch estimator on counts the engine itself measures.
 
 Data: seeded runs of the 6-D exponential(40) generator (the c4 workload's
-distribution) with eps drawn uniformly from [0.01, 0.05].  For each run the
+distribution) with eps drawn uniformly from [0.01, 0.05] and the point count
+drawn log-uniformly up to 1e7, the c4 workload's size.  For each run the
 engine builds its index, computes every cell's 16 features and full-stencil
 distance-calculation count, and measures every point's neighbour count with
 its count pass (sj_degrees); a cell's target is (log2(1+calcs), log2(1+hits)).
 The point count of a run is shrunk until the run's full-stencil work stays
-under a budget, so the collection takes minutes, not hours.
+under a budget (by default a little above the c4 workload's 4.06e13), so the
+heaviest runs reach the cell sizes of that workload.
 
 Training: the 16 -> 64 -> 64 -> 2 MLP is trained with the engine's own FP32
-forward / backward / Adam kernels (sj_mlp_train).  Weights are written as raw
-float32 in the engine's layout (sj_mlp_num_params() values).
+forward / backward / Adam kernels (sj_mlp_train).  The batch planner sums the
+predictions over many cells, so what matters is the error on the cells that
+hold the pairs: the training set is drawn from the collected cells with
+probability proportional to (1 + hits)^beta (beta = 0.5 by default), which
+keeps every cell size represented while the heavy cells that dominate a
+batch's total are seen far more often than their number alone would give.
+Weights are written as raw float32 in the engine's layout (sj_mlp_num_params()
+values).
 
 usage: python -m sjoin.train_estimator [--runs 50] [--out sjoin/estimator_c4.bin]
 """
@@ -46,8 +54,8 @@ def targets(calcs: np.ndarray, hits: np.ndarray) -> np.ndarray:
     return np.stack([np.log2(1.0 + calcs), np.log2(1.0 + hits)], 1).astype(np.float32)
 
 
-def collect(runs: int = 50, seed0: int = 7000, n_max: int = 1_000_000, n_min: int = 50_000,
-            work_budget: float = 4e11, D: int = 6, log=print):
+def collect(runs: int = 50, seed0: int = 7000, n_max: int = 10_000_000, n_min: int = 50_000,
+            work_budget: float = 4.5e13, D: int = 6, log=print):
     rng = np.random.default_rng(seed0)
     xs, ys, meta = [], [], []
     for r in range(runs):
@@ -71,6 +79,15 @@ def collect(runs: int = 50, seed0: int = 7000, n_max: int = 1_000_000, n_min: in
     return np.concatenate(xs), np.concatenate(ys), meta
 
 
+def resample(x: np.ndarray, y: np.ndarray, size: int = 4_000_000, beta: float = 0.5, seed: int = 1):
+    """Training set drawn with probability proportional to (1 + hits)^beta."""
+    hits = np.exp2(y[:, 1].astype(np.float64)) - 1.0
+    p = np.power(1.0 + hits, beta)
+    p /= p.sum()
+    idx = np.random.default_rng(seed).choice(len(x), size=min(size, 4 * len(x)), replace=True, p=p)
+    return x[idx], y[idx]
+
+
 def train(x: np.ndarray, y: np.ndarray, steps: int = 6000, lr: float = 2e-3, batch: int = 4096, seed: int = 1):
     w0 = mlp_init(seed)
     # step-wise learning-rate decay: three stages
@@ -83,16 +100,23 @@ def train(x: np.ndarray, y: np.ndarray, steps: int = 6000, lr: float = 2e-3, bat
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--runs", type=int, default=50)
-    ap.add_argument("--steps", type=int, default=6000)
+    ap.add_argument("--steps", type=int, default=12000)
+    ap.add_argument("--beta", type=float, default=0.5, help="resampling exponent (0: every cell alike)")
+    ap.add_argument("--data-in", default=None, help="train on a saved .npz instead of collecting")
     ap.add_argument("--out", default=DEFAULT_OUT)
     ap.add_argument("--data-out", default=None, help="optional .npz of the collected training set")
     args = ap.parse_args()
     t0 = time.time()
-    x, y, meta = collect(args.runs)
-    print(f"collected {len(x)} cells from {len(meta)} runs in {time.time() - t0:.1f} s", flush=True)
+    if args.data_in:
+        d = np.load(args.data_in)
+        x, y = d["x"], d["y"]
+    else:
+        x, y, meta = collect(args.runs)
+        print(f"collected {len(x)} cells from {len(meta)} runs in {time.time() - t0:.1f} s", flush=True)
     if args.data_out:
         np.savez_compressed(args.data_out, x=x, y=y)
-    w, loss = train(x, y, steps=args.steps)
+    xt, yt = resample(x, y, beta=args.beta) if args.beta > 0 else (x, y)
+    w, loss = train(xt, yt, steps=args.steps)
     full, _ = mlp_loss_grad(x, y, w)
     w.astype(np.float32).tofile(args.out)
     print(json.dumps({"cells": int(len(x)), "final_loss": full, "out": args.out,

@@ -114,11 +114,13 @@ def test_multi_batch_with_overflow_retries(mode, prec):
 @pytest.mark.parametrize("mode", [5, 10])
 def test_device_fold_pipeline_with_overflow_retries(mode, prec):
     # on-device delivery runs every batch back to back on two streams and
-    # re-plans the batches whose count exceeds the buffer: alpha 0 and a tiny
-    # sample make underestimates certain at this capacity
+    # re-plans the batches whose count exceeds the buffer: an untrained
+    # estimator network under-predicts by orders of magnitude, so batches
+    # overflow for certain at this capacity
     pts, eps, k, ix, (ok, ov) = _oracle_pairs("exp2d_dense")
     with sjoin.SelfJoin(2, eps, mode=mode, precision=prec, capacity=65536, alpha=0.0,
-                        sample_rate=0.002) as sj:
+                        scheduler=sjoin.SCHED_LEARNED) as sj:
+        sj.set_estimator(sjoin.mlp_init(3))
         sj.set_points(pts)
         sj.build_index()
         st = sj.join(sjoin.DELIVER_NONE)
