@@ -50,12 +50,15 @@ typedef struct {
     int gpunumdim;            /* GPUNUMDIM: data dimensions (1..16) */
     int numindexeddim;        /* NUMINDEXEDDIM: grid dimensions, the first k dims (1..min(D,16)) */
     double epsilon;           /* search radius (main.cu:62) */
-    int blocksize;            /* BLOCKSIZE: accepted for compatibility; the engine uses 128-thread CTAs */
-    int threadperpoint;       /* THREADPERPOINT: accepted for compatibility (1) */
+    int blocksize;            /* BLOCKSIZE: accepted and not used; the engine's CTA shapes are fixed per
+                                 kernel (128-thread count pass, 256-thread emission) */
+    int threadperpoint;       /* THREADPERPOINT: accepted and not used; the work per query tile is split
+                                 across tasks by the scheduler instead (see search_mode 8) */
     int search_mode;          /* 3 full stencil, 4 Unicomp, 5 B-Unicomp (k=2,3), 6 linear-ID Unicomp,
-                                 7 full stencil in workload order, 8 full stencil with work split by
-                                 workload (the reference's dynamic threads per point), 9 work queue,
-                                 10 work queue + LID-Unicomp */
+                                 7 full stencil in workload order, 8 full stencil with every query tile's
+                                 stream split over 16 / 8 / 2 tasks by the third of the work (in cost
+                                 order) its cell falls in (the reference's dynamic threads per point,
+                                 NB_THREAD_THIRD1..3), 9 work queue, 10 work queue + LID-Unicomp */
     int sort_by_workload;     /* SORT_BY_WORKLOAD: order work by estimated cost, heaviest first */
     int precision;            /* sj_precision */
     int scheduler;            /* sj_scheduler: estimator used to size result batches */
@@ -111,19 +114,23 @@ typedef struct {
     float ms_expand;            /* key-array expansion from the batch's key runs */
 } sj_stats;
 
+/* Opaque engine context: one per device, created by sj_create, released by
+ * sj_destroy.  Not thread-safe; calls on one context must not overlap. */
+typedef struct sj_ctx sj_ctx;
+
 /* Fill `p` with params.h defaults: D=k=2, BLOCKSIZE 256, THREADPERPOINT 1,
  * SORT_BY_WORKLOAD 1, mode 10, FP64, sampling estimator, rate 0.01, alpha 0.05. */
 void sj_params_default(sj_params *p);
 
 /* Replaces the setup half of distanceTableNDGridBatches (GPU.cu:1315-1585) and
  * warmUpGPU (GPU.cu:2572): validates parameters, binds the device. */
-sj_status sj_create(const sj_params *p, void **ctx_out);
-sj_status sj_destroy(void *ctx);
+sj_status sj_create(const sj_params *p, sj_ctx **ctx_out);
+sj_status sj_destroy(sj_ctx *ctx);
 
 /* Replaces importNDDataset + sortInNDBins (import_dataset.cpp:34-80): parses
  * comma/whitespace separated doubles, groups them by gpunumdim, applies the
  * same integer-bin sort (so point ids equal the reference's), uploads. */
-sj_status sj_import_csv(void *ctx, const char *path);
+sj_status sj_import_csv(sj_ctx *ctx, const char *path);
 
 /* The same parse and point order without a device (host memory only): writes
  * up to `cap` points (cap x gpunumdim doubles) to `out` and the number of
@@ -133,17 +140,17 @@ sj_status sj_read_csv(const char *path, int gpunumdim, double *out, uint64_t cap
 /* Supplies points directly: n x gpunumdim doubles, row-major (the flattened
  * NDdataPoints of GPU.cu:1333-1346).  `on_device` = 1 if `pts` is a device
  * pointer; otherwise it is copied host-to-device. */
-sj_status sj_set_points(void *ctx, const double *pts, uint64_t n, int on_device);
+sj_status sj_set_points(sj_ctx *ctx, const double *pts, uint64_t n, int on_device);
 
 /* Replaces generateNDGridDimensions + populateNDGridIndexAndLookupArray
  * (main.cu:240-503), built on the device. */
-sj_status sj_build_index(void *ctx);
+sj_status sj_build_index(sj_ctx *ctx);
 
 /* Reference-layout export of the index for parity checks: sizes first, then
  * arrays (indexLookupArr[n], grid[nNonEmpty], gridCellLookup[nNonEmpty],
  * minArr[k], nCells[k], gridCellNDMask[nMask], gridCellNDMaskOffsets[2k]). */
-sj_status sj_index_sizes(void *ctx, uint32_t *n_nonempty, uint32_t *n_mask_elems, uint64_t *total_cells);
-sj_status sj_index_export(void *ctx, unsigned int *indexLookupArr, sj_grid *grid,
+sj_status sj_index_sizes(sj_ctx *ctx, uint32_t *n_nonempty, uint32_t *n_mask_elems, uint64_t *total_cells);
+sj_status sj_index_export(sj_ctx *ctx, unsigned int *indexLookupArr, sj_grid *grid,
                           sj_grid_cell_lookup *gridCellLookupArr, double *minArr, unsigned int *nCells,
                           unsigned int *gridCellNDMask, unsigned int *gridCellNDMaskOffsets);
 
@@ -151,18 +158,18 @@ sj_status sj_index_export(void *ctx, unsigned int *indexLookupArr, sj_grid *grid
  * estimates, plans batches, and streams every result batch to `cb`.
  * SJ_DELIVER_NONE runs the join and only folds each batch into the pair count
  * and set hash (sj_stats). */
-sj_status sj_join(void *ctx, int delivery, sj_batch_cb cb, void *user);
+sj_status sj_join(sj_ctx *ctx, int delivery, sj_batch_cb cb, void *user);
 
 /* Neighbour count of every point (row lengths of the neighbour table) without
  * materialising pairs.  deg: n uint32 on the host. */
-sj_status sj_degrees(void *ctx, uint32_t *deg);
+sj_status sj_degrees(sj_ctx *ctx, uint32_t *deg);
 
 /* Replaces constructNeighborTableKeyValueWithPtrs (GPU.cu:2595-2637) and the
  * table of main.cu:185: runs the join and fills table[n] with each point's
  * complete neighbour range inside one values array (allocated with malloc,
  * owned by the caller; free it with sj_free).  Keys that span batches are
  * merged, which the reference's table does not do. */
-sj_status sj_neighbor_table(void *ctx, sj_neighbor_table_lookup *table, int **values, uint64_t *total);
+sj_status sj_neighbor_table(sj_ctx *ctx, sj_neighbor_table_lookup *table, int **values, uint64_t *total);
 void sj_free(void *p);
 
 /* On-device CSR neighbour table (replaces the host table of
@@ -174,26 +181,26 @@ void sj_free(void *p);
  * cols.  Fails with SJ_ERR_BAD_INPUT when cols_capacity < total.  Values inside
  * a row are in no particular order (the reference's rows are not sorted
  * either). */
-sj_status sj_neighbor_csr(void *ctx, uint64_t *rowPtr, int32_t *cols, uint64_t cols_capacity, uint64_t *total);
+sj_status sj_neighbor_csr(sj_ctx *ctx, uint64_t *rowPtr, int32_t *cols, uint64_t cols_capacity, uint64_t *total);
 
-sj_status sj_get_stats(void *ctx, sj_stats *st);
+sj_status sj_get_stats(sj_ctx *ctx, sj_stats *st);
 
 /* The CUDA stream (cudaStream_t) this context's work is ordered on, so a
  * caller can record events around sj_build_index / sj_join.  Work the join runs
  * on its internal second stream is joined back into this one before sj_join
  * returns. */
-sj_status sj_get_stream(void *ctx, void **stream);
+sj_status sj_get_stream(sj_ctx *ctx, void **stream);
 
 /* Learned estimator.  Weights: SJ_MLP_NPARAM floats laid out W1[16x64], b1[64],
  * W2[64x64], b2[64], W3[64x2], b3[2] (row-major, input-major). */
 uint32_t sj_mlp_num_params(void);
-sj_status sj_set_estimator_weights(void *ctx, const float *w, uint32_t count);
-sj_status sj_load_estimator(void *ctx, const char *path);
+sj_status sj_set_estimator_weights(sj_ctx *ctx, const float *w, uint32_t count);
+sj_status sj_load_estimator(sj_ctx *ctx, const char *path);
 
 /* Per-cell learned-estimator features and, after sj_degrees or sj_join, the
  * measured per-cell hits and distance calculations (full-stencil semantics).
  * feat: nNonEmpty x 16 floats; hits/calcs: nNonEmpty doubles; NULL skips. */
-sj_status sj_cell_features(void *ctx, float *feat, double *hits, double *calcs);
+sj_status sj_cell_features(sj_ctx *ctx, float *feat, double *hits, double *calcs);
 
 /* Device training of the estimator MLP by the project's own kernels.
  * x: m x 16, y: m x 2 (host float arrays); w: in/out parameters. */

@@ -1,7 +1,8 @@
 """Builds the reference's own sources into oracle/_ref/ (test / baseline infrastructure).
 
-The reference's sources are compiled where they lie (REFERENCE, default
-/root/reference); nothing is copied.  Its dimensions are compile-time macros
+The reference's sources are compiled where they lie: the directory named by
+the SJ_REFERENCE environment variable, else a checkout named `reference` next
+to this repository; nothing is copied.  Its dimensions are compile-time macros
 in params.h, which every file includes with #include "params.h", so each
 configuration gets a directory of symbolic links to the reference files plus a
 generated params.h: the compiler resolves quoted includes relative to the
@@ -33,7 +34,7 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT = os.path.join(HERE, "_ref")
-REFERENCE = os.environ.get("SJ_REFERENCE", "/root/reference")
+REFERENCE = os.environ.get("SJ_REFERENCE") or os.path.join(os.path.dirname(os.path.dirname(HERE)), "reference")
 NVCC = os.path.join(os.environ.get("CUDA_HOME", "/usr/local/cuda"), "bin", "nvcc")
 REF_FILES = ["GPU.cu", "GPU.h", "import_dataset.cpp", "kernel.cu", "kernel.h", "kernelloops.h", "main.cu",
              "stamploops.h", "stamploopsV2.h", "stamploopsSortingCells.h", "structs.h"]

@@ -537,8 +537,8 @@ constexpr uint64_t SJ_MASK_BATCH_WORDS = 1ULL << 29;
 // The task list, built on the device (sj_tasks.cu): per-cell workload and cost
 // key, the cost order (stable radix sort, heaviest first, ties in cell order),
 // one work item per (cell, segment group, query tile) and its tasks.  policy:
-// 0 cost-proportional stream chunks (needs c.rate), 1 fixed chunks, 2 the
-// mode-8 split by thirds of the work.  sampleRate > 0 builds the sampling
+// 0 cost-proportional stream chunks, 1 fixed chunks, 2 the mode-8 split by
+// thirds of the work (0 and 2 predict pairs from c.rate).  sampleRate > 0 builds the sampling
 // estimator's tasks.  With `shard`, keeps this context's shard of the list.
 // Sets c.nTasks; the tasks are in c.dTasks, their predicted pairs in c.dTaskPred.
 sj_status build_tasks_dev(Ctx &c, bool sym, uint64_t cap, bool byCost, int policy, float sampleRate, bool shard)
@@ -549,7 +549,7 @@ sj_status build_tasks_dev(Ctx &c, bool sym, uint64_t cap, bool byCost, int polic
     g.cellStart = c.cellStart.p;
     g.nbrStart = c.nbrStart.p;
     g.nbrCell = c.nbrCell.p;
-    g.rate = policy == 0 ? c.rate.p : nullptr;
+    g.rate = policy == 1 ? nullptr : c.rate.p;   // the split of policy 2 ignores it, its predictions do not
     g.nCells = nc;
     g.tile = SJ_CTA * (uint32_t)sj_query_slots(c.g.Dp, c.p.precision == SJ_PREC_FP32_REFINE);
     g.cap = cap;
@@ -999,7 +999,10 @@ sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
         // between two sets of count-pass records and two sets of key offsets
         // and scan totals; batch i's count pass waits for batch i - 2's
         // emission, the last reader of the set it reuses.
-        bool pipe = nplan > 1;
+        // SJ_SERIAL=1 keeps every stage on the engine's stream (a diagnostic
+        // knob: the per-stage CUDA-event times are then those of each stage alone)
+        const char *serialEnv = getenv("SJ_SERIAL");
+        bool pipe = nplan > 1 && !(serialEnv && atoi(serialEnv) != 0);
         if (pipe) {
             cudaError_t e = c.masks2.ensure(maxMaskWords);
             if (e == cudaSuccess) e = c.colMasks2.ensure(maxColWords);
@@ -1063,14 +1066,22 @@ sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
                                            sA));
             CK(cudaEventRecord(e[3], sA));
             if (pipe) CK(cudaStreamWaitEvent(sB, e[3], 0));
+            // emission (values), then the consumer fold, which reads the values
+            // back and writes the key array in the same pass
             CK(cudaEventRecord(e[4], sB));
-            CKS(expand_keys(c, b, sB, scanTot));
             CK(cudaEventRecord(e[5], sB));
             b.queueHead = pipe ? c.emitHead.p : c.queueHead.p;
             CK(cudaMemsetAsync(b.queueHead, 0, sizeof(uint32_t), sB));
             CK(sj_launch_emit(b, c.numSM, sB));
             CK(cudaEventRecord(e[6], sB));
-            CK(sj_hash_pairs_dev(c.outKey.p, c.outVal.p, b.batchPairs, bufCap, bufCap, c.numSM, c.stat.p + 4, sB));
+            {
+                const size_t slots = sj_expand_long_slots(b.capacity);
+                CK(c.longRuns.ensure(slots));
+                CK(c.longCount.ensure(1));
+                CK(sj_fold_expand(b.keyStart, scanTot, n, c.outVal.p, c.outKey.p, b.batchPairs, bufCap, c.longRuns.p,
+                                  (uint32_t)std::min<size_t>(c.longRuns.n, 0xffffffffu), c.longCount.p, c.stat.p + 4,
+                                  c.numSM, sB));
+            }
             CK(cudaEventRecord(e[7], sB));
         }
         if (pipe) CK(cudaStreamWaitEvent(sA, ev[EV * (nplan - 1) + 7], 0));
@@ -1102,7 +1113,9 @@ sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
             if (tot[i] > bufCap) {
                 // the count pass measured every task's pairs: re-plan this
                 // batch's tasks exactly, so the re-runs cannot overflow again
-                CKS(replan_exact(br, hTaskHits, bufCap, redo));
+                // (against the capacity: the synchronous phase grows the
+                // buffers up to it, and no task's worst case exceeds it)
+                CKS(replan_exact(br, hTaskHits, cap, redo));
                 retries++;
                 continue;
             }
@@ -1398,7 +1411,7 @@ sj_status set_points(Ctx &c, const double *pts, uint64_t n, int onDevice)
     return SJ_OK;
 }
 
-Ctx *as_ctx(void *p) { return reinterpret_cast<Ctx *>(p); }
+Ctx *as_ctx(sj_ctx *p) { return reinterpret_cast<Ctx *>(p); }
 
 sj_status bind(Ctx &c)
 {
@@ -1434,7 +1447,7 @@ void sj_params_default(sj_params *p)
     p->verbose = 0;
 }
 
-sj_status sj_create(const sj_params *p, void **out)
+sj_status sj_create(const sj_params *p, sj_ctx **out)
 {
     if (!p || !out) {
         set_error("null argument");
@@ -1470,11 +1483,11 @@ sj_status sj_create(const sj_params *p, void **out)
         delete c;
         return SJ_ERR_CUDA;
     }
-    *out = c;
+    *out = reinterpret_cast<sj_ctx *>(c);
     return SJ_OK;
 }
 
-sj_status sj_destroy(void *ctx)
+sj_status sj_destroy(sj_ctx *ctx)
 {
     if (!ctx) return SJ_OK;
     Ctx *c = as_ctx(ctx);
@@ -1495,7 +1508,7 @@ sj_status sj_destroy(void *ctx)
     return SJ_OK;
 }
 
-sj_status sj_import_csv(void *ctx, const char *path)
+sj_status sj_import_csv(sj_ctx *ctx, const char *path)
 {
     if (!ctx || !path) {
         set_error("null argument");
@@ -1532,7 +1545,7 @@ sj_status sj_read_csv(const char *path, int gpunumdim, double *out, uint64_t cap
     return SJ_OK;
 }
 
-sj_status sj_set_points(void *ctx, const double *pts, uint64_t n, int on_device)
+sj_status sj_set_points(sj_ctx *ctx, const double *pts, uint64_t n, int on_device)
 {
     if (!ctx) {
         set_error("null context");
@@ -1543,7 +1556,7 @@ sj_status sj_set_points(void *ctx, const double *pts, uint64_t n, int on_device)
     return set_points(c, pts, n, on_device);
 }
 
-sj_status sj_build_index(void *ctx)
+sj_status sj_build_index(sj_ctx *ctx)
 {
     if (!ctx) return SJ_ERR_BAD_INPUT;
     Ctx &c = *as_ctx(ctx);
@@ -1551,7 +1564,7 @@ sj_status sj_build_index(void *ctx)
     return build_index(c);
 }
 
-sj_status sj_index_sizes(void *ctx, uint32_t *n_nonempty, uint32_t *n_mask_elems, uint64_t *total_cells)
+sj_status sj_index_sizes(sj_ctx *ctx, uint32_t *n_nonempty, uint32_t *n_mask_elems, uint64_t *total_cells)
 {
     if (!ctx) return SJ_ERR_BAD_INPUT;
     Ctx &c = *as_ctx(ctx);
@@ -1577,7 +1590,7 @@ sj_status sj_index_sizes(void *ctx, uint32_t *n_nonempty, uint32_t *n_mask_elems
     return SJ_OK;
 }
 
-sj_status sj_index_export(void *ctx, unsigned int *indexLookupArr, sj_grid *grid, sj_grid_cell_lookup *lookup,
+sj_status sj_index_export(sj_ctx *ctx, unsigned int *indexLookupArr, sj_grid *grid, sj_grid_cell_lookup *lookup,
                           double *minArr, unsigned int *nCells, unsigned int *mask, unsigned int *maskOffsets)
 {
     if (!ctx) return SJ_ERR_BAD_INPUT;
@@ -1629,7 +1642,7 @@ sj_status sj_index_export(void *ctx, unsigned int *indexLookupArr, sj_grid *grid
     return SJ_OK;
 }
 
-sj_status sj_join(void *ctx, int delivery, sj_batch_cb cb, void *user)
+sj_status sj_join(sj_ctx *ctx, int delivery, sj_batch_cb cb, void *user)
 {
     if (!ctx) return SJ_ERR_BAD_INPUT;
     if (delivery < SJ_DELIVER_DEVICE || delivery > SJ_DELIVER_NONE) {
@@ -1641,7 +1654,7 @@ sj_status sj_join(void *ctx, int delivery, sj_batch_cb cb, void *user)
     return run_join(c, delivery, cb, user);
 }
 
-sj_status sj_degrees(void *ctx, uint32_t *deg)
+sj_status sj_degrees(sj_ctx *ctx, uint32_t *deg)
 {
     if (!ctx) return SJ_ERR_BAD_INPUT;
     Ctx &c = *as_ctx(ctx);
@@ -1665,7 +1678,7 @@ static int table_cb(const sj_batch *b, void *user)
     return 0;
 }
 
-sj_status sj_neighbor_table(void *ctx, sj_neighbor_table_lookup *table, int **values, uint64_t *total)
+sj_status sj_neighbor_table(sj_ctx *ctx, sj_neighbor_table_lookup *table, int **values, uint64_t *total)
 {
     if (!ctx || !table || !values) return SJ_ERR_BAD_INPUT;
     Ctx &c = *as_ctx(ctx);
@@ -1707,7 +1720,7 @@ sj_status sj_neighbor_table(void *ctx, sj_neighbor_table_lookup *table, int **va
     return SJ_OK;
 }
 
-sj_status sj_neighbor_csr(void *ctx, uint64_t *rowPtr, int32_t *cols, uint64_t cols_capacity, uint64_t *total)
+sj_status sj_neighbor_csr(sj_ctx *ctx, uint64_t *rowPtr, int32_t *cols, uint64_t cols_capacity, uint64_t *total)
 {
     if (!ctx || !rowPtr) {
         set_error("null argument");
@@ -1766,14 +1779,14 @@ sj_status sj_neighbor_csr(void *ctx, uint64_t *rowPtr, int32_t *cols, uint64_t c
 
 void sj_free(void *p) { free(p); }
 
-sj_status sj_get_stream(void *ctx, void **stream)
+sj_status sj_get_stream(sj_ctx *ctx, void **stream)
 {
     if (!ctx || !stream) return SJ_ERR_BAD_INPUT;
     *stream = (void *)as_ctx(ctx)->s;
     return SJ_OK;
 }
 
-sj_status sj_get_stats(void *ctx, sj_stats *st)
+sj_status sj_get_stats(sj_ctx *ctx, sj_stats *st)
 {
     if (!ctx || !st) return SJ_ERR_BAD_INPUT;
     *st = as_ctx(ctx)->st;
@@ -1782,7 +1795,7 @@ sj_status sj_get_stats(void *ctx, sj_stats *st)
 
 uint32_t sj_mlp_num_params(void) { return SJ_MLP_NPARAM; }
 
-sj_status sj_set_estimator_weights(void *ctx, const float *w, uint32_t count)
+sj_status sj_set_estimator_weights(sj_ctx *ctx, const float *w, uint32_t count)
 {
     if (!ctx || !w || count != SJ_MLP_NPARAM) {
         set_error("estimator weights: expected %d floats", SJ_MLP_NPARAM);
@@ -1793,7 +1806,7 @@ sj_status sj_set_estimator_weights(void *ctx, const float *w, uint32_t count)
     return SJ_OK;
 }
 
-sj_status sj_load_estimator(void *ctx, const char *path)
+sj_status sj_load_estimator(sj_ctx *ctx, const char *path)
 {
     if (!ctx || !path) return SJ_ERR_BAD_INPUT;
     FILE *f = fopen(path, "rb");
@@ -1811,7 +1824,7 @@ sj_status sj_load_estimator(void *ctx, const char *path)
     return sj_set_estimator_weights(ctx, w.data(), (uint32_t)w.size());
 }
 
-sj_status sj_cell_features(void *ctx, float *feat, double *hits, double *calcs)
+sj_status sj_cell_features(sj_ctx *ctx, float *feat, double *hits, double *calcs)
 {
     if (!ctx) return SJ_ERR_BAD_INPUT;
     Ctx &c = *as_ctx(ctx);

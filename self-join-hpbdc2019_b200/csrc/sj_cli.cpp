@@ -75,7 +75,7 @@ int main(int argc, char **argv)
     printf("\nDataset file: %s", fname);
     printf("\nEpsilon: %f", eps);
     printf("\nNumber of dimensions (NDIM): %d\n", ndim);
-    void *ctx = nullptr;
+    sj_ctx *ctx = nullptr;
     sj_status s = sj_create(&p, &ctx);
     if (s != SJ_OK) return fail(s);
     s = sj_import_csv(ctx, fname);

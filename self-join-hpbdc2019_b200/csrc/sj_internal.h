@@ -154,9 +154,6 @@ cudaError_t sj_radix_sort_u32_u32(uint32_t *keys, uint32_t *vals, uint32_t *keys
                                   uint64_t n, int bits, void *temp, int *resultInAlt, cudaStream_t s);
 cudaError_t sj_hash_pairs(const int32_t *key, const int32_t *val, uint64_t m,
                           unsigned long long *hashOut, cudaStream_t s);
-// same, with the pair count read on the device (skipped when it exceeds cap)
-cudaError_t sj_hash_pairs_dev(const int32_t *key, const int32_t *val, const unsigned long long *count, uint64_t cap,
-                              uint64_t gridHint, int numSM, unsigned long long *hashOut, cudaStream_t s);
 
 // keys of a batch from its row structure: key k owns [excl[k], excl[k+1])
 // (excl[n] = *total); skipped when the batch's count exceeds cap.  longRuns
@@ -166,6 +163,14 @@ cudaError_t sj_expand_keys(const uint32_t *excl, const uint32_t *total, uint64_t
                            const unsigned long long *batchPairs, uint64_t cap, void *longRuns, uint32_t longCap,
                            uint32_t *longCount, int numSM, cudaStream_t s);
 size_t sj_expand_long_slots(uint64_t cap);
+// consumer fold of a device-resident batch with the key array written in the
+// same pass: reads the values, writes the keys from the key runs (as
+// sj_expand_keys), adds the pairs' set hash to *hashOut; skipped when the
+// batch's count exceeds cap.  longRuns / longCount as for sj_expand_keys.
+cudaError_t sj_fold_expand(const uint32_t *excl, const uint32_t *total, uint64_t n, const int32_t *val,
+                           int32_t *outKey, const unsigned long long *batchPairs, uint64_t cap, void *longRuns,
+                           uint32_t longCap, uint32_t *longCount, unsigned long long *hashOut, int numSM,
+                           cudaStream_t s);
 // appends a batch (values vals, key runs start[0..n], start[n] = *total) to a
 // device CSR table rowPtr[n+1] / cols[colsCap]; fill[n] are the rows' cursors
 cudaError_t sj_csr_append(const uint32_t *start, const uint32_t *total, uint64_t n, const int32_t *vals,

@@ -459,6 +459,7 @@ __global__ void __launch_bounds__(SJ_CTA, F32 ? SJ_JOIN_MIN_BLOCKS_F32 : SJ_JOIN
                 uint32_t *const rowRec = maskBase ? maskBase + sj_row_mask_index(bInTask, 0, task.qCount, nBlk) : nullptr;
                 const uint32_t rowStride = min(64u, nBlk - (bInTask & ~63u));
                 uint32_t *const colRec = colBase ? colBase + ((uint64_t)bInTask * nG + warp) * 32 + lane : nullptr;
+                uint32_t colHits = 0;   // this lane's candidate: hits over the warp's slots
 #pragma unroll
                 for (int r = 0; r < R; r++) {
                     if ((uint32_t)r >= nAct) continue;   // warp-uniform
@@ -484,16 +485,19 @@ __global__ void __launch_bounds__(SJ_CTA, F32 ? SJ_JOIN_MIN_BLOCKS_F32 : SJ_JOIN
                             }
                         }
                     }
-                    evals += __popc(rowValid);
                     const uint32_t rowMask = h & rowValid;   // lane = query, bit = candidate
                     if (rowRec && qValid) rowRec[(uint64_t)qi * rowStride] = rowMask;
                     rowCount[r] += __popc(rowMask);
                     if (sym) {
-                        const uint32_t colW = transpose32(hb ? (rowMask & mir_keep(qi, blk, hb)) : rowMask, lane);
-                        colCnt[warp][jb + lane] += __popc(colW);
+                        // the mirrored direction: lane L gets candidate L's hits (none
+                        // to transpose when the warp's block has no hit at all)
+                        const uint32_t mir = hb ? (rowMask & mir_keep(qi, blk, hb)) : rowMask;
+                        const uint32_t colW = __any_sync(0xffffffffu, mir) ? transpose32(mir, lane) : 0u;
+                        colHits += __popc(colW);
                         if (colRec) colRec[(uint32_t)r * NW * 32] = colW;
                     }
                 }
+                if (sym && colHits) colCnt[warp][jb + lane] += colHits;
             }
             if (sym) {
                 __syncthreads();
@@ -517,6 +521,12 @@ __global__ void __launch_bounds__(SJ_CTA, F32 ? SJ_JOIN_MIN_BLOCKS_F32 : SJ_JOIN
 #pragma unroll
             for (int r = 0; r < R; r++) {
                 const uint32_t qi = (uint32_t)r * SJ_CTA + tid;
+                // evaluations of this query: stream positions [sBegin, sEnd), in the
+                // symmetric home segment only those at or after the query itself
+                if (qi < task.qCount) {
+                    const uint32_t from = max(task.sBegin, min(qi, sym ? homeEnd : 0u));
+                    evals += sEnd > from ? sEnd - from : 0u;
+                }
                 // the key's count before this addition: where this task's row
                 // run starts inside the query's key run
                 const uint32_t rel = rowCount[r] ? atomicAdd(&a.keyCount[qid[r]], rowCount[r]) : 0u;

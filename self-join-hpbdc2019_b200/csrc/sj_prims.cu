@@ -297,39 +297,6 @@ __global__ void __launch_bounds__(256) k_hash_pairs(const int32_t *__restrict__ 
     }
 }
 
-__global__ void __launch_bounds__(256) k_hash_pairs_dev(const int32_t *__restrict__ key,
-                                                        const int32_t *__restrict__ val,
-                                                        const unsigned long long *__restrict__ count, uint64_t cap,
-                                                        unsigned long long *out)
-{
-    const unsigned long long m = *count;
-    if (m > cap) return;
-    unsigned long long h = 0;
-    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    const uint64_t m4 = m / 4;
-    const int4 *k4 = reinterpret_cast<const int4 *>(key);
-    const int4 *v4 = reinterpret_cast<const int4 *>(val);
-    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m4; i += stride) {
-        const int4 a = __ldcs(k4 + i), b = __ldcs(v4 + i);
-        h += splitmix64(((unsigned long long)(uint32_t)a.x << 32) | (uint32_t)b.x);
-        h += splitmix64(((unsigned long long)(uint32_t)a.y << 32) | (uint32_t)b.y);
-        h += splitmix64(((unsigned long long)(uint32_t)a.z << 32) | (uint32_t)b.z);
-        h += splitmix64(((unsigned long long)(uint32_t)a.w << 32) | (uint32_t)b.w);
-    }
-    for (uint64_t i = 4 * m4 + (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += stride)
-        h += splitmix64(((unsigned long long)(uint32_t)key[i] << 32) | (uint32_t)val[i]);
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) h += __shfl_xor_sync(0xffffffffu, h, o);
-    __shared__ unsigned long long ws[8];
-    if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = h;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        unsigned long long t = 0;
-        for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += ws[w];
-        if (t) atomicAdd(out, t);
-    }
-}
-
 // Keys of a batch: key k owns slots [excl[k], excl[k+1]) (excl[n] = *total).
 // A warp takes 32 consecutive keys and writes each key's run with all lanes,
 // 128 contiguous bytes per store.  Runs longer than EXP_LONG slots (a dense
@@ -398,6 +365,113 @@ __global__ void __launch_bounds__(256) k_expand_long(int32_t *__restrict__ outKe
     }
 }
 
+// The consumer fold of a device-resident batch, with the key array written in
+// the same pass: key k owns slots [excl[k], excl[k+1]) (excl[n] = *total); for
+// every slot the value is read back from HBM (it was written by the emission),
+// the key is stored, and splitmix64(key << 32 | value) is added to the set
+// hash.  8 bytes per pair move instead of the 12 of a key expansion followed
+// by a fold that reads both arrays.  Runs longer than EXP_LONG are queued for
+// whole CTAs (k_fold_long).  Skipped when the batch's count exceeds cap.
+__device__ __forceinline__ unsigned long long fold_run(const int32_t *__restrict__ val, int32_t *__restrict__ outKey,
+                                                       uint32_t s0, uint32_t e0, int32_t key, uint32_t t,
+                                                       uint32_t nt)
+{
+    const unsigned long long hk = (unsigned long long)(uint32_t)key << 32;
+    unsigned long long h = 0;
+    const uint32_t a = min((s0 + 3u) & ~3u, e0);
+    const uint32_t b = a + ((e0 - a) & ~3u);
+    if (t < a - s0) {
+        const uint32_t p = s0 + t;
+        outKey[p] = key;
+        h += splitmix64(hk | (uint32_t)__ldcs(val + p));
+    }
+    const int4 kv = make_int4(key, key, key, key);
+    for (uint32_t pos = a + 4 * t; pos < b; pos += 4 * nt) {
+        const int4 v = __ldcs(reinterpret_cast<const int4 *>(val + pos));
+        __stcs(reinterpret_cast<int4 *>(outKey + pos), kv);
+        h += splitmix64(hk | (uint32_t)v.x);
+        h += splitmix64(hk | (uint32_t)v.y);
+        h += splitmix64(hk | (uint32_t)v.z);
+        h += splitmix64(hk | (uint32_t)v.w);
+    }
+    if (t < e0 - b) {
+        const uint32_t p = b + t;
+        outKey[p] = key;
+        h += splitmix64(hk | (uint32_t)__ldcs(val + p));
+    }
+    return h;
+}
+
+__device__ __forceinline__ void block_add_hash(unsigned long long h, unsigned long long *out)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) h += __shfl_xor_sync(0xffffffffu, h, o);
+    __shared__ unsigned long long ws[8];
+    if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = h;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long t = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += ws[w];
+        if (t) atomicAdd(out, t);
+    }
+}
+
+__global__ void __launch_bounds__(256) k_fold_expand(const uint32_t *__restrict__ excl,
+                                                     const uint32_t *__restrict__ total, uint64_t n,
+                                                     const int32_t *__restrict__ val, int32_t *__restrict__ outKey,
+                                                     const unsigned long long *__restrict__ batchPairs, uint64_t cap,
+                                                     uint4 *__restrict__ longRuns, uint32_t longCap,
+                                                     uint32_t *__restrict__ longCount,
+                                                     unsigned long long *__restrict__ hashOut)
+{
+    if (*batchPairs > cap) return;
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint64_t k0 = ((uint64_t)blockIdx.x * 256 + (threadIdx.x & ~31u));
+    unsigned long long h = 0;
+    if (k0 < n) {
+        const uint64_t k = k0 + lane;
+        const uint32_t tot = *total;
+        const uint32_t st = k < n ? excl[k] : tot;
+        const uint32_t en = k + 1 < n ? excl[k + 1] : tot;
+        uint32_t live = __ballot_sync(0xffffffffu, en > st);
+        while (live) {
+            const int i = __ffs(live) - 1;
+            live &= live - 1;
+            const uint32_t s0 = __shfl_sync(0xffffffffu, st, i);
+            const uint32_t e0 = __shfl_sync(0xffffffffu, en, i);
+            const int32_t key = (int32_t)(k0 + i);
+            if (e0 - s0 > EXP_LONG) {
+                uint32_t j = 0;
+                if (lane == 0) j = atomicAdd(longCount, 1u);
+                j = __shfl_sync(0xffffffffu, j, 0);
+                if (j < longCap) {
+                    if (lane == 0) longRuns[j] = make_uint4((uint32_t)key, s0, e0, 0u);
+                    continue;
+                }
+            }
+            h += fold_run(val, outKey, s0, e0, key, lane, 32);
+        }
+    }
+    block_add_hash(h, hashOut);
+}
+
+// The queued long runs of k_fold_expand, one CTA per run at a time.
+__global__ void __launch_bounds__(256) k_fold_long(const int32_t *__restrict__ val, int32_t *__restrict__ outKey,
+                                                   const unsigned long long *__restrict__ batchPairs, uint64_t cap,
+                                                   const uint4 *__restrict__ longRuns, uint32_t longCap,
+                                                   const uint32_t *__restrict__ longCount,
+                                                   unsigned long long *__restrict__ hashOut)
+{
+    if (*batchPairs > cap) return;
+    const uint32_t cnt = min(*longCount, longCap);
+    unsigned long long h = 0;
+    for (uint32_t j = blockIdx.x; j < cnt; j += gridDim.x) {
+        const uint4 r = longRuns[j];
+        h += fold_run(val, outKey, r.y, r.z, (int32_t)r.x, threadIdx.x, blockDim.x);
+    }
+    block_add_hash(h, hashOut);
+}
+
 // Appends a batch to a device CSR neighbour table: key k's run
 // [start[k], start[k+1]) of vals (start[n] = *total) goes to
 // cols[rowPtr[k] + fill[k] ...] and fill[k] grows by its length.  A warp takes
@@ -439,17 +513,6 @@ __global__ void __launch_bounds__(256) k_csr_append(const uint32_t *__restrict__
 
 }  // namespace
 
-cudaError_t sj_hash_pairs_dev(const int32_t *key, const int32_t *val, const unsigned long long *count, uint64_t cap,
-                              uint64_t gridHint, int numSM, unsigned long long *hashOut, cudaStream_t s)
-{
-    uint64_t blocks = ceil_div(gridHint ? gridHint : 1, 256 * 16);
-    if (blocks > (uint64_t)numSM * 8) blocks = (uint64_t)numSM * 8;
-    if (blocks == 0) blocks = 1;
-    k_hash_pairs_dev<<<(unsigned)blocks, 256, 0, s>>>(key, val, count, cap, hashOut);
-    sj_note_launch();
-    return cudaGetLastError();
-}
-
 cudaError_t sj_expand_keys(const uint32_t *excl, const uint32_t *total, uint64_t n, int32_t *outKey,
                            const unsigned long long *batchPairs, uint64_t cap, void *longRuns, uint32_t longCap,
                            uint32_t *longCount, int numSM, cudaStream_t s)
@@ -462,6 +525,23 @@ cudaError_t sj_expand_keys(const uint32_t *excl, const uint32_t *total, uint64_t
     sj_note_launch();
     k_expand_long<<<(unsigned)(numSM * 8), 256, 0, s>>>(outKey, batchPairs, cap, (const uint4 *)longRuns, longCap,
                                                        longCount);
+    sj_note_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t sj_fold_expand(const uint32_t *excl, const uint32_t *total, uint64_t n, const int32_t *val,
+                           int32_t *outKey, const unsigned long long *batchPairs, uint64_t cap, void *longRuns,
+                           uint32_t longCap, uint32_t *longCount, unsigned long long *hashOut, int numSM,
+                           cudaStream_t s)
+{
+    if (n == 0) return cudaSuccess;
+    cudaError_t e = cudaMemsetAsync(longCount, 0, sizeof(uint32_t), s);
+    if (e != cudaSuccess) return e;
+    k_fold_expand<<<(unsigned)ceil_div(n, 256), 256, 0, s>>>(excl, total, n, val, outKey, batchPairs, cap,
+                                                             (uint4 *)longRuns, longCap, longCount, hashOut);
+    sj_note_launch();
+    k_fold_long<<<(unsigned)(numSM * 8), 256, 0, s>>>(val, outKey, batchPairs, cap, (const uint4 *)longRuns, longCap,
+                                                     longCount, hashOut);
     sj_note_launch();
     return cudaGetLastError();
 }
