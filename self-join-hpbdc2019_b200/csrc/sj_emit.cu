@@ -66,6 +66,11 @@ constexpr int PF = SJ_EMIT_PF;
 #ifndef SJ_EMIT_MINB
 #define SJ_EMIT_MINB 4
 #endif
+// 1: a CTA takes EW/32 consecutive units per round (one atomic), 0: each warp
+// takes units on its own
+#ifndef SJ_EMIT_COOP
+#define SJ_EMIT_COOP 0
+#endif
 
 struct WarpSmem {
     uint16_t ent[EM_CAP];   // staged entries in slot order: rows (query << 11) | chunk position,
@@ -344,11 +349,25 @@ __global__ void __launch_bounds__(EW, SJ_EMIT_MINB) k_emit(sj_join_args a)
     }
     const uint64_t u0 = a.unitOff[a.taskBegin];
     const uint32_t nUnits = (uint32_t)(a.unitOff[a.taskEnd] - u0);
+#if SJ_EMIT_COOP
+    // the CTA's warps take consecutive units (mostly of one task), so the
+    // task's candidate ids and query ids are shared through L1
+    __shared__ uint32_t ctaBase;
+#endif
     for (;;) {
+#if SJ_EMIT_COOP
+        __syncthreads();   // every warp is done with the previous round's units
+        if (threadIdx.x == 0) ctaBase = atomicAdd(a.queueHead, (uint32_t)ENW);
+        __syncthreads();
+        if (ctaBase >= nUnits) break;   // uniform over the CTA
+        const uint32_t un = ctaBase + (threadIdx.x >> 5);
+        if (un >= nUnits) continue;
+#else
         uint32_t un = 0;
         if (lane == 0) un = atomicAdd(a.queueHead, 1u);
         un = __shfl_sync(FULL, un, 0);
         if (un >= nUnits) break;
+#endif
         // the unit's task: the last t with unitOff[t] - u0 <= un
         uint32_t lo = a.taskBegin, hi = a.taskEnd;
         while (hi - lo > 1) {
