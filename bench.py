@@ -369,9 +369,13 @@ def run_ours(args):
     sj = make_ctx(prec, learned)
     stream = torch.cuda.ExternalStream(sj.stream())
 
+    delivery = {"none": sjoin.DELIVER_NONE, "device": sjoin.DELIVER_DEVICE}[args.delivery]
+
     def step():
         sj.build_index()
-        return sj.join(sjoin.DELIVER_NONE)
+        if delivery == sjoin.DELIVER_DEVICE:   # every batch handed to a consumer that reads nothing
+            return sj.join(delivery, lambda i, kp, vp, cnt: None)
+        return sj.join(delivery)
 
     sampler = ClockSampler(torch.cuda.current_device())
     # warm-up, then the timed steps (clocks sampled throughout the timed region)
@@ -542,6 +546,9 @@ def main():
     ap.add_argument("--fp64-steps", type=int, default=2,
                     help="timed steps of the plain FP64 method on the same points (0: skip)")
     ap.add_argument("--e2e-steps", type=int, default=1, help="timed end-to-end steps with host delivery (0: skip)")
+    ap.add_argument("--delivery", choices=["none", "device"], default="none",
+                    help="timed steps: on-device fold of every batch (none) or every batch handed to a "
+                         "device-memory consumer one at a time (device)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-ref-cuda", action="store_true",
                     help="skip the small workloads timed beside the reference's own CUDA pipeline")

@@ -192,7 +192,10 @@ sj_status sj_get_stats(sj_ctx *ctx, sj_stats *st);
 sj_status sj_get_stream(sj_ctx *ctx, void **stream);
 
 /* Learned estimator.  Weights: SJ_MLP_NPARAM floats laid out W1[16x64], b1[64],
- * W2[64x64], b2[64], W3[64x2], b3[2] (row-major, input-major). */
+ * W2[64x64], b2[64], W3[64x2], b3[2] (row-major, input-major).  The network's
+ * two outputs predict, per cell, log2(1 + hits among its own points) and
+ * log2(1 + hits among its owned neighbours' points) (the targets
+ * sj_cell_samples measures); the evaluations themselves are computed exactly. */
 uint32_t sj_mlp_num_params(void);
 sj_status sj_set_estimator_weights(sj_ctx *ctx, const float *w, uint32_t count);
 sj_status sj_load_estimator(sj_ctx *ctx, const char *path);
@@ -201,6 +204,16 @@ sj_status sj_load_estimator(sj_ctx *ctx, const char *path);
  * measured per-cell hits and distance calculations (full-stencil semantics).
  * feat: nNonEmpty x 16 floats; hits/calcs: nNonEmpty doubles; NULL skips. */
 sj_status sj_cell_features(sj_ctx *ctx, float *feat, double *hits, double *calcs);
+
+/* Per-cell counts of the sampling estimator (scheduler SJ_SCHED_SAMPLING):
+ * runs the estimate for the built index and writes, per non-empty cell, the
+ * hits and evaluations of its sampled points among its own points (home, self
+ * included) and among its owned neighbours' points (one direction).  With
+ * sample_rate = 1 every point is sampled and the counts are exact: they are
+ * the learned estimator's training targets.  Each array: nNonEmpty doubles;
+ * NULL skips it.  No counterpart in the reference (its estimator returns one
+ * total, GPU.cu:854-1065). */
+sj_status sj_cell_samples(sj_ctx *ctx, double *homeHits, double *homeEvals, double *nbrHits, double *nbrEvals);
 
 /* Device training of the estimator MLP by the project's own kernels.
  * x: m x 16, y: m x 2 (host float arrays); w: in/out parameters. */

@@ -241,6 +241,7 @@ struct Ctx {
     uint64_t csrCap = 0;
     DevBuf<uint32_t> csrFill;
     DevBuf<uint4> longRuns;            // key expansion: runs too long for one warp
+    DevBuf<uint32_t> foldChunkKey;     // consumer fold: the key at each chunk's first slot
     DevBuf<uint32_t> longCount;
     DevBuf<unsigned long long> batchTot;
     std::vector<cudaEvent_t> events;   // per-batch stage boundaries of the asynchronous phase
@@ -261,6 +262,7 @@ struct Ctx {
     DevBuf<unsigned long long> sHits, sCands, sScalars;
     DevBuf<unsigned long long> dCellHits;   // measured hits per cell (after sj_degrees)
     bool haveMeas = false;
+    bool haveSamples = false;   // sHits / sCands hold the last sampling estimate's per-cell counts
     sj_stats st{};
 };
 
@@ -519,7 +521,8 @@ FilterBounds filter_bounds(const Ctx &c)
 // --------------------------------------------------------------- tasks --
 struct BatchRange {
     uint32_t t0, t1;
-    double pred;   // planned batch: its predicted pairs; a part re-planned after an overflow: -1
+    double pred;      // planned batch: its predicted pairs; a part re-planned after an overflow: -1
+    uint64_t exact;   // a re-planned part: its measured pairs (0 for a planned batch)
 };
 
 sj_status run_count(Ctx &c, sj_join_args &a, bool queue, cudaStream_t st = nullptr)
@@ -706,7 +709,7 @@ sj_status plan_dev(Ctx &c, uint64_t cap, std::vector<BatchRange> &plan, uint64_t
     CK(cudaStreamSynchronize(c.s));
     plan.resize(nb);
     for (uint32_t b = 0; b < nb; b++) {
-        plan[b] = {start[b], start[b + 1], (double)st[(size_t)b * 5]};
+        plan[b] = {start[b], start[b + 1], (double)st[(size_t)b * 5], 0};
         for (int k = 0; k < 4; k++) maxes[k] = std::max<uint64_t>(maxes[k], st[(size_t)b * 5 + 1 + k]);
     }
     return SJ_OK;
@@ -724,14 +727,15 @@ sj_status estimate_rates(Ctx &c)
     Timer tm;
     tm.start(c.s);
     const uint32_t nc = c.nCells;
-    CK(c.rate.ensure(nc ? nc : 1));
+    CK(c.rate.ensure(2 * (size_t)(nc ? nc : 1)));
     if (c.p.scheduler == SJ_SCHED_LEARNED && !c.mlpW.empty()) {
         DevBuf<float> &out = c.sMlpOut;
         CK(out.ensure((size_t)nc * SJ_NOUT));
         CK(c.dMlpW.ensure(SJ_MLP_NPARAM));
         CK(cudaMemcpyAsync(c.dMlpW.p, c.mlpW.data(), sizeof(float) * SJ_MLP_NPARAM, cudaMemcpyHostToDevice, c.s));
         CK(sj_launch_mlp_infer(c.feat.p, nc, c.dMlpW.p, out.p, c.s));
-        CK(sj_rates_mlp(out.p, reinterpret_cast<const unsigned long long *>(c.candFull.p), nc, c.rate.p, c.s));
+        CK(sj_rates_mlp(out.p, c.cellStart.p, c.nbrStart.p, c.nbrCell.p, nc, c.rate.p, c.s));
+        c.haveSamples = false;
     } else {
         CKS(build_tasks_dev(c, false, 0xffffffffULL, false, 1, (float)c.p.sample_rate, false));
         const uint32_t nt = c.nTasks;
@@ -756,11 +760,12 @@ sj_status estimate_rates(Ctx &c)
         a.taskBegin = 0;
         a.taskEnd = nt;
         CKS(run_count(c, a, true));
-        CK(c.sHits.ensure(nc ? nc : 1));
-        CK(c.sCands.ensure(nc ? nc : 1));
+        CK(c.sHits.ensure(2 * (size_t)(nc ? nc : 1)));
+        CK(c.sCands.ensure(2 * (size_t)(nc ? nc : 1)));
         CK(c.sScalars.ensure(2 + sj_sample_totals_len()));
         CK(sj_sample_rates(c.dTasks.p, nt, c.taskHits.p, c.dTaskEvals.p, c.cellStart.p, c.sHits.p, c.sCands.p,
                            c.sScalars.p + 2, nc, c.rate.p, c.s));
+        c.haveSamples = true;
     }
     c.st.ms_estimate = tm.stop(c.s);
     return SJ_OK;
@@ -845,13 +850,13 @@ sj_status replan_exact(const BatchRange &br, const std::vector<uint32_t> &taskHi
             return SJ_ERR_INTERNAL;
         }
         if (t > t0 && acc + h > cap) {
-            parts.push_back({t0, t, -1.0});
+            parts.push_back({t0, t, -1.0, acc});
             t0 = t;
             acc = 0;
         }
         acc += h;
     }
-    parts.push_back({t0, br.t1, -1.0});
+    parts.push_back({t0, br.t1, -1.0, acc});
     out.insert(out.end(), parts.begin(), parts.end());
     return SJ_OK;
 }
@@ -962,7 +967,6 @@ sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
     int pinSel = 0;
     sj_status result = SJ_OK;
     CK(c.batchTot.ensure(plan.size() + 1));
-    CK(cudaMemsetAsync(c.batchTot.p, 0, sizeof(unsigned long long) * (plan.size() + 1), c.s));
     CK(cudaMemsetAsync(c.keyCount.p, 0, sizeof(uint32_t) * n, c.s));   // each scan clears it again
     // estimator error of a planned batch against its measured pairs
     auto noteErr = [&](const BatchRange &br, uint64_t measured) {
@@ -973,15 +977,20 @@ sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
     };
 
     // ---- asynchronous phase: batches folded on the device (no host delivery).
-    // Every batch runs count -> scan -> key expansion -> emission -> hash
-    // without a host round trip; a batch whose count exceeds the output buffer
-    // skips its expansion and emission and is re-run below, split.
+    // Every batch runs count -> scan -> emission -> fold without a host round
+    // trip; a batch whose count exceeds the output buffer skips its emission
+    // and fold.  Such batches are re-planned exactly from the count pass's
+    // per-task pairs and run through the same pipeline in a further round (the
+    // exact parts cannot overflow again).
     std::vector<BatchRange> stack;
-    if (delivery == SJ_DELIVER_NONE && !plan.empty()) {
-        double maxPred = 0;
-        for (const BatchRange &br : plan) maxPred = std::max(maxPred, br.pred * (1.0 + c.p.alpha));
+    std::vector<BatchRange> todo;
+    if (delivery == SJ_DELIVER_NONE) todo.assign(plan.rbegin(), plan.rend());   // ascending task order
+    for (int round = 0; !todo.empty(); round++) {
+        double maxPairs = 0;
+        for (const BatchRange &br : todo)
+            maxPairs = std::max(maxPairs, br.pred >= 0 ? br.pred * (1.0 + c.p.alpha) : (double)br.exact);
         uint64_t bufCap = c.p.batch_capacity_pairs ? cap
-                                                   : std::min<uint64_t>(cap, (uint64_t)(1.25 * maxPred) + 65536);
+                                                   : std::min<uint64_t>(cap, (uint64_t)(1.25 * maxPairs) + 65536);
         if (bufCap > c.outKey.n) {
             CK(c.outKey.ensure(bufCap));
             CK(c.outVal.ensure(bufCap));
@@ -990,7 +999,10 @@ sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
         a.outKey = c.outKey.p;
         a.outVal = c.outVal.p;
         a.capacity = bufCap;
-        const size_t nplan = plan.size();
+        CK(c.foldChunkKey.ensure(sj_fold_chunks(bufCap)));
+        CK(c.batchTot.ensure(todo.size() + 1));
+        CK(cudaMemsetAsync(c.batchTot.p, 0, sizeof(unsigned long long) * (todo.size() + 1), c.s));
+        const size_t nplan = todo.size();
         // Two streams when the device has room for a second record set: the
         // count pass and scan of each batch on the engine's stream, its key
         // expansion, emission and fold on the second stream, so batch i + 1's
@@ -1041,7 +1053,7 @@ sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
         }
         cudaEvent_t *ev = c.events.data();
         for (size_t i = 0; i < nplan; i++) {
-            const BatchRange &br = plan[nplan - 1 - i];   // plan is stored as a stack
+            const BatchRange &br = todo[i];
             cudaEvent_t *e = ev + EV * i;
             sj_join_args b = a;
             b.taskBegin = br.t0;
@@ -1074,14 +1086,8 @@ sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
             CK(cudaMemsetAsync(b.queueHead, 0, sizeof(uint32_t), sB));
             CK(sj_launch_emit(b, c.numSM, sB));
             CK(cudaEventRecord(e[6], sB));
-            {
-                const size_t slots = sj_expand_long_slots(b.capacity);
-                CK(c.longRuns.ensure(slots));
-                CK(c.longCount.ensure(1));
-                CK(sj_fold_expand(b.keyStart, scanTot, n, c.outVal.p, c.outKey.p, b.batchPairs, bufCap, c.longRuns.p,
-                                  (uint32_t)std::min<size_t>(c.longRuns.n, 0xffffffffu), c.longCount.p, c.stat.p + 4,
-                                  c.numSM, sB));
-            }
+            CK(sj_fold(b.keyStart, scanTot, n, c.outVal.p, c.outKey.p, b.batchPairs, bufCap, c.foldChunkKey.p,
+                       c.stat.p + 4, c.numSM, sB));
             CK(cudaEventRecord(e[7], sB));
         }
         if (pipe) CK(cudaStreamWaitEvent(sA, ev[EV * (nplan - 1) + 7], 0));
@@ -1108,13 +1114,12 @@ sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
         }
         std::vector<BatchRange> redo;
         for (size_t i = 0; i < nplan; i++) {
-            const BatchRange &br = plan[nplan - 1 - i];
+            const BatchRange &br = todo[i];
             noteErr(br, tot[i]);   // the count pass measured the batch exactly, overflowed or not
             if (tot[i] > bufCap) {
                 // the count pass measured every task's pairs: re-plan this
-                // batch's tasks exactly, so the re-runs cannot overflow again
-                // (against the capacity: the synchronous phase grows the
-                // buffers up to it, and no task's worst case exceeds it)
+                // batch's tasks exactly against the capacity (the next round
+                // grows the buffers up to it; no task's worst case exceeds it)
                 CKS(replan_exact(br, hTaskHits, cap, redo));
                 retries++;
                 continue;
@@ -1122,10 +1127,9 @@ sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
             pairsTotal += tot[i];
             batches++;
         }
-        stack.assign(redo.rbegin(), redo.rend());   // popped in ascending task order
-    } else {
-        stack = plan;
+        todo.swap(redo);
     }
+    if (delivery != SJ_DELIVER_NONE) stack = plan;
 
     // ---- synchronous phase: host / device delivery, and batches to re-plan.
     // Host delivery does not copy the key array over PCIe: the keys of a
@@ -1850,6 +1854,40 @@ sj_status sj_cell_features(sj_ctx *ctx, float *feat, double *hits, double *calcs
         std::vector<unsigned long long> v(nc);
         CK(cudaMemcpy(v.data(), c.dCellHits.p, sizeof(unsigned long long) * nc, cudaMemcpyDeviceToHost));
         for (uint32_t i = 0; i < nc; i++) hits[i] = (double)v[i];
+    }
+    return SJ_OK;
+}
+
+sj_status sj_cell_samples(sj_ctx *ctx, double *homeHits, double *homeEvals, double *nbrHits, double *nbrEvals)
+{
+    if (!ctx) return SJ_ERR_BAD_INPUT;
+    Ctx &c = *as_ctx(ctx);
+    if (!c.indexed) {
+        set_error("index not built");
+        return SJ_ERR_STATE;
+    }
+    if (c.p.scheduler != SJ_SCHED_SAMPLING) {
+        set_error("sj_cell_samples needs the sampling scheduler");
+        return SJ_ERR_STATE;
+    }
+    CKS(bind(c));
+    int pattern;
+    bool queue;
+    CKS(prepare_join(c, pattern, queue));   // owned-neighbour lists and the sampling estimate
+    if (!c.haveSamples) {
+        set_error("internal: no sampling estimate");
+        return SJ_ERR_INTERNAL;
+    }
+    const uint32_t nc = c.nCells;
+    std::vector<unsigned long long> h(2 * (size_t)nc), e(2 * (size_t)nc);
+    CK(cudaMemcpyAsync(h.data(), c.sHits.p, sizeof(unsigned long long) * h.size(), cudaMemcpyDeviceToHost, c.s));
+    CK(cudaMemcpyAsync(e.data(), c.sCands.p, sizeof(unsigned long long) * e.size(), cudaMemcpyDeviceToHost, c.s));
+    CK(cudaStreamSynchronize(c.s));
+    for (uint32_t i = 0; i < nc; i++) {
+        if (homeHits) homeHits[i] = (double)h[2 * (size_t)i];
+        if (homeEvals) homeEvals[i] = (double)e[2 * (size_t)i];
+        if (nbrHits) nbrHits[i] = (double)h[2 * (size_t)i + 1];
+        if (nbrEvals) nbrEvals[i] = (double)e[2 * (size_t)i + 1];
     }
     return SJ_OK;
 }

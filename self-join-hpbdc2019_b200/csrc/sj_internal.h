@@ -120,7 +120,8 @@ struct sj_taskgen {
     const uint32_t *cellStart;   // nCells+1
     const uint32_t *nbrStart;    // nCells+1, owned neighbour lists
     const uint32_t *nbrCell;
-    const float *rate;           // per cell predicted hits per evaluation (null: 0)
+    const float *rate;           // per cell: predicted hits per evaluation against its own points and
+                                 // against its neighbours' (2 floats; null: 0)
     const uint32_t *groupBase;   // per cell: first slot in groupLen (exclusive scan of segment groups)
     uint32_t *groupLen;          // per segment group: stream length without the home segment
     uint32_t nCells;
@@ -166,11 +167,11 @@ size_t sj_expand_long_slots(uint64_t cap);
 // consumer fold of a device-resident batch with the key array written in the
 // same pass: reads the values, writes the keys from the key runs (as
 // sj_expand_keys), adds the pairs' set hash to *hashOut; skipped when the
-// batch's count exceeds cap.  longRuns / longCount as for sj_expand_keys.
-cudaError_t sj_fold_expand(const uint32_t *excl, const uint32_t *total, uint64_t n, const int32_t *val,
-                           int32_t *outKey, const unsigned long long *batchPairs, uint64_t cap, void *longRuns,
-                           uint32_t longCap, uint32_t *longCount, unsigned long long *hashOut, int numSM,
-                           cudaStream_t s);
+// batch's count exceeds cap.  chunkKey: sj_fold_chunks(cap) entries of scratch.
+size_t sj_fold_chunks(uint64_t cap);
+cudaError_t sj_fold(const uint32_t *excl, const uint32_t *total, uint64_t n, const int32_t *val, int32_t *outKey,
+                    const unsigned long long *batchPairs, uint64_t cap, uint32_t *chunkKey,
+                    unsigned long long *hashOut, int numSM, cudaStream_t s);
 // appends a batch (values vals, key runs start[0..n], start[n] = *total) to a
 // device CSR table rowPtr[n+1] / cols[colsCap]; fill[n] are the rows' cursors
 cudaError_t sj_csr_append(const uint32_t *start, const uint32_t *total, uint64_t n, const int32_t *vals,
@@ -242,11 +243,14 @@ cudaError_t sj_plan_batches(unsigned long long *const off[7], uint32_t nt, unsig
 // per batch: predicted pairs, row-mask words, column-mask words, row offsets, candidate records
 cudaError_t sj_plan_stats(const uint32_t *start, uint32_t nb, unsigned long long *const off[7],
                           unsigned long long *stats, cudaStream_t s);
-cudaError_t sj_rates_mlp(const float *out, const unsigned long long *candFull, uint32_t nCells, float *rate,
-                         cudaStream_t s);
-// sampling estimator: per-cell rates from the sampled tasks' hits and
-// evaluations; totals has sj_sample_totals_len() entries (global and per
-// occupancy class, for the cells without a sample)
+// learned estimator: rates (2 per cell: home, owned neighbours) from the
+// network's outputs (log2(1 + home hits), log2(1 + owned-neighbour hits))
+cudaError_t sj_rates_mlp(const float *out, const uint32_t *cellStart, const uint32_t *nbrStart,
+                         const uint32_t *nbrCell, uint32_t nCells, float *rate, cudaStream_t s);
+// sampling estimator: per-cell rates (2 per cell: home, neighbours) from the
+// sampled tasks' hits and evaluations; cellHits / cellEvals: 2 per cell;
+// totals has sj_sample_totals_len() entries (per occupancy class and global,
+// for the cells without a sample)
 size_t sj_sample_totals_len();
 cudaError_t sj_sample_rates(const sj_task *tasks, uint32_t nt, const uint32_t *taskHits, const uint32_t *taskEvals,
                             const uint32_t *cellStart, unsigned long long *cellHits, unsigned long long *cellEvals,

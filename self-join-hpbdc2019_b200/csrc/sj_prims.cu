@@ -366,110 +366,105 @@ __global__ void __launch_bounds__(256) k_expand_long(int32_t *__restrict__ outKe
 }
 
 // The consumer fold of a device-resident batch, with the key array written in
-// the same pass: key k owns slots [excl[k], excl[k+1]) (excl[n] = *total); for
-// every slot the value is read back from HBM (it was written by the emission),
-// the key is stored, and splitmix64(key << 32 | value) is added to the set
-// hash.  8 bytes per pair move instead of the 12 of a key expansion followed
-// by a fold that reads both arrays.  Runs longer than EXP_LONG are queued for
-// whole CTAs (k_fold_long).  Skipped when the batch's count exceeds cap.
-__device__ __forceinline__ unsigned long long fold_run(const int32_t *__restrict__ val, int32_t *__restrict__ outKey,
-                                                       uint32_t s0, uint32_t e0, int32_t key, uint32_t t,
-                                                       uint32_t nt)
+// the same pass.  Key k owns slots [excl[k], excl[k+1]) (excl[n] = *total).
+// The slots are cut into chunks of FOLD_CHUNK; k_fold_chunk_keys records the
+// key at each chunk's first slot (one thread per key writes the chunks its run
+// starts), and in k_fold a warp takes a chunk, reads the values back from HBM
+// in 16-byte streaming loads, finds each slot's key among a window of 32 run
+// ends held one per lane (a 5-step shuffle search), stores the keys in 16-byte
+// streaming stores and adds splitmix64(key << 32 | value) to the set hash.
+// Every chunk is the same size, so the work is balanced whatever the run
+// lengths.  8 bytes per pair move, against 12 for a key expansion followed by
+// a fold that reads both arrays.  Skipped when the batch's count exceeds cap.
+constexpr uint32_t FOLD_CHUNK = 4096;
+
+__global__ void __launch_bounds__(256) k_fold_chunk_keys(const uint32_t *__restrict__ excl,
+                                                         const uint32_t *__restrict__ total, uint64_t n,
+                                                         const unsigned long long *__restrict__ batchPairs,
+                                                         uint64_t cap, uint32_t *__restrict__ chunkKey)
 {
-    const unsigned long long hk = (unsigned long long)(uint32_t)key << 32;
-    unsigned long long h = 0;
-    const uint32_t a = min((s0 + 3u) & ~3u, e0);
-    const uint32_t b = a + ((e0 - a) & ~3u);
-    if (t < a - s0) {
-        const uint32_t p = s0 + t;
-        outKey[p] = key;
-        h += splitmix64(hk | (uint32_t)__ldcs(val + p));
-    }
-    const int4 kv = make_int4(key, key, key, key);
-    for (uint32_t pos = a + 4 * t; pos < b; pos += 4 * nt) {
-        const int4 v = __ldcs(reinterpret_cast<const int4 *>(val + pos));
-        __stcs(reinterpret_cast<int4 *>(outKey + pos), kv);
-        h += splitmix64(hk | (uint32_t)v.x);
-        h += splitmix64(hk | (uint32_t)v.y);
-        h += splitmix64(hk | (uint32_t)v.z);
-        h += splitmix64(hk | (uint32_t)v.w);
-    }
-    if (t < e0 - b) {
-        const uint32_t p = b + t;
-        outKey[p] = key;
-        h += splitmix64(hk | (uint32_t)__ldcs(val + p));
-    }
-    return h;
+    if (*batchPairs > cap) return;
+    const uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const uint32_t tot = *total;
+    const uint32_t st = excl[k];
+    const uint32_t en = k + 1 < n ? excl[k + 1] : tot;
+    for (uint32_t c = (st + FOLD_CHUNK - 1) / FOLD_CHUNK; (uint64_t)c * FOLD_CHUNK < en; c++) chunkKey[c] = (uint32_t)k;
 }
 
-__device__ __forceinline__ void block_add_hash(unsigned long long h, unsigned long long *out)
+__global__ void __launch_bounds__(256) k_fold(const uint32_t *__restrict__ excl, const uint32_t *__restrict__ total,
+                                              uint64_t n, const int32_t *__restrict__ val,
+                                              int32_t *__restrict__ outKey,
+                                              const unsigned long long *__restrict__ batchPairs, uint64_t cap,
+                                              const uint32_t *__restrict__ chunkKey,
+                                              unsigned long long *__restrict__ hashOut)
 {
+    if (*batchPairs > cap) return;
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t tot = *total;
+    const uint32_t nChunks = (tot + FOLD_CHUNK - 1) / FOLD_CHUNK;
+    const uint32_t warpsAll = (gridDim.x * blockDim.x) >> 5;
+    unsigned long long h = 0;
+    // end of the run of key kk (the total past the last key)
+    auto runEnd = [&](uint64_t kk) -> uint32_t { return kk + 1 < n ? excl[kk + 1] : tot; };
+    for (uint32_t c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; c < nChunks; c += warpsAll) {
+        const uint32_t p0 = c * FOLD_CHUNK, p1 = min(p0 + FOLD_CHUNK, tot);
+        uint64_t k = chunkKey[c];
+        uint32_t R = runEnd(k + lane);   // lane j: end of the run of key k + j
+        for (uint32_t base = p0; base < p1; base += 128) {
+            const uint32_t p = base + 4 * lane;
+            const uint32_t cnt = p < p1 ? min(4u, p1 - p) : 0u;   // this lane's slots: p .. p + cnt - 1
+            uint32_t v[4] = {0, 0, 0, 0};
+            if (cnt == 4) {
+                const int4 x = __ldcs(reinterpret_cast<const int4 *>(val + p));
+                v[0] = (uint32_t)x.x; v[1] = (uint32_t)x.y; v[2] = (uint32_t)x.z; v[3] = (uint32_t)x.w;
+            } else {
+                for (uint32_t i = 0; i < cnt; i++) v[i] = (uint32_t)__ldcs(val + p + i);
+            }
+            uint32_t key[4] = {0, 0, 0, 0};
+            uint32_t unres = (1u << cnt) - 1u;   // slots whose key is still unknown
+            for (;;) {
+                // slot s >= the window's first run start has key k + #{j : R_j <= s}
+                // while s is below the window's last run end R_31
+                const uint32_t Rlast = __shfl_sync(0xffffffffu, R, 31);
+#pragma unroll
+                for (int i = 0; i < 4; i++) {
+                    const uint32_t sl = p + (uint32_t)i;
+                    uint32_t m = 0;
+#pragma unroll
+                    for (uint32_t b = 16; b > 0; b >>= 1) {
+                        const uint32_t r = __shfl_sync(0xffffffffu, R, m + b - 1);
+                        if (r <= sl) m += b;
+                    }
+                    if (((unres >> i) & 1u) && sl < Rlast) {
+                        key[i] = (uint32_t)(k + m);
+                        unres &= ~(1u << i);
+                    }
+                }
+                if (__all_sync(0xffffffffu, unres == 0)) break;
+                // some slot lies past all 32 runs of the window: the next 32 runs
+                // (every unresolved slot is at or after their first start)
+                k += 32;
+                R = runEnd(k + lane);
+            }
+            if (cnt == 4) {
+                __stcs(reinterpret_cast<int4 *>(outKey + p), make_int4((int)key[0], (int)key[1], (int)key[2], (int)key[3]));
+            } else {
+                for (uint32_t i = 0; i < cnt; i++) outKey[p + i] = (int32_t)key[i];
+            }
+            for (uint32_t i = 0; i < cnt; i++) h += splitmix64(((unsigned long long)key[i] << 32) | v[i]);
+        }
+    }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) h += __shfl_xor_sync(0xffffffffu, h, o);
     __shared__ unsigned long long ws[8];
-    if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = h;
+    if (lane == 0) ws[threadIdx.x >> 5] = h;
     __syncthreads();
     if (threadIdx.x == 0) {
         unsigned long long t = 0;
         for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += ws[w];
-        if (t) atomicAdd(out, t);
+        if (t) atomicAdd(hashOut, t);
     }
-}
-
-__global__ void __launch_bounds__(256) k_fold_expand(const uint32_t *__restrict__ excl,
-                                                     const uint32_t *__restrict__ total, uint64_t n,
-                                                     const int32_t *__restrict__ val, int32_t *__restrict__ outKey,
-                                                     const unsigned long long *__restrict__ batchPairs, uint64_t cap,
-                                                     uint4 *__restrict__ longRuns, uint32_t longCap,
-                                                     uint32_t *__restrict__ longCount,
-                                                     unsigned long long *__restrict__ hashOut)
-{
-    if (*batchPairs > cap) return;
-    const uint32_t lane = threadIdx.x & 31u;
-    const uint64_t k0 = ((uint64_t)blockIdx.x * 256 + (threadIdx.x & ~31u));
-    unsigned long long h = 0;
-    if (k0 < n) {
-        const uint64_t k = k0 + lane;
-        const uint32_t tot = *total;
-        const uint32_t st = k < n ? excl[k] : tot;
-        const uint32_t en = k + 1 < n ? excl[k + 1] : tot;
-        uint32_t live = __ballot_sync(0xffffffffu, en > st);
-        while (live) {
-            const int i = __ffs(live) - 1;
-            live &= live - 1;
-            const uint32_t s0 = __shfl_sync(0xffffffffu, st, i);
-            const uint32_t e0 = __shfl_sync(0xffffffffu, en, i);
-            const int32_t key = (int32_t)(k0 + i);
-            if (e0 - s0 > EXP_LONG) {
-                uint32_t j = 0;
-                if (lane == 0) j = atomicAdd(longCount, 1u);
-                j = __shfl_sync(0xffffffffu, j, 0);
-                if (j < longCap) {
-                    if (lane == 0) longRuns[j] = make_uint4((uint32_t)key, s0, e0, 0u);
-                    continue;
-                }
-            }
-            h += fold_run(val, outKey, s0, e0, key, lane, 32);
-        }
-    }
-    block_add_hash(h, hashOut);
-}
-
-// The queued long runs of k_fold_expand, one CTA per run at a time.
-__global__ void __launch_bounds__(256) k_fold_long(const int32_t *__restrict__ val, int32_t *__restrict__ outKey,
-                                                   const unsigned long long *__restrict__ batchPairs, uint64_t cap,
-                                                   const uint4 *__restrict__ longRuns, uint32_t longCap,
-                                                   const uint32_t *__restrict__ longCount,
-                                                   unsigned long long *__restrict__ hashOut)
-{
-    if (*batchPairs > cap) return;
-    const uint32_t cnt = min(*longCount, longCap);
-    unsigned long long h = 0;
-    for (uint32_t j = blockIdx.x; j < cnt; j += gridDim.x) {
-        const uint4 r = longRuns[j];
-        h += fold_run(val, outKey, r.y, r.z, (int32_t)r.x, threadIdx.x, blockDim.x);
-    }
-    block_add_hash(h, hashOut);
 }
 
 // Appends a batch to a device CSR neighbour table: key k's run
@@ -529,19 +524,16 @@ cudaError_t sj_expand_keys(const uint32_t *excl, const uint32_t *total, uint64_t
     return cudaGetLastError();
 }
 
-cudaError_t sj_fold_expand(const uint32_t *excl, const uint32_t *total, uint64_t n, const int32_t *val,
-                           int32_t *outKey, const unsigned long long *batchPairs, uint64_t cap, void *longRuns,
-                           uint32_t longCap, uint32_t *longCount, unsigned long long *hashOut, int numSM,
-                           cudaStream_t s)
+size_t sj_fold_chunks(uint64_t cap) { return (size_t)(cap / FOLD_CHUNK) + 2; }
+
+cudaError_t sj_fold(const uint32_t *excl, const uint32_t *total, uint64_t n, const int32_t *val, int32_t *outKey,
+                    const unsigned long long *batchPairs, uint64_t cap, uint32_t *chunkKey,
+                    unsigned long long *hashOut, int numSM, cudaStream_t s)
 {
     if (n == 0) return cudaSuccess;
-    cudaError_t e = cudaMemsetAsync(longCount, 0, sizeof(uint32_t), s);
-    if (e != cudaSuccess) return e;
-    k_fold_expand<<<(unsigned)ceil_div(n, 256), 256, 0, s>>>(excl, total, n, val, outKey, batchPairs, cap,
-                                                             (uint4 *)longRuns, longCap, longCount, hashOut);
+    k_fold_chunk_keys<<<(unsigned)ceil_div(n, 256), 256, 0, s>>>(excl, total, n, batchPairs, cap, chunkKey);
     sj_note_launch();
-    k_fold_long<<<(unsigned)(numSM * 8), 256, 0, s>>>(val, outKey, batchPairs, cap, (const uint4 *)longRuns, longCap,
-                                                     longCount, hashOut);
+    k_fold<<<(unsigned)(numSM * 8), 256, 0, s>>>(excl, total, n, val, outKey, batchPairs, cap, chunkKey, hashOut);
     sj_note_launch();
     return cudaGetLastError();
 }

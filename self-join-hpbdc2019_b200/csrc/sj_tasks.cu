@@ -98,10 +98,28 @@ __device__ __forceinline__ uint32_t chunk_len(const sj_taskgen &g, float rate, u
 
 struct TileWork {
     uint32_t qBegin, qc, L, homeLen, sc, nChunks;
-    uint64_t evals;
+    uint64_t evHome, evOther;   // evaluations against the home segment / the owned neighbours
 };
 
+// Predicted hits per evaluation of cell c: [0] against its own points, [1]
+// against its neighbours' (both 0 without estimates).
+__device__ __forceinline__ float2 rates_of(const sj_taskgen &g, uint32_t c)
+{
+    return g.rate ? make_float2(g.rate[2 * c], g.rate[2 * c + 1]) : make_float2(0.0f, 0.0f);
+}
+
+// Predicted pairs of evH home and evO neighbour evaluations with `diag` of
+// the home ones a query against itself: a symmetric traversal emits a hit
+// in both directions, a self pair once.
+__device__ __forceinline__ double pairs_of(const sj_taskgen &g, float2 r, uint64_t evH, uint64_t evO, uint64_t diag)
+{
+    const double hits = (double)evH * (double)r.x + (double)evO * (double)r.y;
+    return g.sym ? fmax(0.0, 2.0 * hits - (double)diag) : hits;
+}
+
 // Query tile `tile` of cell c against segment group grp (non-home length S).
+// Sampling tasks (policy 1) chunk the home segment and the neighbours
+// separately, so that their hits are measured apart.
 __device__ __forceinline__ TileWork tile_work(const sj_taskgen &g, uint32_t c, uint32_t grp, uint32_t tile, uint32_t S,
                                               int workers)
 {
@@ -113,14 +131,30 @@ __device__ __forceinline__ TileWork tile_work(const sj_taskgen &g, uint32_t c, u
     w.qc = min(g.tile, nq - q0);
     w.homeLen = grp == 0 ? (g.sym ? occ - q0 : occ) : 0u;
     w.L = S + w.homeLen;
-    w.sc = chunk_len(g, g.rate ? g.rate[c] : 0.0f, w.qc, w.L, workers);
-    w.nChunks = (w.L + w.sc - 1) / w.sc;
     const uint64_t qc = w.qc;
-    if (g.sym && grp == 0)
-        w.evals = diag_evals(0, w.homeLen, qc) + qc * (uint64_t)S;
+    w.evHome = g.sym ? diag_evals(0, w.homeLen, qc) : qc * (uint64_t)w.homeLen;
+    w.evOther = qc * (uint64_t)S;
+    const float2 r = rates_of(g, c);
+    const double ev = (double)(w.evHome + w.evOther);
+    const float rate = ev > 0 ? (float)(((double)w.evHome * r.x + (double)w.evOther * r.y) / ev) : 0.0f;
+    w.sc = chunk_len(g, rate, w.qc, w.L, workers);
+    if (g.policy == 1)
+        w.nChunks = (w.homeLen + w.sc - 1) / w.sc + (S + w.sc - 1) / w.sc;
     else
-        w.evals = qc * (uint64_t)w.L;
+        w.nChunks = (w.L + w.sc - 1) / w.sc;
     return w;
+}
+
+// Stream positions of chunk j of a tile (see tile_work).
+__device__ __forceinline__ uint2 chunk_range(const sj_taskgen &g, const TileWork &w, uint32_t j)
+{
+    if (g.policy == 1) {
+        const uint32_t nh = (w.homeLen + w.sc - 1) / w.sc;
+        if (j < nh) return make_uint2(j * w.sc, min(w.homeLen, (j + 1) * w.sc));
+        const uint32_t s0 = w.homeLen + (j - nh) * w.sc;
+        return make_uint2(s0, min(w.L, s0 + w.sc));
+    }
+    return make_uint2(j * w.sc, min(w.L, (j + 1) * w.sc));
 }
 
 __device__ __forceinline__ uint32_t n_groups(const sj_taskgen &g, uint32_t c)
@@ -159,8 +193,9 @@ __global__ void __launch_bounds__(256) k_tg_cells(sj_taskgen g, const uint32_t *
     const uint32_t nSegAll = 1 + (g.nbrStart[c + 1] - nb0);
     const uint32_t G = (nSegAll + SJ_MAX_SEG - 1) / SJ_MAX_SEG;
     const uint32_t T = n_tiles(g, c);
-    const float rate = g.rate ? g.rate[c] : 0.0f;
+    const float2 r = rates_of(g, c);
     uint64_t cnt = 0, ev = 0;
+    double pred = 0.0;
     for (uint32_t grp = 0; grp < G; grp++) {
         const uint32_t s0 = grp * SJ_MAX_SEG, s1 = min(nSegAll, s0 + SJ_MAX_SEG);
         uint64_t S = 0;
@@ -174,17 +209,18 @@ __global__ void __launch_bounds__(256) k_tg_cells(sj_taskgen g, const uint32_t *
         for (uint32_t t = lane; t < T; t += 32) {
             const TileWork w = tile_work(g, c, grp, t, (uint32_t)S, workers);
             cnt += w.nChunks;
-            ev += w.evals;
+            ev += w.evHome + w.evOther;
+            pred += pairs_of(g, r, w.evHome, w.evOther, w.homeLen ? w.qc : 0u);
         }
     }
     cnt = warp_sum_u64(cnt);
     ev = warp_sum_u64(ev);
+    pred = warp_sum_f64(pred);
     if (lane == 0) {
         posCnt[pos] = (uint32_t)min(cnt, (uint64_t)FULL);
         if (posEv) posEv[pos] = ev;
         if (costKey) {
             // mean predicted task cost: evaluations plus a write cost per pair
-            const double pred = (double)ev * (double)rate * (g.sym ? 2.0 : 1.0);
             const double cost = cnt ? ((double)ev + 4.0 * pred) / (double)cnt : 0.0;
             costKey[pos] = ~(unsigned long long)__double_as_longlong(cost);   // cost >= 0: descending
         }
@@ -274,18 +310,19 @@ __global__ void __launch_bounds__(256) k_tg_item_write(sj_taskgen g, const uint3
     const TileWork w = tile_work(g, it.c, it.grp, it.tile, S, workersAt ? (int)workersAt[it.pos] : 0);
     const uint32_t nSegAll = 1 + (g.nbrStart[it.c + 1] - g.nbrStart[it.c]);
     const uint32_t segBase = it.grp * SJ_MAX_SEG;
-    const float rate = g.rate ? g.rate[it.c] : 0.0f;
-    const double mult = (double)rate * (g.sym ? 2.0 : 1.0);
+    const float2 r = rates_of(g, it.c);
     uint32_t t = itemTaskStart[j];
-    for (uint32_t s0 = 0; s0 < w.L; s0 += w.sc, t++) {
-        const uint32_t s1 = min(w.L, s0 + w.sc);
-        uint64_t ev;
-        if (g.sym && it.grp == 0 && s0 < w.homeLen) {
-            const uint32_t h1 = min(s1, w.homeLen);
-            ev = diag_evals(s0, h1, w.qc) + (uint64_t)w.qc * (s1 - h1);
-        } else {
-            ev = (uint64_t)w.qc * (s1 - s0);
+    for (uint32_t ch = 0; ch < w.nChunks; ch++, t++) {
+        const uint2 sr = chunk_range(g, w, ch);
+        const uint32_t s0 = sr.x, s1 = sr.y;
+        // evaluations against the home segment (positions < homeLen) and the rest
+        const uint32_t h1 = min(s1, w.homeLen);
+        uint64_t evH = 0, diag = 0;
+        if (s0 < h1) {
+            evH = g.sym ? diag_evals(s0, h1, w.qc) : (uint64_t)w.qc * (h1 - s0);
+            diag = s0 < w.qc ? min(h1, w.qc) - s0 : 0u;   // queries whose own position is in the chunk
         }
+        const uint64_t evO = (uint64_t)w.qc * (s1 - max(s0, h1));
         sj_task k;
         k.cell = it.c;
         k.qBegin = w.qBegin;
@@ -296,7 +333,7 @@ __global__ void __launch_bounds__(256) k_tg_item_write(sj_taskgen g, const uint3
         k.sEnd = s1;
         k.flags = (g.sym ? SJ_TASK_SYM : 0u) | (it.grp == 0 ? SJ_TASK_HOME : 0u);
         tasks[t] = k;
-        pred[t] = (float)((double)ev * mult);
+        pred[t] = (float)pairs_of(g, r, evH, evO, diag);
     }
 }
 
@@ -502,22 +539,37 @@ __global__ void __launch_bounds__(256) k_plan_stats(const uint32_t *__restrict__
 }
 
 // ------------------------------------------------------------ estimates --
-// Learned estimator: per-cell hits per evaluation from the network's
-// log2(1 + hits) output and the cell's full-stencil evaluations.
-__global__ void __launch_bounds__(256) k_rates_mlp(const float *__restrict__ out, const unsigned long long *candFull,
-                                                   uint32_t nCells, float *__restrict__ rate)
+// Learned estimator: per-cell hits per evaluation from the network's two
+// outputs, log2(1 + hits of the cell's points among its own points) and
+// log2(1 + hits among its owned neighbours' points): divided by the cell's
+// occupancy squared and by its occupancy times the owned neighbours' total.
+__global__ void __launch_bounds__(256) k_rates_mlp(const float *__restrict__ out, const uint32_t *__restrict__ cellStart,
+                                                   const uint32_t *__restrict__ nbrStart,
+                                                   const uint32_t *__restrict__ nbrCell, uint32_t nCells,
+                                                   float *__restrict__ rate)
 {
     const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= nCells) return;
-    const double hits = exp2((double)out[(uint64_t)c * SJ_NOUT + 1]) - 1.0;
-    const double calcs = (double)candFull[c];
-    const double r = calcs > 0 ? hits / calcs : 0.0;
-    rate[c] = (float)fmin(1.0, fmax(r, 0.0));
+    const double occ = (double)(cellStart[c + 1] - cellStart[c]);
+    double nbr = 0.0;
+    for (uint32_t i = nbrStart[c]; i < nbrStart[c + 1]; i++) {
+        const uint32_t b = nbrCell[i];
+        nbr += (double)(cellStart[b + 1] - cellStart[b]);
+    }
+    const double hHome = exp2((double)out[(uint64_t)c * SJ_NOUT]) - 1.0;
+    const double hNbr = exp2((double)out[(uint64_t)c * SJ_NOUT + 1]) - 1.0;
+    const double rH = occ > 0 ? hHome / (occ * occ) : 0.0;
+    const double rN = occ > 0 && nbr > 0 ? hNbr / (occ * nbr) : 0.0;
+    rate[2 * c] = (float)fmin(1.0, fmax(rH, 0.0));
+    rate[2 * c + 1] = (float)fmin(1.0, fmax(rN, 0.0));
 }
 
-// Sampling estimator: hits and evaluations of the sampled queries, per cell,
-// per occupancy class of the cell (floor(log2(occupancy)), 32 classes) and in
-// total.  totals: [0] hits, [1] evaluations, [2 + 2b] / [3 + 2b] class b's.
+// Sampling estimator: hits and evaluations of the sampled queries, per cell
+// and segment kind (its own points, its neighbours'), per occupancy class of
+// the cell (floor(log2(occupancy)), 32 classes) and in total.  A sampling task
+// is a home task when it covers home-segment positions only (they are chunked
+// apart).  totals: [4 * b + 2 * kind + 0/1] class b's hits / evaluations,
+// [128 + 2 * kind + 0/1] the totals.
 constexpr int SAMPLE_BINS = 32;
 
 __device__ __forceinline__ uint32_t occ_bin(const uint32_t *__restrict__ cellStart, uint32_t c)
@@ -536,23 +588,26 @@ __global__ void __launch_bounds__(256) k_sample_sums(const sj_task *__restrict__
 {
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= nt) return;
-    const uint32_t c = tasks[t].cell;
+    const sj_task k = tasks[t];
+    const uint32_t c = k.cell;
+    const uint32_t occ = cellStart[c + 1] - cellStart[c];
+    const uint32_t kind = (k.segBase == 0 && k.sEnd <= occ) ? 0u : 1u;
     const uint32_t h = taskHits[t], e = taskEvals[t];
     const uint32_t b = occ_bin(cellStart, c);
     if (h) {
-        atomicAdd(&cellHits[c], (unsigned long long)h);
-        atomicAdd(&totals[0], (unsigned long long)h);
-        atomicAdd(&totals[2 + 2 * b], (unsigned long long)h);
+        atomicAdd(&cellHits[2 * c + kind], (unsigned long long)h);
+        atomicAdd(&totals[4 * b + 2 * kind], (unsigned long long)h);
+        atomicAdd(&totals[4 * SAMPLE_BINS + 2 * kind], (unsigned long long)h);
     }
     if (e) {
-        atomicAdd(&cellEvals[c], (unsigned long long)e);
-        atomicAdd(&totals[1], (unsigned long long)e);
-        atomicAdd(&totals[3 + 2 * b], (unsigned long long)e);
+        atomicAdd(&cellEvals[2 * c + kind], (unsigned long long)e);
+        atomicAdd(&totals[4 * b + 2 * kind + 1], (unsigned long long)e);
+        atomicAdd(&totals[4 * SAMPLE_BINS + 2 * kind + 1], (unsigned long long)e);
     }
 }
 
-// A cell without a sampled query takes the rate of the sampled cells of its
-// occupancy class, or the global rate when that class has none.
+// A cell and segment kind without a sampled evaluation take the rate of the
+// sampled cells of the cell's occupancy class, or the global rate.
 __global__ void __launch_bounds__(256) k_sample_rates(const unsigned long long *__restrict__ cellHits,
                                                       const unsigned long long *__restrict__ cellEvals,
                                                       const unsigned long long *__restrict__ totals,
@@ -561,14 +616,18 @@ __global__ void __launch_bounds__(256) k_sample_rates(const unsigned long long *
 {
     const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= nCells) return;
-    if (cellEvals[c]) {
-        rate[c] = (float)((double)cellHits[c] / (double)cellEvals[c]);
-        return;
-    }
     const uint32_t b = occ_bin(cellStart, c);
-    const unsigned long long bh = totals[2 + 2 * b], be = totals[3 + 2 * b];
-    const double global = totals[1] ? (double)totals[0] / (double)totals[1] : 1.0;
-    rate[c] = (float)(be ? (double)bh / (double)be : global);
+    for (int kind = 0; kind < 2; kind++) {
+        float v;
+        if (cellEvals[2 * c + kind]) {
+            v = (float)((double)cellHits[2 * c + kind] / (double)cellEvals[2 * c + kind]);
+        } else {
+            const unsigned long long bh = totals[4 * b + 2 * kind], be = totals[4 * b + 2 * kind + 1];
+            const unsigned long long gh = totals[4 * SAMPLE_BINS + 2 * kind], ge = totals[4 * SAMPLE_BINS + 2 * kind + 1];
+            v = (float)(be ? (double)bh / (double)be : (ge ? (double)gh / (double)ge : 1.0));
+        }
+        rate[2 * c + kind] = v;
+    }
 }
 
 // ------------------------------------------------------------ statistics --
@@ -814,23 +873,23 @@ cudaError_t sj_plan_stats(const uint32_t *start, uint32_t nb, unsigned long long
     return cudaGetLastError();
 }
 
-cudaError_t sj_rates_mlp(const float *out, const unsigned long long *candFull, uint32_t nCells, float *rate,
-                         cudaStream_t s)
+cudaError_t sj_rates_mlp(const float *out, const uint32_t *cellStart, const uint32_t *nbrStart,
+                         const uint32_t *nbrCell, uint32_t nCells, float *rate, cudaStream_t s)
 {
     if (nCells == 0) return cudaSuccess;
-    k_rates_mlp<<<blocks_for(nCells, 256), 256, 0, s>>>(out, candFull, nCells, rate);
+    k_rates_mlp<<<blocks_for(nCells, 256), 256, 0, s>>>(out, cellStart, nbrStart, nbrCell, nCells, rate);
     sj_note_launch();
     return cudaGetLastError();
 }
 
-size_t sj_sample_totals_len() { return 2 + 2 * SAMPLE_BINS; }
+size_t sj_sample_totals_len() { return 4 * SAMPLE_BINS + 4; }
 
 cudaError_t sj_sample_rates(const sj_task *tasks, uint32_t nt, const uint32_t *taskHits, const uint32_t *taskEvals,
                             const uint32_t *cellStart, unsigned long long *cellHits, unsigned long long *cellEvals,
                             unsigned long long *totals, uint32_t nCells, float *rate, cudaStream_t s)
 {
-    cudaError_t e = cudaMemsetAsync(cellHits, 0, sizeof(unsigned long long) * nCells, s);
-    if (e == cudaSuccess) e = cudaMemsetAsync(cellEvals, 0, sizeof(unsigned long long) * nCells, s);
+    cudaError_t e = cudaMemsetAsync(cellHits, 0, sizeof(unsigned long long) * 2 * nCells, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(cellEvals, 0, sizeof(unsigned long long) * 2 * nCells, s);
     if (e == cudaSuccess) e = cudaMemsetAsync(totals, 0, sizeof(unsigned long long) * sj_sample_totals_len(), s);
     if (e != cudaSuccess) return e;
     if (nt) {

@@ -30,7 +30,7 @@ EXPORTS = [
     "sj_params_default", "sj_create", "sj_destroy", "sj_import_csv", "sj_read_csv", "sj_set_points", "sj_build_index",
     "sj_index_sizes", "sj_index_export", "sj_join", "sj_degrees", "sj_neighbor_table", "sj_neighbor_csr", "sj_free",
     "sj_get_stats", "sj_get_stream", "sj_mlp_num_params", "sj_set_estimator_weights", "sj_load_estimator",
-    "sj_cell_features", "sj_mlp_train", "sj_mlp_loss_grad", "sj_mlp_forward", "sj_mlp_loss_grad_noalloc",
+    "sj_cell_features", "sj_cell_samples", "sj_mlp_train", "sj_mlp_loss_grad", "sj_mlp_forward", "sj_mlp_loss_grad_noalloc",
     "sj_status_string",
     "sj_last_error", "sj_version", "sj_kernel_launch_count",
 ]
@@ -124,6 +124,7 @@ def load() -> C.CDLL:
     L.sj_set_estimator_weights.argtypes = [vp, vp, u32]
     L.sj_load_estimator.argtypes = [vp, C.c_char_p]
     L.sj_cell_features.argtypes = [vp, vp, vp, vp]
+    L.sj_cell_samples.argtypes = [vp, vp, vp, vp, vp]
     L.sj_mlp_train.argtypes = [vp, vp, u32, vp, i32, C.c_float, u32, u64, C.POINTER(C.c_float), i32]
     L.sj_mlp_loss_grad.argtypes = [vp, vp, u32, vp, C.POINTER(C.c_float), vp, i32]
     L.sj_mlp_forward.argtypes = [vp, u32, vp, vp, i32]
@@ -357,6 +358,12 @@ class SelfJoin:
     def load_estimator(self, path: str):
         _check(load().sj_load_estimator(self._h, path.encode()))
 
+    def cell_samples(self):
+        """(home hits, home evaluations, owned-neighbour hits, owned-neighbour
+        evaluations) per cell from the sampling estimator (exact with
+        sample_rate=1)."""
+        return _cell_samples(self)
+
     def cell_features(self, with_hits: bool = True):
         nne = int(self.stats().n_nonempty_cells)
         f = np.zeros((nne, 16), np.float32)
@@ -364,6 +371,13 @@ class SelfJoin:
         c = np.zeros(nne, np.float64)
         _check(load().sj_cell_features(self._h, _ptr(f), _ptr(h) if with_hits else None, _ptr(c)))
         return f, (h if with_hits else None), c
+
+
+def _cell_samples(sj: "SelfJoin"):
+    nne = int(sj.stats().n_nonempty_cells)
+    out = [np.zeros(nne, np.float64) for _ in range(4)]
+    _check(load().sj_cell_samples(sj._h, *[_ptr(a) for a in out]))
+    return tuple(out)
 
 
 def mlp_loss_grad(x: np.ndarray, y: np.ndarray, w: np.ndarray, device: int = 0):

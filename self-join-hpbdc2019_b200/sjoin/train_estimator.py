@@ -3,12 +3,16 @@
 Data: seeded runs of the 6-D exponential(40) generator (the c4 workload's
 distribution) with eps drawn uniformly from [0.01, 0.05] and the point count
 drawn log-uniformly up to 1e7, the c4 workload's size.  For each run the
-engine builds its index, computes every cell's 16 features and full-stencil
-distance-calculation count, and measures every point's neighbour count with
-its count pass (sj_degrees); a cell's target is (log2(1+calcs), log2(1+hits)).
-The point count of a run is shrunk until the run's full-stencil work stays
-under a budget (by default a little above the c4 workload's 4.06e13), so the
-heaviest runs reach the cell sizes of that workload.
+engine builds its index and computes every cell's 16 features; its count
+pass then measures, with the sampling estimator at sample rate 1 (every
+point, sj_cell_samples), each cell's hits among its own points and among its
+owned neighbours' points under the linear-ID Unicomp traversal (search mode
+10).  A cell's targets are (log2(1 + home hits), log2(1 + neighbour hits)):
+the engine divides them by the cell's exactly known evaluation counts to get
+the two hit rates that predict every task's pairs.  The point count of a run
+is shrunk until the run's full-stencil work stays under a budget (by default
+a little above the c4 workload's 4.06e13), so the heaviest runs reach the
+cell sizes of that workload.
 
 Training: the 16 -> 64 -> 64 -> 2 MLP is trained with the engine's own FP32
 forward / backward / Adam kernels (sj_mlp_train).  The batch planner sums the
@@ -32,26 +36,29 @@ import time
 
 import numpy as np
 
-from . import PREC_FP32_REFINE, SelfJoin, datasets, mlp_init, mlp_loss_grad, mlp_train
+from . import PREC_FP32_REFINE, SCHED_SAMPLING, SelfJoin, datasets, mlp_init, mlp_loss_grad, mlp_train
 
 PKG = os.path.dirname(os.path.abspath(__file__))
 DEFAULT_OUT = os.path.join(PKG, "estimator_c4.bin")
 
 
 def cell_table(pts: np.ndarray, eps: float, k: int, with_hits: bool = True):
-    """(features, calcs, hits) of every non-empty cell, measured by the engine."""
+    """(features, full-stencil calcs, targets or None) of every non-empty cell, measured by the engine."""
     D = pts.shape[1]
-    with SelfJoin(D, eps, indexed_dims=k, mode=10, precision=PREC_FP32_REFINE) as sj:
+    with SelfJoin(D, eps, indexed_dims=k, mode=10, precision=PREC_FP32_REFINE, scheduler=SCHED_SAMPLING,
+                  sample_rate=1.0) as sj:
         sj.set_points(pts)
         sj.build_index()
+        feat, _, calcs = sj.cell_features(with_hits=False)
+        y = None
         if with_hits:
-            sj.degrees()
-        feat, hits, calcs = sj.cell_features(with_hits=with_hits)
-    return feat, calcs, hits
+            home, _, nbr, _ = sj.cell_samples()
+            y = targets(home, nbr)
+    return feat, calcs, y
 
 
-def targets(calcs: np.ndarray, hits: np.ndarray) -> np.ndarray:
-    return np.stack([np.log2(1.0 + calcs), np.log2(1.0 + hits)], 1).astype(np.float32)
+def targets(home_hits: np.ndarray, nbr_hits: np.ndarray) -> np.ndarray:
+    return np.stack([np.log2(1.0 + home_hits), np.log2(1.0 + nbr_hits)], 1).astype(np.float32)
 
 
 def collect(runs: int = 50, seed0: int = 7000, n_max: int = 10_000_000, n_min: int = 50_000,
@@ -70,18 +77,18 @@ def collect(runs: int = 50, seed0: int = 7000, n_max: int = 10_000_000, n_min: i
                 break
             n = max(n_min, int(n * math.sqrt(work_budget / work) * 0.9))
         t0 = time.time()
-        feat, calcs, hits = cell_table(pts, eps, D, with_hits=True)
+        feat, calcs, y = cell_table(pts, eps, D, with_hits=True)
         xs.append(feat)
-        ys.append(targets(calcs, hits))
+        ys.append(y)
         meta.append(dict(run=r, seed=seed, n=n, eps=eps, cells=len(feat), calcs=float(calcs.sum()),
-                         hits=float(hits.sum()), s=round(time.time() - t0, 2)))
+                         hits=float((np.exp2(y.astype(np.float64)) - 1.0).sum()), s=round(time.time() - t0, 2)))
         log(json.dumps(meta[-1]))
     return np.concatenate(xs), np.concatenate(ys), meta
 
 
 def resample(x: np.ndarray, y: np.ndarray, size: int = 4_000_000, beta: float = 0.5, seed: int = 1):
-    """Training set drawn with probability proportional to (1 + hits)^beta."""
-    hits = np.exp2(y[:, 1].astype(np.float64)) - 1.0
+    """Training set drawn with probability proportional to (1 + hits)^beta (home + neighbour hits)."""
+    hits = (np.exp2(y.astype(np.float64)) - 1.0).sum(1)
     p = np.power(1.0 + hits, beta)
     p /= p.sum()
     idx = np.random.default_rng(seed).choice(len(x), size=min(size, 4 * len(x)), replace=True, p=p)
