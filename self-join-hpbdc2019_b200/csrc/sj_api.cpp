@@ -525,12 +525,26 @@ struct BatchRange {
     uint64_t exact;   // a re-planned part: its measured pairs (0 for a planned batch)
 };
 
-sj_status run_count(Ctx &c, sj_join_args &a, bool queue, cudaStream_t st = nullptr)
+sj_status run_count(Ctx &c, sj_join_args &a, bool queue, cudaStream_t st = nullptr, int maxCtasPerSM = 0)
 {
     if (!st) st = c.s;
     if (queue) CK(cudaMemsetAsync(c.queueHead.p, 0, sizeof(uint32_t), st));
-    CK(sj_launch_join(a, c.g, c.p.precision == SJ_PREC_FP32_REFINE ? 1 : 0, queue ? 1 : 0, c.numSM, st));
+    CK(sj_launch_join(a, c.g, c.p.precision == SJ_PREC_FP32_REFINE ? 1 : 0, queue ? 1 : 0, c.numSM, maxCtasPerSM,
+                      st));
     return SJ_OK;
+}
+
+// Resident CTAs per SM of the count pass and the emission when they run side by
+// side on two streams (0: as many as fit).  Kernels that each fill every SM
+// would only take turns; smaller grids let both be resident at once, so the
+// emission's memory-latency-bound warps use the issue slots the count pass
+// leaves.  SJ_JOIN_CTAS / SJ_EMIT_CTAS override them.
+void pipe_ctas(int &join, int &emit)
+{
+    join = 0;
+    emit = 0;
+    if (const char *e = getenv("SJ_JOIN_CTAS")) join = atoi(e);
+    if (const char *e = getenv("SJ_EMIT_CTAS")) emit = atoi(e);
 }
 
 // Hit-mask words (row or column) one batch may record (4 bytes each); a batch
@@ -1009,8 +1023,9 @@ sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
         // count pass and scan run beside batch i's emission (and the launch
         // tails of each stage fill with the other's work).  Batches alternate
         // between two sets of count-pass records and two sets of key offsets
-        // and scan totals; batch i's count pass waits for batch i - 2's
-        // emission, the last reader of the set it reuses.
+        // and scan totals; batch i's count pass waits for batch i - 2's fold,
+        // the last reader of the set it reuses (the emission reads the
+        // records, the fold the key offsets and the scan total).
         // SJ_SERIAL=1 keeps every stage on the engine's stream (a diagnostic
         // knob: the per-stage CUDA-event times are then those of each stage alone)
         const char *serialEnv = getenv("SJ_SERIAL");
@@ -1037,6 +1052,8 @@ sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
             }
         }
         cudaStream_t sA = c.s, sB = pipe ? c.cs : c.s;
+        int joinCtas, emitCtas;
+        pipe_ctas(joinCtas, emitCtas);
         // the second stream's work is waited for on every way out
         struct Drain {
             cudaStream_t s;
@@ -1069,9 +1086,9 @@ sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
                 b.candRel = c.candRel2.p;
                 b.keyStart = c.keyStart2.p;
             }
-            if (pipe && i > 1) CK(cudaStreamWaitEvent(sA, ev[EV * (i - 2) + 6], 0));   // set reused: emission i-2 done
+            if (pipe && i > 1) CK(cudaStreamWaitEvent(sA, ev[EV * (i - 2) + 7], 0));   // set reused: fold i-2 done
             CK(cudaEventRecord(e[0], sA));
-            CKS(run_count(c, b, queue, sA));
+            CKS(run_count(c, b, queue, sA, pipe ? joinCtas : 0));
             CK(cudaEventRecord(e[1], sA));
             CK(cudaEventRecord(e[2], sA));
             CK(sj_exclusive_scan_u32_clear(c.keyCount.p, const_cast<uint32_t *>(b.keyStart), n, c.scanTemp.p, scanTot,
@@ -1084,7 +1101,7 @@ sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
             CK(cudaEventRecord(e[5], sB));
             b.queueHead = pipe ? c.emitHead.p : c.queueHead.p;
             CK(cudaMemsetAsync(b.queueHead, 0, sizeof(uint32_t), sB));
-            CK(sj_launch_emit(b, c.numSM, sB));
+            CK(sj_launch_emit(b, c.numSM, pipe ? emitCtas : 0, sB));
             CK(cudaEventRecord(e[6], sB));
             CK(sj_fold(b.keyStart, scanTot, n, c.outVal.p, c.outKey.p, b.batchPairs, bufCap, c.foldChunkKey.p,
                        c.stat.p + 4, c.numSM, sB));
@@ -1228,7 +1245,7 @@ sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
         // this set's values must have been copied out before the emission rewrites them
         if (setUsed[sel]) CK(cudaStreamWaitEvent(c.s, c.evVals[sel], 0));
         CK(cudaMemsetAsync(c.queueHead.p, 0, sizeof(uint32_t), c.s));
-        CK(sj_launch_emit(a, c.numSM, c.s));
+        CK(sj_launch_emit(a, c.numSM, 0, c.s));
         CK(cudaEventRecord(ev(4), c.s));
         CK(sj_hash_pairs(c.outKey.p, valBuf, cnt, c.stat.p + 4, c.s));
         if (delivery == SJ_DELIVER_CSR) {

@@ -115,6 +115,38 @@ __device__ __forceinline__ void decode_bits(uint32_t m, uint32_t n, uint32_t tag
     if (n) p[-1] = (uint16_t)(tag | top_bit(m));
 }
 
+// decode_bits for two words at once (two independent chains of bit scans):
+// word a's n_a entries go to buf[ka ..), word b's to buf[kb ..).
+__device__ __forceinline__ void decode_bits2(uint32_t ma, uint32_t na, uint32_t tagA, uint32_t ka, uint32_t mb,
+                                             uint32_t nb, uint32_t tagB, uint32_t kb, uint16_t *buf)
+{
+    uint16_t *pa = buf + ka + na, *pb = buf + kb + nb;
+    while (na >= 2 || nb >= 2) {
+        if (na >= 2) {
+            const uint32_t b0 = top_bit(ma);
+            ma ^= 1u << b0;
+            const uint32_t b1 = top_bit(ma);
+            ma ^= 1u << b1;
+            pa[-1] = (uint16_t)(tagA | b0);
+            pa[-2] = (uint16_t)(tagA | b1);
+            pa -= 2;
+            na -= 2;
+        }
+        if (nb >= 2) {
+            const uint32_t b0 = top_bit(mb);
+            mb ^= 1u << b0;
+            const uint32_t b1 = top_bit(mb);
+            mb ^= 1u << b1;
+            pb[-1] = (uint16_t)(tagB | b0);
+            pb[-2] = (uint16_t)(tagB | b1);
+            pb -= 2;
+            nb -= 2;
+        }
+    }
+    if (na) pa[-1] = (uint16_t)(tagA | top_bit(ma));
+    if (nb) pb[-1] = (uint16_t)(tagB | top_bit(mb));
+}
+
 // Stores one value.  FITS: the caller has shown that every slot of the window
 // is below the capacity; otherwise each slot is checked.
 template <bool FITS>
@@ -251,8 +283,7 @@ __device__ __forceinline__ void emit_rows(const sj_join_args &a, const UnitTask 
             // a query's first word: base = its chunk start slot minus its flat prefix
             if (fa < nw && ra == 0) w.base[qa] = w.start[qa] - (carry + exA);
             if (fb < nw && rb == 0) w.base[qb] = w.start[qb] - (carry + exB);
-            decode_bits(wa, ca, (qa << 11) | (ra << 5), w.ent, exA);
-            decode_bits(wb, cbt, (qb << 11) | (rb << 5), w.ent, exB);
+            decode_bits2(wa, ca, (qa << 11) | (ra << 5), exA, wb, cbt, (qb << 11) | (rb << 5), exB, w.ent);
             __syncwarp();
             // copy-out.  Every entry is valid by construction (words of queries
             // < nq, bits inside the stream).
@@ -408,10 +439,12 @@ int emit_occupancy()
 
 }  // namespace
 
-cudaError_t sj_launch_emit(const sj_join_args &a, int numSM, cudaStream_t s)
+cudaError_t sj_launch_emit(const sj_join_args &a, int numSM, int maxCtasPerSM, cudaStream_t s)
 {
     if (a.taskEnd == a.taskBegin) return cudaSuccess;
-    k_emit<<<(unsigned)(numSM * emit_occupancy()), EW, 0, s>>>(a);
+    int perSM = emit_occupancy();
+    if (maxCtasPerSM > 0 && maxCtasPerSM < perSM) perSM = maxCtasPerSM;
+    k_emit<<<(unsigned)(numSM * perSM), EW, 0, s>>>(a);
     sj_note_launch();
     return cudaGetLastError();
 }

@@ -199,11 +199,12 @@ cudaError_t sj_launch_neighbours(const uint64_t *cellLid, const uint32_t *cellCo
                                  float *feat, int pass, cudaStream_t s);
 
 // join (sj_join.cu): the count pass (per-key pair counts, hit masks)
+// (persistent queue: numSM x resident CTAs per SM, at most maxCtasPerSM when > 0)
 cudaError_t sj_launch_join(const sj_join_args &a, const sj_grid_dev &g, int fp32, int queue, int numSM,
-                           cudaStream_t s);
+                           int maxCtasPerSM, cudaStream_t s);
 // emission (sj_emit.cu): the values of the pairs from the recorded hit masks
 // into their key runs; a.queueHead must be zero at launch
-cudaError_t sj_launch_emit(const sj_join_args &a, int numSM, cudaStream_t s);
+cudaError_t sj_launch_emit(const sj_join_args &a, int numSM, int maxCtasPerSM, cudaStream_t s);
 
 // emission units of a task: one per group of 32 queries, plus one per block of
 // 32 stream positions for a symmetric task

@@ -579,12 +579,16 @@ int occupancy_of()
 }
 
 template <int DP, bool F32>
-cudaError_t launch_one(const sj_join_args &a, const sj_grid_dev &g, int queue, int numSM, cudaStream_t s)
+cudaError_t launch_one(const sj_join_args &a, const sj_grid_dev &g, int queue, int numSM, int maxCtasPerSM,
+                       cudaStream_t s)
 {
     const uint32_t nt = a.taskEnd - a.taskBegin;
     if (nt == 0) return cudaSuccess;
-    // persistent queue: one full wave of resident CTAs
-    unsigned grid = queue ? (unsigned)(numSM * occupancy_of<DP, F32>()) : nt;
+    // persistent queue: one full wave of resident CTAs (or fewer per SM, to
+    // leave room for a kernel of the other stream)
+    int perSM = occupancy_of<DP, F32>();
+    if (maxCtasPerSM > 0 && maxCtasPerSM < perSM) perSM = maxCtasPerSM;
+    unsigned grid = queue ? (unsigned)(numSM * perSM) : nt;
     if (queue && grid > nt) grid = nt;
     k_join<DP, F32, sj_query_slots(DP, F32)><<<grid, SJ_CTA, 0, s>>>(a, g, queue);
     sj_note_launch();
@@ -592,25 +596,27 @@ cudaError_t launch_one(const sj_join_args &a, const sj_grid_dev &g, int queue, i
 }
 
 template <int DP>
-cudaError_t launch_dp(const sj_join_args &a, const sj_grid_dev &g, int fp32, int queue, int numSM, cudaStream_t s)
+cudaError_t launch_dp(const sj_join_args &a, const sj_grid_dev &g, int fp32, int queue, int numSM, int maxCtas,
+                      cudaStream_t s)
 {
-    return fp32 ? launch_one<DP, true>(a, g, queue, numSM, s) : launch_one<DP, false>(a, g, queue, numSM, s);
+    return fp32 ? launch_one<DP, true>(a, g, queue, numSM, maxCtas, s)
+                : launch_one<DP, false>(a, g, queue, numSM, maxCtas, s);
 }
 
 }  // namespace
 
 cudaError_t sj_launch_join(const sj_join_args &a, const sj_grid_dev &g, int fp32, int queue, int numSM,
-                           cudaStream_t s)
+                           int maxCtasPerSM, cudaStream_t s)
 {
     switch (g.Dp) {
-    case 1: return launch_dp<1>(a, g, fp32, queue, numSM, s);
-    case 2: return launch_dp<2>(a, g, fp32, queue, numSM, s);
-    case 3: return launch_dp<3>(a, g, fp32, queue, numSM, s);
-    case 4: return launch_dp<4>(a, g, fp32, queue, numSM, s);
-    case 6: return launch_dp<6>(a, g, fp32, queue, numSM, s);
-    case 8: return launch_dp<8>(a, g, fp32, queue, numSM, s);
-    case 12: return launch_dp<12>(a, g, fp32, queue, numSM, s);
-    case 16: return launch_dp<16>(a, g, fp32, queue, numSM, s);
+    case 1: return launch_dp<1>(a, g, fp32, queue, numSM, maxCtasPerSM, s);
+    case 2: return launch_dp<2>(a, g, fp32, queue, numSM, maxCtasPerSM, s);
+    case 3: return launch_dp<3>(a, g, fp32, queue, numSM, maxCtasPerSM, s);
+    case 4: return launch_dp<4>(a, g, fp32, queue, numSM, maxCtasPerSM, s);
+    case 6: return launch_dp<6>(a, g, fp32, queue, numSM, maxCtasPerSM, s);
+    case 8: return launch_dp<8>(a, g, fp32, queue, numSM, maxCtasPerSM, s);
+    case 12: return launch_dp<12>(a, g, fp32, queue, numSM, maxCtasPerSM, s);
+    case 16: return launch_dp<16>(a, g, fp32, queue, numSM, maxCtasPerSM, s);
     }
     return cudaErrorInvalidValue;
 }

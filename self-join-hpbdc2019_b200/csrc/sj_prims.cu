@@ -442,9 +442,28 @@ __global__ void __launch_bounds__(256) k_fold(const uint32_t *__restrict__ excl,
                     }
                 }
                 if (__all_sync(0xffffffffu, unres == 0)) break;
-                // some slot lies past all 32 runs of the window: the next 32 runs
-                // (every unresolved slot is at or after their first start)
-                k += 32;
+                // some slot lies past all 32 runs of the window.  Runs of the keys
+                // in between can be empty over long stretches (keys are point
+                // ids), so the window jumps to the key of the smallest unresolved
+                // slot: a 32-ary search over the run starts (each step one load
+                // per lane).  Invariant: excl[lo] <= smin, and hi == n or
+                // excl[hi] > smin.
+                uint32_t smin = 0xffffffffu;
+#pragma unroll
+                for (int i = 0; i < 4; i++)
+                    if ((unres >> i) & 1u) smin = min(smin, p + (uint32_t)i);
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) smin = min(smin, __shfl_xor_sync(0xffffffffu, smin, o));
+                uint64_t lo = k + 32, hi = n;   // excl[k + 32] = the window's last end <= smin
+                while (hi - lo > 1) {
+                    const uint64_t step = (hi - lo + 31) / 32;
+                    const uint64_t probe = lo + (uint64_t)(lane + 1) * step;
+                    const bool ok = probe < hi && excl[probe] <= smin;
+                    const uint32_t cntOk = __popc(__ballot_sync(0xffffffffu, ok));   // a prefix of the lanes
+                    lo += (uint64_t)cntOk * step;
+                    hi = min(hi, lo + step);
+                }
+                k = lo;
                 R = runEnd(k + lane);
             }
             if (cnt == 4) {
