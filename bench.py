@@ -256,6 +256,9 @@ def _config(args, spec, prec, learned):
         "scheduler": "learned" if learned else "sampling",
         "l2": "flushed between steps (256 MiB write); outputs far exceed L2",
         "parallelism": (f"task shards x{_dist()[0]}" if getattr(args, "shard", False) else f"replicas x{_dist()[0]}"),
+        **({"task_sample": f"task shard 0 of {args.task_sample} (every {args.task_sample}th task of the cost "
+                           f"order; a reduced case for profiler captures)"}
+           if getattr(args, "task_sample", 1) > 1 else {}),
     }
 
 
@@ -360,7 +363,8 @@ def run_ours(args):
         sj = sjoin.SelfJoin(spec["D"], eps, indexed_dims=k, mode=spec["mode"], precision=precision,
                             scheduler=sjoin.SCHED_LEARNED if use_learned else sjoin.SCHED_SAMPLING,
                             capacity=spec["capacity"], device=local,
-                            shard_index=rank if args.shard else 0, shard_count=ws if args.shard else 1)
+                            shard_index=rank if args.shard else 0,
+                            shard_count=ws if args.shard else max(1, args.task_sample))
         if use_learned:
             sj.load_estimator(args.weights)
         sj.set_points(host.numpy())
@@ -397,6 +401,21 @@ def run_ours(args):
     job_ms, job_pairs, job_hash = ms, pairs, stats[-1]["pair_hash"]
     if ws > 1:
         job_ms, job_pairs, job_hash = combine_ranks(ms, pairs, job_hash, "cuda")
+
+    # stage probe: one more step with every stage on one stream (the engine's
+    # SJ_SERIAL knob), so each kernel's CUDA-event time is its own, not shared
+    # with the other stream's kernels; the rooflines use these times
+    probe = None
+    if not args.no_stage_probe:
+        prior = os.environ.get("SJ_SERIAL")
+        os.environ["SJ_SERIAL"] = "1"
+        try:
+            probe = step().as_dict()
+        finally:
+            if prior is None:
+                del os.environ["SJ_SERIAL"]
+            else:
+                os.environ["SJ_SERIAL"] = prior
 
     # end to end through the C ABI with host buffers: pinned H2D of the points,
     # index, join, and every batch's pairs delivered into pinned host memory
@@ -455,10 +474,13 @@ def run_ours(args):
         return
     peak, peak_kind = _peaks()
     s = stats[-1]
-    nb = max(1, s["num_batches"])
-    emit_ms = s["ms_fill_kernel"]
+    ps = probe or s   # per-kernel times: the stage probe's when it ran
+    nb = max(1, ps["num_batches"])
+    emit_ms = ps["ms_fill_kernel"]
     achieved = (4 * pairs) / (emit_ms / 1e3) / 1e9 if emit_ms > 0 else None
     traffic = EMIT_TRAFFIC_BYTES_PER_PAIR * pairs / nb if EMIT_TRAFFIC_BYTES_PER_PAIR else None
+    fold_ms = ps["ms_deliver"]
+    fold_gbs = (8 * pairs) / (fold_ms / 1e3) / 1e9 if fold_ms > 0 else None
     cpu = None
     if not args.no_cpu and ws == 1:   # the CPU baseline is rank 0's at N = 1 only
         rate, cores, sample, _ = cpu_oracle_rate(pts, eps, k, target_s=args.cpu_seconds)
@@ -478,9 +500,17 @@ def run_ours(args):
                      "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": (achieved / peak) if achieved else None, "peak_kind": peak_kind,
                      "algorithmic_bytes_per_launch": 4 * pairs / nb, "launches": nb, "traffic": traffic,
-                     "note": ("4 B of values written per pair; launch time from CUDA events on the emission's "
-                              "stream, which it shares with the next batch's count pass")},
-        "roofline_distance_loop": _pipe_roofline(s, prec, spec["D"], clocks),
+                     "note": ("4 B of values written per pair; launch times from CUDA events around each launch "
+                              "in the stage probe (every stage on one stream)" if probe else
+                              "4 B of values written per pair; launch times from CUDA events on the emission's "
+                              "stream, shared with the next batch's count pass")},
+        "roofline_fold": {"bound": "hbm", "kernel": "k_fold: values read back, keys written, set hash",
+                          "achieved": fold_gbs, "peak": peak, "unit": "GB/s",
+                          "frac": (fold_gbs / peak) if fold_gbs else None, "peak_kind": peak_kind,
+                          "algorithmic_bytes_per_launch": 8 * pairs / nb},
+        "roofline_distance_loop": _pipe_roofline(ps, prec, spec["D"], clocks),
+        "stage_probe_ms": ({k2: round(probe[k2], 3) for k2 in ("ms_count", "ms_scan", "ms_fill", "ms_deliver",
+                                                               "ms_total")} if probe else None),
         "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clocks,
         "host_threads_per_rank": rank_host_threads(),
         "phases_ms": {k2: round(s[k2], 3) for k2 in ("ms_index", "ms_tasks", "ms_estimate", "ms_count", "ms_scan",
@@ -538,6 +568,9 @@ def main():
     ap.add_argument("--shard", action="store_true",
                     help="N > 1: split one join over the ranks (strong scaling) instead of N replicas")
     ap.add_argument("--capacity", type=int, default=None, help="batch capacity in pairs (default: the workload's)")
+    ap.add_argument("--task-sample", type=int, default=1,
+                    help="K > 1: join only task shard 0 of K (every Kth task of the cost order), a reduced case "
+                         "with the full workload's cell density for profiler captures")
     ap.add_argument("--precision", type=int, default=None, help="0 FP64, 1 FP32 filter + FP64 refine")
     ap.add_argument("--mode", type=int, default=None, help="search mode (default: the workload's)")
     ap.add_argument("--scheduler", choices=["learned", "sampling"], default=None,
@@ -550,6 +583,8 @@ def main():
                     help="timed steps: on-device fold of every batch (none) or every batch handed to a "
                          "device-memory consumer one at a time (device)")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-stage-probe", action="store_true",
+                    help="skip the extra step whose stages run one after another (per-kernel times)")
     ap.add_argument("--no-ref-cuda", action="store_true",
                     help="skip the small workloads timed beside the reference's own CUDA pipeline")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)

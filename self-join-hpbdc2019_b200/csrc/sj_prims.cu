@@ -369,14 +369,24 @@ __global__ void __launch_bounds__(256) k_expand_long(int32_t *__restrict__ outKe
 // the same pass.  Key k owns slots [excl[k], excl[k+1]) (excl[n] = *total).
 // The slots are cut into chunks of FOLD_CHUNK; k_fold_chunk_keys records the
 // key at each chunk's first slot (one thread per key writes the chunks its run
-// starts), and in k_fold a warp takes a chunk, reads the values back from HBM
-// in 16-byte streaming loads, finds each slot's key among a window of 32 run
-// ends held one per lane (a 5-step shuffle search), stores the keys in 16-byte
-// streaming stores and adds splitmix64(key << 32 | value) to the set hash.
-// Every chunk is the same size, so the work is balanced whatever the run
-// lengths.  8 bytes per pair move, against 12 for a key expansion followed by
-// a fold that reads both arrays.  Skipped when the batch's count exceeds cap.
+// starts), and in k_fold a warp takes a chunk in rounds of 128 slots, lane L
+// holding slots 4L .. 4L+3 of the round.  The warp keeps a window of 32
+// consecutive keys, one per lane (its run start and end); each lane whose
+// non-empty run starts inside the round marks key + 1 at that slot in a
+// per-warp shared array, and an inclusive max-scan over the round (4 slots per
+// lane, then across the lanes, seeded with the key carried from the previous
+// round) gives every slot its key, since keys ascend with the slots.  When the
+// window's runs end inside the round, the window jumps to the key whose run
+// holds the first slot past it (a 32-ary search over the run starts, which
+// steps over stretches of empty runs: keys are point ids).  The values are
+// read back in 16-byte streaming loads, the keys stored in 16-byte streaming
+// stores, and splitmix64(key << 32 | value) is added to the set hash.  Every
+// chunk is the same size, so the work is balanced whatever the run lengths.
+// 8 bytes per pair move, against 12 for a key expansion followed by a fold
+// that reads both arrays.  Skipped when the batch's count exceeds cap.
 constexpr uint32_t FOLD_CHUNK = 4096;
+constexpr int FOLD_THREADS = 256;
+constexpr int FOLD_CTAS_PER_SM = 6;   // resident k_fold CTAs per SM (the register budget allows 6)
 
 __global__ void __launch_bounds__(256) k_fold_chunk_keys(const uint32_t *__restrict__ excl,
                                                          const uint32_t *__restrict__ total, uint64_t n,
@@ -392,96 +402,102 @@ __global__ void __launch_bounds__(256) k_fold_chunk_keys(const uint32_t *__restr
     for (uint32_t c = (st + FOLD_CHUNK - 1) / FOLD_CHUNK; (uint64_t)c * FOLD_CHUNK < en; c++) chunkKey[c] = (uint32_t)k;
 }
 
-__global__ void __launch_bounds__(256) k_fold(const uint32_t *__restrict__ excl, const uint32_t *__restrict__ total,
-                                              uint64_t n, const int32_t *__restrict__ val,
-                                              int32_t *__restrict__ outKey,
-                                              const unsigned long long *__restrict__ batchPairs, uint64_t cap,
-                                              const uint32_t *__restrict__ chunkKey,
-                                              unsigned long long *__restrict__ hashOut)
+__global__ void __launch_bounds__(FOLD_THREADS, FOLD_CTAS_PER_SM) k_fold(const uint32_t *__restrict__ excl,
+                                                       const uint32_t *__restrict__ total, uint64_t n,
+                                                       const int32_t *__restrict__ val, int32_t *__restrict__ outKey,
+                                                       const unsigned long long *__restrict__ batchPairs,
+                                                       uint64_t cap, const uint32_t *__restrict__ chunkKey,
+                                                       unsigned long long *__restrict__ hashOut)
 {
+    __shared__ __align__(16) uint32_t marks[FOLD_THREADS / 32][128];   // per warp: key + 1 at each run start
     if (*batchPairs > cap) return;
     const uint32_t lane = threadIdx.x & 31u;
+    uint32_t *const mk = marks[threadIdx.x >> 5];
     const uint32_t tot = *total;
     const uint32_t nChunks = (tot + FOLD_CHUNK - 1) / FOLD_CHUNK;
     const uint32_t warpsAll = (gridDim.x * blockDim.x) >> 5;
     unsigned long long h = 0;
-    // end of the run of key kk (the total past the last key)
+    *reinterpret_cast<uint4 *>(mk + 4 * lane) = make_uint4(0u, 0u, 0u, 0u);
+    // run start and end of key kk (both the total for kk >= n)
+    auto runStart = [&](uint64_t kk) -> uint32_t { return kk < n ? excl[kk] : tot; };
     auto runEnd = [&](uint64_t kk) -> uint32_t { return kk + 1 < n ? excl[kk + 1] : tot; };
     for (uint32_t c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; c < nChunks; c += warpsAll) {
         const uint32_t p0 = c * FOLD_CHUNK, p1 = min(p0 + FOLD_CHUNK, tot);
-        uint64_t k = chunkKey[c];
-        uint32_t R = runEnd(k + lane);   // lane j: end of the run of key k + j
+        uint64_t k = chunkKey[c];         // its run holds slot p0
+        uint32_t carry = (uint32_t)k;     // key of the round's slots before its first marked start
+        uint32_t S = runStart(k + lane), R = runEnd(k + lane);
         for (uint32_t base = p0; base < p1; base += 128) {
+            const uint32_t lim = min(base + 128u, p1);
             const uint32_t p = base + 4 * lane;
-            const uint32_t cnt = p < p1 ? min(4u, p1 - p) : 0u;   // this lane's slots: p .. p + cnt - 1
-            uint32_t v[4] = {0, 0, 0, 0};
+            const uint32_t cnt = p < lim ? min(4u, lim - p) : 0u;   // this lane's slots: p .. p + cnt - 1
+            int4 v = make_int4(0, 0, 0, 0);   // the values, loaded while the keys are found
             if (cnt == 4) {
-                const int4 x = __ldcs(reinterpret_cast<const int4 *>(val + p));
-                v[0] = (uint32_t)x.x; v[1] = (uint32_t)x.y; v[2] = (uint32_t)x.z; v[3] = (uint32_t)x.w;
+                v = __ldcs(reinterpret_cast<const int4 *>(val + p));
             } else {
-                for (uint32_t i = 0; i < cnt; i++) v[i] = (uint32_t)__ldcs(val + p + i);
+                if (cnt > 0) v.x = __ldcs(val + p);
+                if (cnt > 1) v.y = __ldcs(val + p + 1);
+                if (cnt > 2) v.z = __ldcs(val + p + 2);
             }
-            uint32_t key[4] = {0, 0, 0, 0};
-            uint32_t unres = (1u << cnt) - 1u;   // slots whose key is still unknown
+            __syncwarp();   // every lane has cleared its slots of the previous round
             for (;;) {
-                // slot s >= the window's first run start has key k + #{j : R_j <= s}
-                // while s is below the window's last run end R_31
+                if (R > S && S >= base && S < lim) mk[S - base] = (uint32_t)(k + lane) + 1u;
                 const uint32_t Rlast = __shfl_sync(0xffffffffu, R, 31);
-#pragma unroll
-                for (int i = 0; i < 4; i++) {
-                    const uint32_t sl = p + (uint32_t)i;
-                    uint32_t m = 0;
-#pragma unroll
-                    for (uint32_t b = 16; b > 0; b >>= 1) {
-                        const uint32_t r = __shfl_sync(0xffffffffu, R, m + b - 1);
-                        if (r <= sl) m += b;
-                    }
-                    if (((unres >> i) & 1u) && sl < Rlast) {
-                        key[i] = (uint32_t)(k + m);
-                        unres &= ~(1u << i);
-                    }
-                }
-                if (__all_sync(0xffffffffu, unres == 0)) break;
-                // some slot lies past all 32 runs of the window.  Runs of the keys
-                // in between can be empty over long stretches (keys are point
-                // ids), so the window jumps to the key of the smallest unresolved
-                // slot: a 32-ary search over the run starts (each step one load
-                // per lane).  Invariant: excl[lo] <= smin, and hi == n or
-                // excl[hi] > smin.
-                uint32_t smin = 0xffffffffu;
-#pragma unroll
-                for (int i = 0; i < 4; i++)
-                    if ((unres >> i) & 1u) smin = min(smin, p + (uint32_t)i);
-#pragma unroll
-                for (int o = 16; o > 0; o >>= 1) smin = min(smin, __shfl_xor_sync(0xffffffffu, smin, o));
-                uint64_t lo = k + 32, hi = n;   // excl[k + 32] = the window's last end <= smin
+                if (Rlast >= lim || k + 32 >= n) break;   // warp-uniform
+                // the window's runs end inside the round: jump to the largest
+                // key k' with excl[k'] <= Rlast (the keys in between have empty
+                // runs).  Invariant: excl[lo] <= Rlast, and hi == n or
+                // excl[hi] > Rlast.
+                uint64_t lo = k + 32, hi = n;
                 while (hi - lo > 1) {
                     const uint64_t step = (hi - lo + 31) / 32;
                     const uint64_t probe = lo + (uint64_t)(lane + 1) * step;
-                    const bool ok = probe < hi && excl[probe] <= smin;
+                    const bool ok = probe < hi && excl[probe] <= Rlast;
                     const uint32_t cntOk = __popc(__ballot_sync(0xffffffffu, ok));   // a prefix of the lanes
                     lo += (uint64_t)cntOk * step;
                     hi = min(hi, lo + step);
                 }
                 k = lo;
+                S = runStart(k + lane);
                 R = runEnd(k + lane);
             }
-            if (cnt == 4) {
-                __stcs(reinterpret_cast<int4 *>(outKey + p), make_int4((int)key[0], (int)key[1], (int)key[2], (int)key[3]));
-            } else {
-                for (uint32_t i = 0; i < cnt; i++) outKey[p + i] = (int32_t)key[i];
+            __syncwarp();
+            const uint4 m = *reinterpret_cast<const uint4 *>(mk + 4 * lane);
+            *reinterpret_cast<uint4 *>(mk + 4 * lane) = make_uint4(0u, 0u, 0u, 0u);
+            // keys ascend with the slots: each slot's key + 1 is the largest mark
+            // at or before it (or the carried key + 1)
+            const uint32_t m1 = max(m.x, m.y), m2 = max(m1, m.z), m3 = max(m2, m.w);
+            uint32_t x = m3;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+                if (lane >= (uint32_t)o) x = max(x, y);
             }
-            for (uint32_t i = 0; i < cnt; i++) h += splitmix64(((unsigned long long)key[i] << 32) | v[i]);
+            uint32_t pre = __shfl_up_sync(0xffffffffu, x, 1);
+            pre = max(lane ? pre : 0u, carry + 1u);
+            const uint32_t k0 = max(pre, m.x) - 1u, k1 = max(pre, m1) - 1u, k2 = max(pre, m2) - 1u,
+                           k3 = max(pre, m3) - 1u;
+            carry = __shfl_sync(0xffffffffu, k3, 31);
+            if (cnt == 4) {
+                __stcs(reinterpret_cast<int4 *>(outKey + p), make_int4((int)k0, (int)k1, (int)k2, (int)k3));
+            } else {
+                if (cnt > 0) outKey[p] = (int32_t)k0;
+                if (cnt > 1) outKey[p + 1] = (int32_t)k1;
+                if (cnt > 2) outKey[p + 2] = (int32_t)k2;
+            }
+            if (cnt > 0) h += splitmix64(((unsigned long long)k0 << 32) | (uint32_t)v.x);
+            if (cnt > 1) h += splitmix64(((unsigned long long)k1 << 32) | (uint32_t)v.y);
+            if (cnt > 2) h += splitmix64(((unsigned long long)k2 << 32) | (uint32_t)v.z);
+            if (cnt > 3) h += splitmix64(((unsigned long long)k3 << 32) | (uint32_t)v.w);
         }
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) h += __shfl_xor_sync(0xffffffffu, h, o);
-    __shared__ unsigned long long ws[8];
+    __shared__ unsigned long long ws[FOLD_THREADS / 32];
     if (lane == 0) ws[threadIdx.x >> 5] = h;
     __syncthreads();
     if (threadIdx.x == 0) {
         unsigned long long t = 0;
-        for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += ws[w];
+        for (int w = 0; w < FOLD_THREADS / 32; w++) t += ws[w];
         if (t) atomicAdd(hashOut, t);
     }
 }
@@ -552,7 +568,7 @@ cudaError_t sj_fold(const uint32_t *excl, const uint32_t *total, uint64_t n, con
     if (n == 0) return cudaSuccess;
     k_fold_chunk_keys<<<(unsigned)ceil_div(n, 256), 256, 0, s>>>(excl, total, n, batchPairs, cap, chunkKey);
     sj_note_launch();
-    k_fold<<<(unsigned)(numSM * 8), 256, 0, s>>>(excl, total, n, val, outKey, batchPairs, cap, chunkKey, hashOut);
+    k_fold<<<(unsigned)(numSM * FOLD_CTAS_PER_SM), FOLD_THREADS, 0, s>>>(excl, total, n, val, outKey, batchPairs, cap, chunkKey, hashOut);
     sj_note_launch();
     return cudaGetLastError();
 }
