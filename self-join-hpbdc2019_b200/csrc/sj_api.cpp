@@ -168,6 +168,51 @@ double eps_threshold(double eps)
     return t;
 }
 
+// Estimator feature weights: for two points uniform in two eps-wide cells whose
+// coordinates differ by one in m of k dimensions and agree in the others, the
+// probability that they lie within eps over those k dimensions.  Per dimension,
+// u = (difference / eps)^2 has CDF 2 sqrt(v) - v on [0, 1] for a shared cell
+// coordinate and v / 2 for adjacent ones; the sum of k such terms is below 1
+// with the mass that discretised convolutions (NB bins on [0, 1]) give.  Uniform
+// density makes these exact scale-free constants; the estimator learns how the
+// data's density departs from them.
+void offset_class_weights(int k, float *w)
+{
+    constexpr int NB = 1024;
+    static std::mutex mu;
+    static std::vector<float> cache[SJ_MAX_K + 1];
+    std::lock_guard<std::mutex> lock(mu);
+    if (k < 1 || k > SJ_MAX_K) return;
+    if (cache[k].empty()) {
+        std::vector<double> p0(NB), p1(NB);
+        for (int i = 0; i < NB; i++) {
+            const double a = (double)i / NB, b = (double)(i + 1) / NB;
+            p0[i] = (2.0 * std::sqrt(b) - b) - (2.0 * std::sqrt(a) - a);
+            p1[i] = (b - a) / 2.0;
+        }
+        auto conv = [](const std::vector<double> &x, const std::vector<double> &y) {
+            std::vector<double> z(NB, 0.0);
+            for (int i = 0; i < NB; i++) {
+                if (x[i] == 0.0) continue;
+                for (int j = 0; i + j < NB; j++) z[i + j] += x[i] * y[j];
+            }
+            return z;
+        };
+        std::vector<std::vector<double>> pow0(k + 1, std::vector<double>(NB, 0.0)), pow1 = pow0;
+        pow0[0][0] = pow1[0][0] = 1.0;   // the sum of no terms: mass 1 at 0
+        for (int j = 1; j <= k; j++) {
+            pow0[j] = conv(pow0[j - 1], p0);
+            pow1[j] = conv(pow1[j - 1], p1);
+        }
+        cache[k].resize(k + 1);
+        for (int m = 0; m <= k; m++) {
+            const std::vector<double> z = conv(pow1[m], pow0[k - m]);
+            cache[k][m] = (float)std::accumulate(z.begin(), z.end(), 0.0);
+        }
+    }
+    for (int m = 0; m <= k; m++) w[m] = cache[k][m];
+}
+
 struct Ctx {
     sj_params p{};
     int dev = 0, numSM = 148;
@@ -351,6 +396,7 @@ sj_status build_index(Ctx &c)
     g.k = k;
     g.eps = c.p.epsilon;
     g.thresh = eps_threshold(c.p.epsilon);
+    offset_class_weights(k, g.offW);
     for (int j = 0; j < D; j++) {
         c.dataMin[j] = hmm[2 * j];
         c.dataMax[j] = hmm[2 * j + 1];
@@ -1128,6 +1174,34 @@ sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
             msExpand += tx;
             msFill += tf;
             msDeliver += th;
+        }
+        // SJ_BATCH_LOG=<file>: one line per batch of this round appended to the
+        // file (a diagnostic knob): tasks, pairs, record sizes, stage times
+        if (const char *logPath = getenv("SJ_BATCH_LOG")) {
+            if (FILE *lf = fopen(logPath, "a")) {
+                std::vector<unsigned long long> ho[5];
+                for (int q = 0; q < 5; q++) {
+                    ho[q].resize((size_t)nt + 1);
+                    CK(cudaMemcpy(ho[q].data(), c.off[q].p, sizeof(unsigned long long) * (nt + 1),
+                                  cudaMemcpyDeviceToHost));
+                }
+                for (size_t i = 0; i < nplan; i++) {
+                    const BatchRange &br = todo[i];
+                    const cudaEvent_t *e = ev + EV * i;
+                    float tc, tf, th;
+                    cudaEventElapsedTime(&tc, e[0], e[1]);
+                    cudaEventElapsedTime(&tf, e[5], e[6]);
+                    cudaEventElapsedTime(&th, e[6], e[7]);
+                    fprintf(lf,
+                            "{\"round\": %d, \"batch\": %zu, \"t0\": %u, \"t1\": %u, \"pairs\": %llu, "
+                            "\"row_words\": %llu, \"col_words\": %llu, \"query_recs\": %llu, \"cand_recs\": %llu, "
+                            "\"units\": %llu, \"count_ms\": %.4f, \"emit_ms\": %.4f, \"fold_ms\": %.4f}\n",
+                            round, i, br.t0, br.t1, tot[i], ho[0][br.t1] - ho[0][br.t0], ho[1][br.t1] - ho[1][br.t0],
+                            ho[2][br.t1] - ho[2][br.t0], ho[3][br.t1] - ho[3][br.t0], ho[4][br.t1] - ho[4][br.t0], tc,
+                            tf, th);
+                }
+                fclose(lf);
+            }
         }
         std::vector<BatchRange> redo;
         for (size_t i = 0; i < nplan; i++) {

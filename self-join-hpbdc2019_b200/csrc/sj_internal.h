@@ -43,6 +43,8 @@ struct sj_grid_dev {
     unsigned nCells[SJ_MAX_K];
     unsigned long long mult[SJ_MAX_K];
     double center[SJ_MAX_DIM];  // origin used for non-indexed dimensions in the FP32 filter
+    float offW[SJ_MAX_K + 1];   // estimator features: P(two points uniform in two cells whose coordinates
+                                // differ by one in m of the k indexed dims lie within eps), m = 0..k
 };
 
 // One unit of join work: query points [qBegin, qBegin+qCount) of cell `cell`

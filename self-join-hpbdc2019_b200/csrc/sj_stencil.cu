@@ -89,7 +89,9 @@ __global__ void __launch_bounds__(128) k_neighbours(const uint64_t *__restrict__
     uint32_t owned = 0, writePos = (pass == 1) ? nbrStart[c] : 0u;
     unsigned long long stencilOcc = 0;
     uint32_t hist[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    uint32_t nonEmpty = 0;
+    // owned neighbours' occupancy weighted by the uniform-density hit
+    // probability of their offset class (all classes, classes 1 and 2)
+    float ownW = 0.0f, ownW1 = 0.0f, ownW2 = 0.0f;
 
     int j = k - 1;
     t[j] = 0;
@@ -114,12 +116,19 @@ __global__ void __launch_bounds__(128) k_neighbours(const uint64_t *__restrict__
                     stencilOcc += occ;
                     bool home = (b == c);
                     if (!home) {
-                        nonEmpty++;
                         int bin = 31 - __clz(occ);
                         hist[bin > 7 ? 7 : bin]++;
                         if (owns(pattern, k, a, off, myLid, cellLid[b])) {
                             if (pass == 1) out[writePos++] = b;
                             owned++;
+                            if (feat) {
+                                int m = 0;
+                                for (int q = 0; q < k; q++) m += off[q] != 0;
+                                const float wo = (float)occ * g.offW[m];
+                                ownW += wo;
+                                if (m == 1) ownW1 += wo;
+                                else if (m == 2) ownW2 += wo;
+                            }
                         }
                     }
                     t[0]++;
@@ -142,14 +151,19 @@ __global__ void __launch_bounds__(128) k_neighbours(const uint64_t *__restrict__
             float nst = 1.0f;
             for (int q = 0; q < k; q++) nst *= 3.0f;
             nst -= 1.0f;
-            f[0] = log2f(1.0f + (float)myOcc);
+            // occupancy, neighbour-occupancy histogram, eps / cell width,
+            // dimension; f9, f13, f14: the expected hits with the owned
+            // neighbours (all offset classes, face neighbours, edge neighbours)
+            // under a locally uniform density, log2(1 + occupancy x weighted sum)
+            const float o = (float)myOcc;
+            f[0] = log2f(1.0f + o);
             for (int b = 0; b < 8; b++) f[1 + b] = (float)hist[b] / nst;
-            f[9] = log2f(1.0f + (float)(stencilOcc - myOcc));
+            f[9] = log2f(1.0f + o * ownW);
             f[10] = log2f(1.0f + (float)stencilOcc);
             f[11] = 1.0f;                          // eps / cell width (cells are eps wide)
             f[12] = (float)g.D / 16.0f;
-            f[13] = (float)k / 16.0f;
-            f[14] = (float)nonEmpty / nst;
+            f[13] = log2f(1.0f + o * ownW1);
+            f[14] = log2f(1.0f + o * ownW2);
             f[15] = log2f((float)g.eps) / 8.0f;
         }
     }
