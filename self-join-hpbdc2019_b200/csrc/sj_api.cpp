@@ -235,6 +235,10 @@ struct Ctx {
     int nbrPattern = -1;
     uint32_t nbrTotal = 0;
     DevBuf<uint32_t> nbrStart, nbrCell;
+    DevBuf<uint32_t> nbrPre;           // per owned-neighbour entry: occupancy prefix within its cell
+    DevBuf<double> nbrPreW, cellW;     // occupancy x offset-class weight: per-entry prefix, per-cell total
+    DevBuf<float> nbrWt;               // per entry: offset-class weight
+    bool rateLearned = false;          // c.rate holds the learned estimator's predictions
     DevBuf<uint64_t> candFull;
     DevBuf<float> feat;
     // per-cell predicted hits per evaluation (learned or sampled)
@@ -504,6 +508,12 @@ sj_status build_neighbours(Ctx &c, int pattern)
     CK(c.nbrCell.ensure(h.total));
     CK(sj_launch_neighbours(c.cellLid.p, c.cellCoord.p, c.cellStart.p, nc, c.g, pattern, c.nbrStart.p, c.nbrCell.p,
                             nullptr, nullptr, nullptr, 1, c.s));
+    CK(c.nbrPre.ensure(h.total ? h.total : 1));
+    CK(c.nbrPreW.ensure(h.total ? h.total : 1));
+    CK(c.nbrWt.ensure(h.total ? h.total : 1));
+    CK(c.cellW.ensure(nc ? nc : 1));
+    CK(sj_nbr_spread(c.cellStart.p, c.cellCoord.p, c.nbrStart.p, c.nbrCell.p, nc, c.g, c.nbrPre.p, c.nbrPreW.p,
+                     c.nbrWt.p, c.cellW.p, c.s));
     c.nbrTotal = h.total;
     c.st.full_stencil_calcs = h.full;
     c.nbrPattern = pattern;
@@ -594,8 +604,17 @@ void pipe_ctas(int &join, int &emit)
 }
 
 // Hit-mask words (row or column) one batch may record (4 bytes each); a batch
-// is also cut when its masks would exceed this.
-constexpr uint64_t SJ_MASK_BATCH_WORDS = 1ULL << 29;
+// is also cut when its masks would exceed this.  SJ_MASK_WORDS overrides it
+// (a tuning knob, at most 2^31).
+uint64_t mask_batch_words()
+{
+    uint64_t w = 1ULL << 29;
+    if (const char *e = getenv("SJ_MASK_WORDS")) {
+        const double v = atof(e);
+        if (v >= 65536.0 && v <= 2147483648.0) w = (uint64_t)v;
+    }
+    return w;
+}
 
 // The task list, built on the device (sj_tasks.cu): per-cell workload and cost
 // key, the cost order (stable radix sort, heaviest first, ties in cell order),
@@ -624,9 +643,22 @@ sj_status build_tasks_dev(Ctx &c, bool sym, uint64_t cap, bool byCost, int polic
         const double v = atof(ev);
         if (v >= 1.0) g.pairsPerTask = v;
     }
+    // evaluations per task at most: about 2 ms of one count-pass CTA, so a
+    // batch's tail is short next to its ~10^10 evaluations over ~740 CTAs.
+    // SJ_TASK_EVALS overrides it (0: no limit; a tuning knob)
+    g.evalsPerTask = 4.0e6;
+    if (const char *ev = getenv("SJ_TASK_EVALS")) g.evalsPerTask = std::max(0.0, atof(ev));
     g.sym = sym ? 1 : 0;
     g.policy = policy;
     g.sampleRate = sampleRate;
+    // the learned scheduler shares a cell's predicted neighbour pairs among its
+    // tasks by the offset-class model its features use; the sampling estimate
+    // keeps the cell's mean rate
+    g.spread = (c.rateLearned && policy != 1) ? 1 : 0;
+    g.nbrPre = c.nbrPre.p;
+    g.nbrPreW = c.nbrPreW.p;
+    g.nbrWt = c.nbrWt.p;
+    g.cellW = c.cellW.p;
     DevBuf<uint8_t> &tmp = c.sTemp;
     CK(tmp.ensure(std::max(sj_scan_temp_bytes(nc + 1), sj_radix_temp_bytes(nc))));
     CK(c.tgTot32.ensure(2));
@@ -749,7 +781,7 @@ sj_status plan_dev(Ctx &c, uint64_t cap, std::vector<BatchRange> &plan, uint64_t
     CK(c.planNext.ensure(nt ? nt : 1));
     CK(c.planStart.ensure((size_t)nt + 1));
     CK(c.planCount.ensure(1));
-    CK(sj_plan_batches(off, nt, cap, SJ_MASK_BATCH_WORDS, c.planNext.p, c.planStart.p, c.planCount.p, c.s));
+    CK(sj_plan_batches(off, nt, cap, mask_batch_words(), c.planNext.p, c.planStart.p, c.planCount.p, c.s));
     struct {
         uint32_t nb;
         unsigned long long pred;
@@ -796,7 +828,9 @@ sj_status estimate_rates(Ctx &c)
         CK(sj_launch_mlp_infer(c.feat.p, nc, c.dMlpW.p, out.p, c.s));
         CK(sj_rates_mlp(out.p, c.cellStart.p, c.nbrStart.p, c.nbrCell.p, nc, c.rate.p, c.s));
         c.haveSamples = false;
+        c.rateLearned = true;
     } else {
+        c.rateLearned = false;
         CKS(build_tasks_dev(c, false, 0xffffffffULL, false, 1, (float)c.p.sample_rate, false));
         const uint32_t nt = c.nTasks;
         CK(c.keyCount.ensure(c.n));

@@ -130,9 +130,17 @@ struct sj_taskgen {
     uint32_t tile;               // query points per task (SJ_CTA x query slots)
     uint64_t cap;                // batch capacity: a task's worst case must fit
     double pairsPerTask;         // chunking target of policy 0
+    double evalsPerTask;         // policy 0: evaluations per task at most (0: no limit)
     int sym;                     // symmetric traversal (owned neighbours, both directions emitted)
     int policy;                  // 0 cost-proportional chunks, 1 fixed 65536, 2 mode-8 split by thirds of the work
     float sampleRate;            // > 0: tasks for the sampled queries of each cell only (sampling estimator)
+    // spread != 0: a task's neighbour pairs follow the offset-class model
+    // (sj_nbr_spread) instead of the cell's mean rate
+    int spread;
+    const uint32_t *nbrPre;      // per owned-neighbour entry: exclusive prefix of occupancy within its cell
+    const double *nbrPreW;       // per entry: exclusive prefix of occupancy x offset-class weight
+    const float *nbrWt;          // per entry: its offset-class weight
+    const double *cellW;         // per cell: sum of occupancy x weight over its owned neighbours
 };
 
 // Kernel launches made by this library since load (every launcher calls
@@ -217,6 +225,13 @@ __host__ __device__ inline uint32_t sj_task_units(uint32_t qCount, uint32_t stre
 
 // device task builder (sj_tasks.cu)
 cudaError_t sj_tg_groups(const sj_taskgen &g, uint32_t *cnt, cudaStream_t s);
+// Per owned-neighbour entry of every cell: the exclusive prefixes of the
+// neighbours' occupancy and of occupancy x offset-class weight (g.offW of the
+// number of indexed coordinates in which the two cells differ), the entry's
+// weight, and per cell the weighted total.
+cudaError_t sj_nbr_spread(const uint32_t *cellStart, const uint32_t *cellCoord, const uint32_t *nbrStart,
+                          const uint32_t *nbrCell, uint32_t nCells, const sj_grid_dev &g, uint32_t *nbrPre,
+                          double *nbrPreW, float *nbrWt, double *cellW, cudaStream_t s);
 cudaError_t sj_tg_cells(const sj_taskgen &g, const uint32_t *order, const uint8_t *workersAt, uint32_t *posCnt,
                         unsigned long long *posEv, unsigned long long *costKey, unsigned long long *totals,
                         cudaStream_t s);

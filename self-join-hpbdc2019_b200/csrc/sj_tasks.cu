@@ -86,7 +86,11 @@ __device__ __forceinline__ uint32_t chunk_len(const sj_taskgen &g, float rate, u
         s = 65536;
     } else {
         const double perEval = fmax((double)rate, 1e-6) * (g.sym ? 2.0 : 1.0);
-        const double chunk = g.pairsPerTask / (perEval * (double)qc);
+        double chunk = g.pairsPerTask / (perEval * (double)qc);
+        // a sparse stretch (few pairs per evaluation) is also cut by its
+        // evaluations, so that no task runs much longer than the others and
+        // a batch's last tasks leave little of the device idle
+        if (g.evalsPerTask > 0.0) chunk = fmin(chunk, g.evalsPerTask / (double)qc);
         s = (uint64_t)fmin(65536.0, fmax(256.0, chunk));
     }
     const uint64_t worst = g.cap / ((g.sym ? 2ULL : 1ULL) * (uint64_t)qc);
@@ -111,10 +115,47 @@ __device__ __forceinline__ float2 rates_of(const sj_taskgen &g, uint32_t c)
 // Predicted pairs of evH home and evO neighbour evaluations with `diag` of
 // the home ones a query against itself: a symmetric traversal emits a hit
 // in both directions, a self pair once.
-__device__ __forceinline__ double pairs_of(const sj_taskgen &g, float2 r, uint64_t evH, uint64_t evO, uint64_t diag)
+__device__ __forceinline__ double pairs_of(const sj_taskgen &g, float2 r, uint64_t evH, double evO, uint64_t diag)
 {
-    const double hits = (double)evH * (double)r.x + (double)evO * (double)r.y;
+    const double hits = (double)evH * (double)r.x + evO * (double)r.y;
     return g.sym ? fmax(0.0, 2.0 * hits - (double)diag) : hits;
+}
+
+// Weighted prefix of cell c's owned-neighbour stream at position x (0 at the
+// first neighbour, cellW at the end): the entries' weighted prefix plus the
+// weight of the part of x's own segment before x.
+__device__ __forceinline__ double weighted_prefix(const sj_taskgen &g, uint32_t c, uint32_t x)
+{
+    uint32_t lo = g.nbrStart[c], hi = g.nbrStart[c + 1];
+    if (lo == hi) return 0.0;
+    // the last entry whose prefix is <= x
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (g.nbrPre[mid] <= x) lo = mid; else hi = mid;
+    }
+    const uint32_t b = g.nbrCell[lo];
+    const uint32_t len = g.cellStart[b + 1] - g.cellStart[b];
+    const uint32_t in = min(x - g.nbrPre[lo], len);
+    return g.nbrPreW[lo] + (double)in * (double)g.nbrWt[lo];
+}
+
+// Neighbour evaluations of a task, as the mean-rate equivalent: with the
+// spread, qc x (its stream's weighted length) x (the cell's mean weight)^-1,
+// so that the cell's tasks share its predicted neighbour hits in proportion to
+// the uniform-density hits of the segments they cover; otherwise qc x length.
+// [n0, n1): the task's positions in its group's neighbour stream.
+__device__ __forceinline__ double neighbour_evals(const sj_taskgen &g, uint32_t c, uint32_t grp, uint32_t qc,
+                                                  uint32_t n0, uint32_t n1)
+{
+    if (n1 <= n0) return 0.0;
+    if (!g.spread || g.cellW[c] <= 0.0) return (double)qc * (double)(n1 - n0);
+    const uint32_t e0 = g.nbrStart[c], e1 = g.nbrStart[c + 1];
+    const uint32_t eg = e0 + (grp == 0 ? 0u : grp * SJ_MAX_SEG - 1u);   // the group's first neighbour entry
+    const uint32_t base = g.nbrPre[eg];
+    const uint32_t bl = g.nbrCell[e1 - 1];
+    const double total = (double)g.nbrPre[e1 - 1] + (double)(g.cellStart[bl + 1] - g.cellStart[bl]);
+    const double wl = weighted_prefix(g, c, base + n1) - weighted_prefix(g, c, base + n0);
+    return (double)qc * wl * total / g.cellW[c];
 }
 
 // Query tile `tile` of cell c against segment group grp (non-home length S).
@@ -229,6 +270,57 @@ __global__ void __launch_bounds__(256) k_tg_cells(sj_taskgen g, const uint32_t *
     }
 }
 
+// One warp per cell: exclusive prefixes over its owned-neighbour entries of the
+// occupancy and of occupancy x offset-class weight (see sj_nbr_spread).
+__global__ void __launch_bounds__(256) k_nbr_spread(const uint32_t *__restrict__ cellStart,
+                                                    const uint32_t *__restrict__ cellCoord,
+                                                    const uint32_t *__restrict__ nbrStart,
+                                                    const uint32_t *__restrict__ nbrCell, uint32_t nCells,
+                                                    sj_grid_dev gd, uint32_t *__restrict__ nbrPre,
+                                                    double *__restrict__ nbrPreW, float *__restrict__ nbrWt,
+                                                    double *__restrict__ cellW)
+{
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (c >= nCells) return;
+    const int k = gd.k;
+    const uint32_t e0 = nbrStart[c], e1 = nbrStart[c + 1];
+    uint32_t carryP = 0;
+    double carryW = 0.0;
+    for (uint32_t base = e0; base < e1; base += 32) {
+        const uint32_t e = base + lane;
+        uint32_t occ = 0;
+        float w = 0.0f;
+        if (e < e1) {
+            const uint32_t b = nbrCell[e];
+            occ = cellStart[b + 1] - cellStart[b];
+            int m = 0;
+            for (int j = 0; j < k; j++) m += cellCoord[(uint64_t)c * k + j] != cellCoord[(uint64_t)b * k + j];
+            w = gd.offW[m];
+        }
+        const double wv = (double)occ * (double)w;
+        uint32_t ip = occ;
+        double iw = wv;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t yp = __shfl_up_sync(FULL, ip, o);
+            const double yw = __shfl_up_sync(FULL, iw, o);
+            if (lane >= (uint32_t)o) {
+                ip += yp;
+                iw += yw;
+            }
+        }
+        if (e < e1) {
+            nbrPre[e] = carryP + ip - occ;
+            nbrPreW[e] = carryW + iw - wv;
+            nbrWt[e] = w;
+        }
+        carryP += __shfl_sync(FULL, ip, 31);
+        carryW += __shfl_sync(FULL, iw, 31);
+    }
+    if (lane == 0) cellW[c] = carryW;
+}
+
 __global__ void __launch_bounds__(256) k_iota(uint32_t *v, uint32_t n)
 {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -322,7 +414,7 @@ __global__ void __launch_bounds__(256) k_tg_item_write(sj_taskgen g, const uint3
             evH = g.sym ? diag_evals(s0, h1, w.qc) : (uint64_t)w.qc * (h1 - s0);
             diag = s0 < w.qc ? min(h1, w.qc) - s0 : 0u;   // queries whose own position is in the chunk
         }
-        const uint64_t evO = (uint64_t)w.qc * (s1 - max(s0, h1));
+        const double evO = neighbour_evals(g, it.c, it.grp, w.qc, max(s0, h1) - w.homeLen, s1 - w.homeLen);
         sj_task k;
         k.cell = it.c;
         k.qBegin = w.qBegin;
@@ -752,6 +844,17 @@ __global__ void __launch_bounds__(S64T) k_s64_write(const unsigned long long *__
 inline unsigned blocks_for(uint64_t n, unsigned per) { return (unsigned)((n + per - 1) / per); }
 
 }  // namespace
+
+cudaError_t sj_nbr_spread(const uint32_t *cellStart, const uint32_t *cellCoord, const uint32_t *nbrStart,
+                          const uint32_t *nbrCell, uint32_t nCells, const sj_grid_dev &g, uint32_t *nbrPre,
+                          double *nbrPreW, float *nbrWt, double *cellW, cudaStream_t s)
+{
+    if (nCells == 0) return cudaSuccess;
+    k_nbr_spread<<<blocks_for((uint64_t)nCells * 32, 256), 256, 0, s>>>(cellStart, cellCoord, nbrStart, nbrCell,
+                                                                          nCells, g, nbrPre, nbrPreW, nbrWt, cellW);
+    sj_note_launch();
+    return cudaGetLastError();
+}
 
 cudaError_t sj_tg_groups(const sj_taskgen &g, uint32_t *cnt, cudaStream_t s)
 {
