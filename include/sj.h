@@ -112,6 +112,8 @@ typedef struct {
     float ms_fill_kernel;       /* fill kernel time alone */
     uint64_t kernel_launches;   /* this library's kernel launches during the last join */
     float ms_expand;            /* key-array expansion from the batch's key runs */
+    uint32_t exact_plan_batches;/* batches the same greedy plan needs with the measured per-task pairs
+                                   in place of the predictions (the estimator-free reference count) */
 } sj_stats;
 
 /* Opaque engine context: one per device, created by sj_create, released by

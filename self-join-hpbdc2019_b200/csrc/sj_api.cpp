@@ -238,6 +238,7 @@ struct Ctx {
     DevBuf<uint32_t> nbrPre;           // per owned-neighbour entry: occupancy prefix within its cell
     DevBuf<double> nbrPreW, cellW;     // occupancy x offset-class weight: per-entry prefix, per-cell total
     DevBuf<float> nbrWt;               // per entry: offset-class weight
+    DevBuf<float> exactPred;           // per task: its measured pairs (the exact plan of the statistics)
     bool rateLearned = false;          // c.rate holds the learned estimator's predictions
     DevBuf<uint64_t> candFull;
     DevBuf<float> feat;
@@ -608,7 +609,7 @@ void pipe_ctas(int &join, int &emit)
 // (a tuning knob, at most 2^31).
 uint64_t mask_batch_words()
 {
-    uint64_t w = 1ULL << 29;
+    uint64_t w = 1ULL << 30;
     if (const char *e = getenv("SJ_MASK_WORDS")) {
         const double v = atof(e);
         if (v >= 65536.0 && v <= 2147483648.0) w = (uint64_t)v;
@@ -1446,6 +1447,20 @@ sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
         c.st.distance_calcs = sm[0];
         c.st.refined_pairs = sm[1];
         c.st.estimator_task_rel_err = sm[2] ? err / (double)sm[2] : 0.0;
+    }
+    if (nt) {
+        // the estimator-free reference count: the same greedy plan with every
+        // task's measured pairs in place of its prediction
+        CK(c.exactPred.ensure(nt));
+        CK(sj_u32_to_f32(c.taskHits.p, nt, c.exactPred.p, c.s));
+        unsigned long long *o[7];
+        for (int k = 0; k < 7; k++) o[k] = c.off[k].p;
+        CK(sj_task_offsets(c.dTasks.p, c.exactPred.p, nt, c.p.alpha, c.offTemp.p, o, c.s));
+        CK(sj_plan_batches(o, nt, cap, mask_batch_words(), c.planNext.p, c.planStart.p, c.planCount.p, c.s));
+        uint32_t nbExact = 0;
+        CK(cudaMemcpyAsync(&nbExact, c.planCount.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, c.s));
+        CK(cudaStreamSynchronize(c.s));
+        c.st.exact_plan_batches = nbExact;
     }
     c.st.total_pairs = pairsTotal;
     c.st.pair_hash = hs[4];

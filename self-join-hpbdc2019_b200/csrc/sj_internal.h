@@ -179,6 +179,8 @@ size_t sj_expand_long_slots(uint64_t cap);
 // sj_expand_keys), adds the pairs' set hash to *hashOut; skipped when the
 // batch's count exceeds cap.  chunkKey: sj_fold_chunks(cap) entries of scratch.
 size_t sj_fold_chunks(uint64_t cap);
+// out[i] = (float)in[i]
+cudaError_t sj_u32_to_f32(const uint32_t *in, uint64_t n, float *out, cudaStream_t s);
 cudaError_t sj_fold(const uint32_t *excl, const uint32_t *total, uint64_t n, const int32_t *val, int32_t *outKey,
                     const unsigned long long *batchPairs, uint64_t cap, uint32_t *chunkKey,
                     unsigned long long *hashOut, int numSM, cudaStream_t s);

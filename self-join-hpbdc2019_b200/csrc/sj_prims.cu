@@ -541,7 +541,22 @@ __global__ void __launch_bounds__(256) k_csr_append(const uint32_t *__restrict__
     }
 }
 
+__global__ void __launch_bounds__(256) k_u32_to_f32(const uint32_t *__restrict__ in, uint64_t n,
+                                                    float *__restrict__ out)
+{
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = (float)in[i];
+}
+
 }  // namespace
+
+cudaError_t sj_u32_to_f32(const uint32_t *in, uint64_t n, float *out, cudaStream_t s)
+{
+    if (n == 0) return cudaSuccess;
+    k_u32_to_f32<<<(unsigned)ceil_div(n, 256), 256, 0, s>>>(in, n, out);
+    sj_note_launch();
+    return cudaGetLastError();
+}
 
 cudaError_t sj_expand_keys(const uint32_t *excl, const uint32_t *total, uint64_t n, int32_t *outKey,
                            const unsigned long long *batchPairs, uint64_t cap, void *longRuns, uint32_t longCap,

@@ -57,7 +57,7 @@ class Stats(C.Structure):
         ("ms_upload", C.c_float), ("ms_index", C.c_float), ("ms_tasks", C.c_float), ("ms_estimate", C.c_float),
         ("ms_count", C.c_float), ("ms_scan", C.c_float), ("ms_fill", C.c_float), ("ms_deliver", C.c_float),
         ("ms_total", C.c_float), ("ms_join_kernels", C.c_float), ("ms_fill_kernel", C.c_float),
-        ("kernel_launches", C.c_uint64), ("ms_expand", C.c_float),
+        ("kernel_launches", C.c_uint64), ("ms_expand", C.c_float), ("exact_plan_batches", C.c_uint32),
     ]
 
     def as_dict(self) -> dict:

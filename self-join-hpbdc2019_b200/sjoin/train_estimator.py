@@ -21,8 +21,10 @@ hold the pairs: the training set is drawn from the collected cells with
 probability proportional to (1 + hits)^beta (beta = 0.5 by default), which
 keeps every cell size represented while the heavy cells that dominate a
 batch's total are seen far more often than their number alone would give.
-Weights are written as raw float32 in the engine's layout (sj_mlp_num_params()
-values).
+Last, the two output biases are shifted so that the summed predictions over
+every collected cell equal the measured sums (a log-space fit predicts typical
+values, while a batch's size is a sum).  Weights are written as raw float32 in
+the engine's layout (sj_mlp_num_params() values).
 
 usage: python -m sjoin.train_estimator [--runs 50] [--out sjoin/estimator_c4.bin]
 """
@@ -36,7 +38,7 @@ import time
 
 import numpy as np
 
-from . import PREC_FP32_REFINE, SCHED_SAMPLING, SelfJoin, datasets, mlp_init, mlp_loss_grad, mlp_train
+from . import PREC_FP32_REFINE, SCHED_SAMPLING, SelfJoin, datasets, mlp_forward, mlp_init, mlp_loss_grad, mlp_train
 
 PKG = os.path.dirname(os.path.abspath(__file__))
 DEFAULT_OUT = os.path.join(PKG, "estimator_c4.bin")
@@ -104,6 +106,18 @@ def train(x: np.ndarray, y: np.ndarray, steps: int = 6000, lr: float = 2e-3, bat
     return w, loss
 
 
+def calibrate(x: np.ndarray, y: np.ndarray, w: np.ndarray):
+    """Shifts the two output biases so that the network's hits, summed over every collected cell,
+    equal the measured sums.  A fit in log space predicts a typical value rather than the mean,
+    while a batch's size is a sum of predictions: the shift removes that bias from the sums."""
+    pred = mlp_forward(x, w).astype(np.float64)
+    meas = np.exp2(y.astype(np.float64)) - 1.0
+    shift = np.log2(meas.sum(0) / np.maximum(np.exp2(pred) - 1.0, 0.0).sum(0))
+    w = w.astype(np.float32).copy()
+    w[-2:] += shift.astype(np.float32)
+    return w, [round(float(v), 6) for v in shift]
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--runs", type=int, default=50)
@@ -124,9 +138,10 @@ def main():
         np.savez_compressed(args.data_out, x=x, y=y)
     xt, yt = resample(x, y, beta=args.beta) if args.beta > 0 else (x, y)
     w, loss = train(xt, yt, steps=args.steps)
+    w, shift = calibrate(x, y, w)
     full, _ = mlp_loss_grad(x, y, w)
     w.astype(np.float32).tofile(args.out)
-    print(json.dumps({"cells": int(len(x)), "final_loss": full, "out": args.out,
+    print(json.dumps({"cells": int(len(x)), "final_loss": full, "output_shift": shift, "out": args.out,
                       "seconds": round(time.time() - t0, 1)}), flush=True)
 
 
