@@ -462,7 +462,7 @@ def run_ours(args):
         fs = f_stats[-1]
         fp64 = {"ms_per_step": fm, "step_ms": f_ms, "steps": args.fp64_steps, "warmup": 1,
                 "pairs_per_step": fp, "pair_hash": fh, "scheduler": "sampling", "precision": "fp64",
-                "batches": fs["num_batches"], "overflow_retries": fs["overflow_retries"],
+                "batches": fs["num_batches"], "exact_plan_batches": fs["exact_plan_batches"], "overflow_retries": fs["overflow_retries"],
                 "phases_ms": {k2: round(fs[k2], 3) for k2 in ("ms_index", "ms_tasks", "ms_estimate", "ms_count",
                                                               "ms_scan", "ms_fill", "ms_expand", "ms_deliver",
                                                               "ms_total")},
@@ -515,7 +515,7 @@ def run_ours(args):
         "host_threads_per_rank": rank_host_threads(),
         "phases_ms": {k2: round(s[k2], 3) for k2 in ("ms_index", "ms_tasks", "ms_estimate", "ms_count", "ms_scan",
                                                      "ms_fill", "ms_expand", "ms_deliver", "ms_total")},
-        "batches": s["num_batches"], "overflow_retries": s["overflow_retries"], "tasks": s["num_tasks"],
+        "batches": s["num_batches"], "exact_plan_batches": s["exact_plan_batches"], "overflow_retries": s["overflow_retries"], "tasks": s["num_tasks"],
         "distance_calcs": s["distance_calcs"], "full_stencil_calcs": s["full_stencil_calcs"],
         "refined_pairs": s["refined_pairs"], "step_ms": step_ms,
         "scheduler": "learned" if learned else "sampling", "estimated_pairs": s["estimated_pairs"],
