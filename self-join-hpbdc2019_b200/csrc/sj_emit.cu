@@ -368,178 +368,6 @@ __device__ __forceinline__ void emit_cols(const sj_join_args &a, const UnitTask 
     }
 }
 
-// Column unit, whole rounds: lane j holds candidate j's words of CG query
-// groups at once.  Its entries of those groups are consecutive in the
-// candidate's run (group by group, bits ascending), so one scan of the lanes'
-// totals places the round, the lane decodes its words one after another, and
-// one copy-out writes the round: a scan and a copy-out per CG groups instead of
-// per group, which is what a sparse column (a few bits per word) pays for.  A
-// round with more entries than the staging buffer goes group by group.
-#ifndef SJ_EMIT_COLS2
-#define SJ_EMIT_COLS2 1
-#endif
-constexpr int CG = 8;   // query groups per column round; entry = (lane << 8) | (group in round << 5) | bit
-
-__device__ __forceinline__ void emit_cols_rounds(const sj_join_args &a, const UnitTask &u, uint32_t b, WarpSmem &w,
-                                                 uint32_t lane)
-{
-    const uint32_t nG = (u.qc + 31) / 32;
-    const uint32_t s = b * 32 + lane;
-    const uint64_t rec = a.candOff[u.t] - a.candOff[a.taskBegin];
-    // words of positions past the stream end are zero (the count pass masks them)
-    const uint32_t *const cw = a.colMasks + (a.colOff[u.t] - a.colOff[a.taskBegin]) + (uint64_t)b * nG * 32 + lane;
-    const uint32_t *const qids = a.ids + u.qBegin;
-    uint32_t slot = 0;
-    __syncwarp();        // the previous unit is done with the warp's shared memory
-    if (s < u.L) {
-        slot = a.keyStart[a.candId[rec + s]] + a.candRel[rec + s];
-    }
-    // one round: the words m (cnt set bits in all) of groups g0 .. g0 + CG - 1
-    auto round = [&](const uint32_t (&m)[CG], uint32_t cnt, uint32_t g0) {
-        const uint32_t incl = warp_incl_scan(cnt, lane);
-        const uint32_t T = __shfl_sync(FULL, incl, 31);
-        const uint32_t ex = incl - cnt;
-        __syncwarp();   // the previous round's copy-out is done with ent / base
-        w.base[lane] = slot - ex;   // lane L's entries [ex_L, ex_L + cnt_L) go to slot_L onwards
-        uint32_t pos = ex;
-#pragma unroll
-        for (int i = 0; i < CG; i++) {
-            const uint32_t c = __popc(m[i]);
-            decode_bits(m[i], c, (lane << 8) | ((uint32_t)i << 5), w.ent, pos);
-            pos += c;
-        }
-        __syncwarp();
-        const uint32_t *const base = w.base;
-        const auto slotOf = [base](uint32_t en, uint32_t e) { return base[en >> 8] + e; };
-        const auto srcOf = [](uint32_t en) { return en & 0xffu; };
-        if (__all_sync(FULL, (uint64_t)slot + cnt <= a.capacity))
-            copy_out<true>(a, w.ent, T, qids + g0 * 32, lane, slotOf, srcOf);
-        else
-            copy_out<false>(a, w.ent, T, qids + g0 * 32, lane, slotOf, srcOf);
-        slot += cnt;
-        return T;
-    };
-    for (uint32_t g0 = 0; g0 < nG; g0 += CG) {
-        uint32_t cur[CG];
-        uint32_t tot = 0;
-#pragma unroll
-        for (int i = 0; i < CG; i++) {
-            const uint32_t g = g0 + (uint32_t)i;
-            uint32_t x = g < nG ? __ldg(cw + (uint64_t)g * 32) : 0u;
-            // positions past the stream end and queries past the tile have no
-            // bits in a consistent count pass
-            const uint32_t nq = g < nG ? u.qc - g * 32 : 0u;
-            const uint32_t valid = s >= u.L ? 0u : (nq >= 32u ? FULL : (1u << nq) - 1u);
-            if (x & ~valid) {
-                atomicMax(&a.stat[6], 1ULL);
-                x &= valid;
-            }
-            cur[i] = x;
-            tot += __popc(x);
-        }
-        if (__ballot_sync(FULL, tot) == 0) continue;   // warp-uniform
-        const uint32_t T = __reduce_add_sync(FULL, tot);
-        if (T <= (uint32_t)EM_CAP) {
-            round(cur, tot, g0);
-        } else {
-            // a dense round: one group at a time (at most 1024 entries each)
-#pragma unroll
-            for (int i = 0; i < CG; i++) {
-                uint32_t one[CG];
-#pragma unroll
-                for (int j = 0; j < CG; j++) one[j] = j == i ? cur[i] : 0u;
-                const uint32_t c = __popc(cur[i]);
-                if (__ballot_sync(FULL, c)) round(one, c, g0);
-            }
-        }
-    }
-}
-
-// Row unit, whole rounds: lane q holds RB consecutive words (blocks) of query
-// q0 + q in the current chunk; the query's entries of those blocks are
-// consecutive in its run (blocks ascending, bits ascending), so, as for the
-// columns, one scan of the lanes' totals, a decode per lane and one copy-out
-// place a round of 32 x RB words.  A round with more entries than the staging
-// buffer is done in sub-rounds of two words per lane (at most 2048 entries).
-#ifndef SJ_EMIT_ROWS2
-#define SJ_EMIT_ROWS2 1
-#endif
-constexpr int RB = 8;   // blocks per row round; entry = (lane << 11) | (block in chunk << 5) | bit
-
-__device__ __forceinline__ void emit_rows_rounds(const sj_join_args &a, const UnitTask &u, uint32_t g, WarpSmem &w,
-                                                 uint32_t lane)
-{
-    const uint32_t qc = u.qc;
-    const uint32_t q0 = g * 32;
-    const uint32_t nq = min(32u, qc - q0);
-    const uint32_t nBlk = (u.L + 31) / 32;
-    const uint32_t *const masks = a.masks + (a.maskOff[u.t] - a.maskOff[a.taskBegin]);
-    const uint32_t *const cid = a.candId + (a.candOff[u.t] - a.candOff[a.taskBegin]);
-    const uint32_t *const rel = a.rowRel + (a.rowOff[u.t] - a.rowOff[a.taskBegin]);
-    uint32_t slot = 0;   // lane q: slot of query q's next pair
-    __syncwarp();        // the previous unit is done with the warp's shared memory
-    if (lane < nq) {
-        const uint32_t qid = a.ids[u.qBegin + q0 + lane];
-        slot = a.keyStart[qid] + rel[q0 + lane];
-    }
-    for (uint32_t c0 = 0; c0 < nBlk; c0 += 64) {
-        const uint32_t cb = min(64u, nBlk - c0);   // blocks of this chunk
-        // query q0 + l's words of this chunk: wq[l * cb .. l * cb + cb)
-        const uint32_t *const wq = masks + (uint64_t)c0 * qc + (uint64_t)q0 * cb + (uint64_t)lane * cb;
-        const uint32_t *const pcid = cid + c0 * 32;
-        auto round = [&](const uint32_t (&m)[RB], uint32_t cnt, uint32_t j0) {
-            const uint32_t incl = warp_incl_scan(cnt, lane);
-            const uint32_t T = __shfl_sync(FULL, incl, 31);
-            const uint32_t ex = incl - cnt;
-            __syncwarp();   // the previous round's copy-out is done with ent / base
-            w.base[lane] = slot - ex;
-            uint32_t pos = ex;
-#pragma unroll
-            for (int i = 0; i < RB; i++) {
-                const uint32_t c = __popc(m[i]);
-                decode_bits(m[i], c, (lane << 11) | ((j0 + (uint32_t)i) << 5), w.ent, pos);
-                pos += c;
-            }
-            __syncwarp();
-            const uint32_t *const base = w.base;
-            const auto slotOf = [base](uint32_t en, uint32_t e) { return base[en >> 11] + e; };
-            const auto srcOf = [](uint32_t en) { return en & 0x7ffu; };
-            if (__all_sync(FULL, (uint64_t)slot + cnt <= a.capacity))
-                copy_out<true>(a, w.ent, T, pcid, lane, slotOf, srcOf);
-            else
-                copy_out<false>(a, w.ent, T, pcid, lane, slotOf, srcOf);
-            slot += cnt;
-        };
-        for (uint32_t j0 = 0; j0 < cb; j0 += RB) {
-            uint32_t m[RB];
-            uint32_t tot = 0;
-#pragma unroll
-            for (int i = 0; i < RB; i++) {
-                const uint32_t j = j0 + (uint32_t)i;
-                uint32_t x = (lane < nq && j < cb) ? __ldg(wq + j) : 0u;
-                // bits past the stream end are never set by a consistent count pass
-                if (x) x = stream_checked(a, x, (c0 + j) * 32u, u.L);
-                m[i] = x;
-                tot += __popc(x);
-            }
-            if (__ballot_sync(FULL, tot) == 0) continue;   // warp-uniform
-            if (__reduce_add_sync(FULL, tot) <= (uint32_t)EM_CAP) {
-                round(m, tot, j0);
-            } else {
-                // a dense round: two blocks per lane at a time (at most 2048 entries)
-#pragma unroll
-                for (int h = 0; h < RB; h += 2) {
-                    uint32_t two[RB];
-#pragma unroll
-                    for (int i = 0; i < RB; i++) two[i] = (i == h || i == h + 1) ? m[i] : 0u;
-                    const uint32_t c = __popc(m[h]) + __popc(m[h + 1]);
-                    if (__ballot_sync(FULL, c)) round(two, c, j0);
-                }
-            }
-        }
-    }
-}
-
 __global__ void __launch_bounds__(EW, SJ_EMIT_MINB) k_emit(sj_join_args a)
 {
     __shared__ WarpSmem smem[ENW];
@@ -587,20 +415,8 @@ __global__ void __launch_bounds__(EW, SJ_EMIT_MINB) k_emit(sj_join_args a)
         const bool sym = (tp->flags & SJ_TASK_SYM) != 0;
         const uint32_t k = un - (uint32_t)(a.unitOff[lo] - u0);
         const uint32_t nG = (u.qc + 31) / 32;
-        if (k < nG) {
-#if SJ_EMIT_ROWS2
-            emit_rows_rounds(a, u, k, w, lane);
-#else
-            emit_rows(a, u, k, w, lane);
-#endif
-        }
-        else if (sym) {
-#if SJ_EMIT_COLS2
-            emit_cols_rounds(a, u, k - nG, w, lane);
-#else
-            emit_cols(a, u, k - nG, w, lane);
-#endif
-        }
+        if (k < nG) emit_rows(a, u, k, w, lane);
+        else if (sym) emit_cols(a, u, k - nG, w, lane);
     }
 }
 

@@ -402,23 +402,6 @@ __global__ void __launch_bounds__(256) k_fold_chunk_keys(const uint32_t *__restr
     for (uint32_t c = (st + FOLD_CHUNK - 1) / FOLD_CHUNK; (uint64_t)c * FOLD_CHUNK < en; c++) chunkKey[c] = (uint32_t)k;
 }
 
-constexpr int FOLD_PF = 2;   // rounds of values loaded ahead
-
-// The values of slots p .. p + 3 below end (zeros past it): one 16-byte
-// streaming load when all four are present (p is a multiple of 4).
-__device__ __forceinline__ int4 fold_load(const int32_t *__restrict__ val, uint32_t p, uint32_t end)
-{
-    int4 v = make_int4(0, 0, 0, 0);
-    if (p + 4 <= end) {
-        v = __ldcs(reinterpret_cast<const int4 *>(val + p));
-    } else if (p < end) {
-        v.x = __ldcs(val + p);
-        if (p + 1 < end) v.y = __ldcs(val + p + 1);
-        if (p + 2 < end) v.z = __ldcs(val + p + 2);
-    }
-    return v;
-}
-
 __global__ void __launch_bounds__(FOLD_THREADS, FOLD_CTAS_PER_SM) k_fold(const uint32_t *__restrict__ excl,
                                                        const uint32_t *__restrict__ total, uint64_t n,
                                                        const int32_t *__restrict__ val, int32_t *__restrict__ outKey,
@@ -443,20 +426,18 @@ __global__ void __launch_bounds__(FOLD_THREADS, FOLD_CTAS_PER_SM) k_fold(const u
         uint64_t k = chunkKey[c];         // its run holds slot p0
         uint32_t carry = (uint32_t)k;     // key of the round's slots before its first marked start
         uint32_t S = runStart(k + lane), R = runEnd(k + lane);
-        // the values of the next FOLD_PF rounds are in flight while a round's
-        // keys are found and hashed (enough bytes in flight per SM to cover
-        // the DRAM latency at full bandwidth)
-        int4 ring[FOLD_PF];
-#pragma unroll
-        for (int r = 0; r < FOLD_PF; r++) ring[r] = fold_load(val, p0 + 128u * r + 4 * lane, p1);
         for (uint32_t base = p0; base < p1; base += 128) {
             const uint32_t lim = min(base + 128u, p1);
             const uint32_t p = base + 4 * lane;
             const uint32_t cnt = p < lim ? min(4u, lim - p) : 0u;   // this lane's slots: p .. p + cnt - 1
-            const int4 v = ring[0];
-#pragma unroll
-            for (int r = 0; r + 1 < FOLD_PF; r++) ring[r] = ring[r + 1];
-            ring[FOLD_PF - 1] = fold_load(val, p + 128u * FOLD_PF, p1);
+            int4 v = make_int4(0, 0, 0, 0);   // the values, loaded while the keys are found
+            if (cnt == 4) {
+                v = __ldcs(reinterpret_cast<const int4 *>(val + p));
+            } else {
+                if (cnt > 0) v.x = __ldcs(val + p);
+                if (cnt > 1) v.y = __ldcs(val + p + 1);
+                if (cnt > 2) v.z = __ldcs(val + p + 2);
+            }
             __syncwarp();   // every lane has cleared its slots of the previous round
             for (;;) {
                 if (R > S && S >= base && S < lim) mk[S - base] = (uint32_t)(k + lane) + 1u;
