@@ -1213,13 +1213,13 @@ sj_status run_join(Ctx &c, int delivery, sj_batch_cb cb, void *user)
         // SJ_BATCH_LOG=<file>: one line per batch of this round appended to the
         // file (a diagnostic knob): tasks, pairs, record sizes, stage times
         if (const char *logPath = getenv("SJ_BATCH_LOG")) {
+            std::vector<unsigned long long> ho[5];
+            for (int q = 0; q < 5; q++) {
+                ho[q].resize((size_t)nt + 1);
+                CK(cudaMemcpy(ho[q].data(), c.off[q].p, sizeof(unsigned long long) * (nt + 1),
+                              cudaMemcpyDeviceToHost));
+            }
             if (FILE *lf = fopen(logPath, "a")) {
-                std::vector<unsigned long long> ho[5];
-                for (int q = 0; q < 5; q++) {
-                    ho[q].resize((size_t)nt + 1);
-                    CK(cudaMemcpy(ho[q].data(), c.off[q].p, sizeof(unsigned long long) * (nt + 1),
-                                  cudaMemcpyDeviceToHost));
-                }
                 for (size_t i = 0; i < nplan; i++) {
                     const BatchRange &br = todo[i];
                     const cudaEvent_t *e = ev + EV * i;
