@@ -45,6 +45,7 @@ def lib():
         L.orc_index_grid.argtypes = [vp, vp, vp]
         L.orc_index_export.argtypes = [vp, vp, vp, vp, vp, vp]
         L.orc_join_stats.argtypes = [vp, C.c_int, i64, i64, i64, C.c_int, u64p, u64p, u64p]
+        L.orc_join_stats_unicomp.argtypes = [vp, C.c_int, i64, i64, i64, C.c_int, u64p, u64p, u64p]
         L.orc_join_degrees.argtypes = [vp, C.c_int, C.c_int, vp]
         L.orc_query_rows.argtypes = [vp, C.c_int, vp, i64, C.c_int, vp, vp, vp, vp, i64]
         L.orc_join_pairs.restype = i64
@@ -122,12 +123,15 @@ class OracleIndex:
         return dict(indexLookupArr=lookup, grid=grid, gridLinearID=lid,
                     gridCellNDMask=mask[:nmask], gridCellNDMaskOffsets=moff)
 
-    def stats(self, fma_mode=1, q0=0, q1=None, qstride=1, threads=0):
-        """(pair count, set hash, candidate evaluations) for sampled query ids."""
+    def stats(self, fma_mode=1, q0=0, q1=None, qstride=1, threads=0, unicomp=False):
+        """(pair count, set hash, candidate evaluations) for sampled query ids.
+        unicomp=True: each sampled point evaluates only the candidates it owns
+        under the linear-ID Unicomp rule and counts both directions of a hit
+        (over all points: the same pairs and hash, half the evaluations)."""
         P, H, E = C.c_uint64(), C.c_uint64(), C.c_uint64()
         q1 = self.n if q1 is None else q1
-        lib().orc_join_stats(self._h, fma_mode, q0, q1, qstride, threads,
-                             C.byref(P), C.byref(H), C.byref(E))
+        fn = lib().orc_join_stats_unicomp if unicomp else lib().orc_join_stats
+        fn(self._h, fma_mode, q0, q1, qstride, threads, C.byref(P), C.byref(H), C.byref(E))
         return P.value, H.value, E.value
 
     def degrees(self, fma_mode=1, threads=0) -> np.ndarray:

@@ -372,6 +372,63 @@ int orc_join_stats(const orc_index *ix, int fma_mode, int64_t q0, int64_t q1, in
     return 0;
 }
 
+/* orc_join_stats under the linear-ID Unicomp ownership (kernel.cu:1529-1534):
+ * a sampled point p evaluates the points of its own cell with a larger id and
+ * every point of the stencil cells with a larger linear id, and each hit
+ * counts both directions, (p,q) and (q,p) (a self pair once).  Over all points
+ * the pairs and the set hash equal orc_join_stats's with half the candidate
+ * evaluations: the CPU baseline's join (a CPU self-join evaluates each
+ * unordered pair once, as the reference's Unicomp kernels do). */
+int orc_join_stats_unicomp(const orc_index *ix, int fma_mode, int64_t q0, int64_t q1, int64_t qstride,
+                           int nthreads, uint64_t *pairs, uint64_t *hash, uint64_t *evals)
+{
+    const int D = ix->g.D;
+    const double eps = ix->g.eps;
+    const double *pts = ix->pts;
+    if (qstride < 1) qstride = 1;
+    if (q1 > ix->n) q1 = ix->n;
+    uint64_t P = 0, H = 0, E = 0;
+    int64_t cap = orc_stencil_cap(ix->g.k);
+#ifdef _OPENMP
+    if (nthreads < 1) nthreads = omp_get_max_threads();
+#pragma omp parallel num_threads(nthreads) reduction(+ : P, H, E)
+#endif
+    {
+        int64_t *nb = malloc(sizeof(int64_t) * (size_t)cap);
+        int64_t nq = (q1 - q0 + qstride - 1) / qstride;
+#ifdef _OPENMP
+#pragma omp for schedule(dynamic, 64)
+#endif
+        for (int64_t t = 0; t < nq; t++) {
+            int64_t p = q0 + t * qstride;
+            const double *qp = pts + p * D;
+            const int64_t c = ix->pointCell[p];
+            int m = orc_stencil(ix, (uint32_t)c, nb);
+            for (int b = 0; b < m; b++) {
+                if (nb[b] < c) continue;   /* owned by the cell with the larger linear id */
+                const int home = nb[b] == c;
+                for (int32_t s = ix->cellMin[nb[b]]; s <= ix->cellMax[nb[b]]; s++) {
+                    uint32_t q = ix->lookup[s];
+                    if (home && (int64_t)q < p) continue;
+                    E++;
+                    if (orc_within(orc_dist2(pts + (int64_t)q * D, qp, D, fma_mode), eps)) {
+                        if ((int64_t)q == p) {
+                            P += 1;
+                            H += orc_pair_hash((int32_t)p, (int32_t)p);
+                        } else {
+                            P += 2;
+                            H += orc_pair_hash((int32_t)p, (int32_t)q) + orc_pair_hash((int32_t)q, (int32_t)p);
+                        }
+                    }
+                }
+            }
+        }
+        free(nb);
+    }
+    *pairs = P; *hash = H; *evals = E;
+    return 0;
+}
+
 /* Neighbour count of every point (its row length in the neighbour table). */
 int orc_join_degrees(const orc_index *ix, int fma_mode, int nthreads, uint32_t *deg)
 {

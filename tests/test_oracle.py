@@ -107,3 +107,20 @@ def test_degrees_sum_to_pairs():
     k, _ = ix.pairs()
     assert int(deg.sum()) == len(k)
     assert np.array_equal(np.bincount(k, minlength=len(pts)), deg)
+
+
+@pytest.mark.parametrize("n,d,k,eps,kind", [
+    (3000, 2, 2, 0.02, "uniform"),
+    (2000, 6, 6, 0.08, "exp"),
+    (1500, 8, 4, 0.2, "uniform"),
+])
+def test_unicomp_stats_equal_full_stencil_stats(n, d, k, eps, kind):
+    """The CPU baseline's linear-ID Unicomp join: over all points the same pair
+    count and set hash as the full-stencil join, with about half its candidate
+    evaluations (each unordered pair once, plus the diagonal)."""
+    pts = np.random.default_rng(n + 7 * d).random((n, d)) if kind == "uniform" else exp_points(n, d, n + d)
+    ix = oracle.OracleIndex(pts, eps, k)
+    P, H, E = ix.stats()
+    Pu, Hu, Eu = ix.stats(unicomp=True)
+    assert (Pu, Hu) == (P, H)
+    assert Eu == (E + n) // 2
